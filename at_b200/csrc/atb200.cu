@@ -1,0 +1,738 @@
+/*
+ * Host runtime of the C ABI declared in include/atb200.h: device buffers,
+ * lattice tables, segment planning, launch configuration and the
+ * refpts-snapshot streaming of at_atpass (pyat/at.c:340-681).
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/atb200.h"
+#include "atb_kernel_api.h"
+#include "atb_table.h"
+
+/* FP64 roofline probe: independent DFMA chains, no memory traffic */
+__global__ void atb_dfma_probe(double* out, int iters, double a, double b) {
+    double x0 = threadIdx.x * 1e-9, x1 = x0 + 1e-9, x2 = x0 + 2e-9, x3 = x0 + 3e-9;
+    double x4 = x0 + 4e-9, x5 = x0 + 5e-9, x6 = x0 + 6e-9, x7 = x0 + 7e-9;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+        }
+    }
+    double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == 12345.678) out[0] = s;   /* keeps the chains live */
+}
+
+extern "C" __global__ void atb_track_kernel_exact(const AtbJob*, const AtbTile*, int, int*, int*,
+                                                  int);
+extern "C" __global__ void atb_track_kernel_fast(const AtbJob*, const AtbTile*, int, int*, int*,
+                                                 int);
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define ATB_CUDA(call)                                                                 \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return fail(ATB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+/* A growable device allocation. */
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct Lattice {
+    bool used = false;
+    int nelem = 0;
+    int64_t nwords = 0;
+    std::vector<uint32_t> off;
+    std::vector<AtbSeg> segs;   /* pipelined segments (empty when resident) */
+    bool resident = false;
+    int plan_cap = 0;           /* seg capacity used to build the plan      */
+    DevBuf words, doff, dsegs;
+};
+
+}  // namespace
+
+struct atb_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    int smem_optin = 0;
+    int threads = 256;
+    int seg_cap_words = 6144;          /* 48 KB per buffer, two buffers    */
+    int resident_max_words = 14336;    /* tables up to 112 KB stay resident */
+    int64_t rout_budget = 4LL << 30;
+    std::vector<Lattice> lats;
+    DevBuf r, rout, lost, lturn, lelem, lcoord, refpts, jobs, tiles, counter, status, alive,
+        moments;
+    std::vector<AtbTile> h_tiles;
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+/* greedy segmentation of the element records, each segment <= cap words */
+int plan_segments(Lattice& L, int cap) {
+    L.segs.clear();
+    int i = 0;
+    while (i < L.nelem) {
+        int j = i;
+        while (j < L.nelem && (int64_t)(L.off[j + 1] - L.off[i]) <= cap) ++j;
+        if (j == i)
+            return fail(ATB_ERR_ARG, "element record longer than the shared-memory segment");
+        AtbSeg s;
+        s.first_elem = i;
+        s.nelem = j - i;
+        s.word0 = L.off[i];
+        int nw = (int)(L.off[j] - L.off[i]);
+        s.nwords = nw + (nw & 1);
+        s.pad = 0;
+        L.segs.push_back(s);
+        i = j;
+    }
+    L.plan_cap = cap;
+    return ATB_OK;
+}
+
+int seg_of(const Lattice& L, int elem) {
+    /* index of the segment holding element `elem` */
+    int lo = 0, hi = (int)L.segs.size() - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) / 2;
+        if (L.segs[mid].first_elem <= elem) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+int upload_plan(atb_handle* h, Lattice& L) {
+    L.resident = (L.nelem > 0) && (L.nwords <= h->resident_max_words);
+    if (L.resident) {
+        L.segs.clear();
+        AtbSeg s;
+        s.first_elem = 0;
+        s.nelem = L.nelem;
+        s.word0 = 0;
+        s.nwords = (int)(L.nwords + (L.nwords & 1));
+        s.pad = 0;
+        L.segs.push_back(s);
+        L.plan_cap = h->seg_cap_words;
+    } else {
+        int rc = plan_segments(L, h->seg_cap_words);
+        if (rc) return rc;
+    }
+    if (!L.segs.empty()) {
+        if (L.dsegs.ensure(L.segs.size() * sizeof(AtbSeg)) != cudaSuccess)
+            return fail(ATB_ERR_CUDA, "cudaMalloc(segments) failed");
+        ATB_CUDA(cudaMemcpy(L.dsegs.p, L.segs.data(), L.segs.size() * sizeof(AtbSeg),
+                            cudaMemcpyHostToDevice));
+    }
+    return ATB_OK;
+}
+
+/* at.c refpts walk (pyat/at.c:618-651): snapshots taken in one turn */
+int64_t count_records(const uint32_t* refpts, int nref, int start, int end, int nelem) {
+    const uint32_t kNone = 0x7fffffffu; /* INT_MAX as at.c assigns it */
+    int nri = 0;
+    uint32_t nextref = (nri < nref) ? refpts[nri++] : kNone;
+    int64_t cnt = 0;
+    for (int e = start; e < end; ++e) {
+        if ((uint32_t)e == nextref) {
+            ++cnt;
+            nextref = (nri < nref) ? refpts[nri++] : kNone;
+        }
+    }
+    if ((uint32_t)nelem == nextref) ++cnt;
+    return cnt;
+}
+
+void fill_job_lattice(AtbJob& J, const Lattice& L, int start_elem, int end_elem) {
+    J.table = L.words.as<double>();
+    J.segs = L.dsegs.as<AtbSeg>();
+    J.elem_off = L.doff.as<uint32_t>();
+    J.nelem = L.nelem;
+    J.resident = L.resident ? 1 : 0;
+    J.start_elem = start_elem;
+    J.end_elem = end_elem;
+    if (L.nelem == 0 || L.segs.empty()) {
+        J.resident = 0;
+        J.seg_first0 = 0;
+        J.nseg_first = 0;
+        J.nseg_turn = 0;
+    } else if (L.resident) {
+        J.seg_first0 = 0;
+        J.nseg_first = 1;
+        J.nseg_turn = 1;
+    } else {
+        if (start_elem >= end_elem) {
+            J.seg_first0 = 0;
+            J.nseg_first = 0;
+        } else {
+            J.seg_first0 = seg_of(L, start_elem);
+            J.nseg_first = seg_of(L, end_elem - 1) - J.seg_first0 + 1;
+        }
+        J.nseg_turn = (end_elem > 0) ? seg_of(L, end_elem - 1) + 1 : 0;
+    }
+}
+
+int kernel_config(atb_handle* h, const std::vector<const Lattice*>& lats, int mode,
+                  int* smem_bytes, int* grid_max) {
+    bool any_pipe = false;
+    int64_t res_words = 0;
+    for (const Lattice* L : lats) {
+        if (L->resident) res_words = std::max<int64_t>(res_words, L->nwords + (L->nwords & 1));
+        else if (!L->segs.empty()) any_pipe = true;
+    }
+    int64_t words = any_pipe ? 2LL * h->seg_cap_words : 0;
+    words = std::max<int64_t>(words, res_words);
+    int bytes = (int)(words * 8);
+    if (bytes > h->smem_optin)
+        return fail(ATB_ERR_ARG, "shared-memory plan exceeds the per-block limit");
+    *smem_bytes = bytes;
+    const void* fn = mode == ATB_MODE_EXACT ? (const void*)atb_track_kernel_exact
+                                            : (const void*)atb_track_kernel_fast;
+    int per_sm = 0;
+    ATB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->threads, bytes));
+    if (per_sm < 1) return fail(ATB_ERR_ARG, "launch configuration does not fit on an SM");
+    *grid_max = per_sm * h->sm_count;
+    return ATB_OK;
+}
+
+int launch(atb_handle* h, const std::vector<AtbJob>& jobs, const std::vector<AtbTile>& tiles,
+           int smem_bytes, int grid_max, int mode, cudaStream_t st) {
+    if (tiles.empty()) return ATB_OK;
+    if (h->jobs.ensure(jobs.size() * sizeof(AtbJob)) != cudaSuccess ||
+        h->tiles.ensure(tiles.size() * sizeof(AtbTile)) != cudaSuccess)
+        return fail(ATB_ERR_CUDA, "cudaMalloc(launch lists) failed");
+    ATB_CUDA(cudaMemcpyAsync(h->jobs.p, jobs.data(), jobs.size() * sizeof(AtbJob),
+                             cudaMemcpyHostToDevice, st));
+    ATB_CUDA(cudaMemcpyAsync(h->tiles.p, tiles.data(), tiles.size() * sizeof(AtbTile),
+                             cudaMemcpyHostToDevice, st));
+    ATB_CUDA(cudaMemsetAsync(h->counter.p, 0, sizeof(int), st));
+    int grid = std::min<int64_t>((int64_t)tiles.size(), grid_max);
+    int cap = h->seg_cap_words;
+    if (mode == ATB_MODE_EXACT)
+        atb_track_kernel_exact<<<grid, h->threads, smem_bytes, st>>>(
+            h->jobs.as<AtbJob>(), h->tiles.as<AtbTile>(), (int)tiles.size(), h->counter.as<int>(),
+            h->status.as<int>(), cap);
+    else
+        atb_track_kernel_fast<<<grid, h->threads, smem_bytes, st>>>(
+            h->jobs.as<AtbJob>(), h->tiles.as<AtbTile>(), (int)tiles.size(), h->counter.as<int>(),
+            h->status.as<int>(), cap);
+    ATB_CUDA(cudaGetLastError());
+    return ATB_OK;
+}
+
+void make_tiles(std::vector<AtbTile>& tiles, int job, int64_t np, int threads) {
+    for (int64_t f = 0; f < np; f += threads) {
+        AtbTile t;
+        t.job = job;
+        t.first = f;
+        t.count = (int32_t)std::min<int64_t>(threads, np - f);
+        tiles.push_back(t);
+    }
+}
+
+Lattice* get_lat(atb_handle* h, int id) {
+    if (id < 0 || id >= (int)h->lats.size() || !h->lats[id].used) return nullptr;
+    return &h->lats[id];
+}
+
+int check_status(atb_handle* h, cudaStream_t st) {
+    int s = 0;
+    ATB_CUDA(cudaMemcpyAsync(&s, h->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ATB_CUDA(cudaStreamSynchronize(st));
+    if (s & ATB_STATUS_WAIT_TIMEOUT) {
+        cudaMemsetAsync(h->status.p, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
+        return fail(ATB_ERR_TIMEOUT, "a bounded shared-memory staging wait timed out");
+    }
+    return ATB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int atb_version(void) { return 10000; }
+
+const char* atb_last_error(void) { return g_err.c_str(); }
+
+int atb_device_count(int* count) {
+    if (!count) return fail(ATB_ERR_ARG, "count is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *count = 0;
+        return fail(ATB_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    }
+    *count = n;
+    return ATB_OK;
+}
+
+int atb_device_info(int device, char* name, int name_len, int* cc_major, int* cc_minor,
+                    int* sm_count, uint64_t* total_mem) {
+    cudaDeviceProp p;
+    ATB_CUDA(cudaGetDeviceProperties(&p, device));
+    if (name && name_len > 0) {
+        std::strncpy(name, p.name, name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    if (cc_major) *cc_major = p.major;
+    if (cc_minor) *cc_minor = p.minor;
+    if (sm_count) *sm_count = p.multiProcessorCount;
+    if (total_mem) *total_mem = p.totalGlobalMem;
+    return ATB_OK;
+}
+
+int atb_create(int device, atb_handle** out) {
+    if (!out) return fail(ATB_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    ATB_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) return fail(ATB_ERR_ARG, "invalid device id");
+    DeviceGuard g(device);
+    std::unique_ptr<atb_handle> h(new atb_handle());
+    h->device = device;
+    cudaDeviceProp p;
+    ATB_CUDA(cudaGetDeviceProperties(&p, device));
+    if (p.major < 10)
+        return fail(ATB_ERR_ARG, "this build targets sm_100a (B200); device is sm_" +
+                                     std::to_string(p.major) + std::to_string(p.minor));
+    h->sm_count = p.multiProcessorCount;
+    ATB_CUDA(cudaDeviceGetAttribute(&h->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                    device));
+    /* leave room for the kernel's static shared memory */
+    h->smem_optin -= 1024;
+    ATB_CUDA(cudaFuncSetAttribute(atb_track_kernel_exact,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
+    ATB_CUDA(cudaFuncSetAttribute(atb_track_kernel_fast,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
+    ATB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    if (h->counter.ensure(sizeof(int)) != cudaSuccess || h->status.ensure(sizeof(int)) != cudaSuccess)
+        return fail(ATB_ERR_CUDA, "cudaMalloc failed");
+    ATB_CUDA(cudaMemset(h->status.p, 0, sizeof(int)));
+    *out = h.release();
+    return ATB_OK;
+}
+
+int atb_destroy(atb_handle* h) {
+    if (!h) return ATB_OK;
+    {
+        DeviceGuard g(h->device);
+        if (h->stream) cudaStreamSynchronize(h->stream);
+        for (Lattice& L : h->lats) {
+            L.words.release();
+            L.doff.release();
+            L.dsegs.release();
+        }
+        for (DevBuf* b : {&h->r, &h->rout, &h->lost, &h->lturn, &h->lelem, &h->lcoord,
+                          &h->refpts, &h->jobs, &h->tiles, &h->counter, &h->status, &h->alive,
+                          &h->moments})
+            b->release();
+        if (h->stream) cudaStreamDestroy(h->stream);
+    }
+    delete h;
+    return ATB_OK;
+}
+
+int atb_set_launch(atb_handle* h, int threads, int seg_cap_words, int resident_max_words,
+                   int64_t rout_budget_bytes) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    if (threads) {
+        if (threads < 32 || threads > ATB_MAX_THREADS || threads % 32)
+            return fail(ATB_ERR_ARG, "threads per block must be a multiple of 32 in [32, 512]");
+        h->threads = threads;
+    }
+    if (seg_cap_words) {
+        if (seg_cap_words < ATB_MAX_RECORD_WORDS + 1 || seg_cap_words % 2 ||
+            (int64_t)seg_cap_words * 16 > h->smem_optin)
+            return fail(ATB_ERR_ARG, "segment capacity out of range");
+        h->seg_cap_words = seg_cap_words;
+    }
+    if (resident_max_words) {
+        if ((int64_t)resident_max_words * 8 > h->smem_optin)
+            return fail(ATB_ERR_ARG, "resident table limit exceeds shared memory");
+        h->resident_max_words = resident_max_words;
+    }
+    if (rout_budget_bytes > 0) h->rout_budget = rout_budget_bytes;
+    /* re-plan every lattice for the new capacities */
+    DeviceGuard g(h->device);
+    for (Lattice& L : h->lats)
+        if (L.used) {
+            int rc = upload_plan(h, L);
+            if (rc) return rc;
+        }
+    return ATB_OK;
+}
+
+int atb_lattice_upload(atb_handle* h, const double* words, int64_t nwords,
+                       const uint32_t* elem_off, int32_t nelem, int32_t* lattice_id) {
+    if (!h || !lattice_id) return fail(ATB_ERR_ARG, "NULL argument");
+    if (nelem < 0 || nwords < 0 || (nelem > 0 && (!words || !elem_off)))
+        return fail(ATB_ERR_ARG, "invalid lattice table");
+    if (nelem > 0 && (elem_off[0] != 0 || (int64_t)elem_off[nelem] != nwords))
+        return fail(ATB_ERR_ARG, "element offsets do not span the table");
+    for (int i = 0; i < nelem; ++i) {
+        uint32_t a = elem_off[i], b = elem_off[i + 1];
+        if (b <= a || (a & 1u) || (b - a) > ATB_MAX_RECORD_WORDS)
+            return fail(ATB_ERR_ARG, "invalid element record bounds");
+        uint64_t hdr;
+        std::memcpy(&hdr, words + a, 8);
+        uint32_t len = (uint32_t)((hdr >> ATB_H_LEN_SHIFT) & ATB_H_LEN_MASK);
+        uint32_t op = (uint32_t)((hdr >> ATB_H_OP_SHIFT) & ATB_H_OP_MASK);
+        if (len != b - a || op >= ATB_NUM_OPS)
+            return fail(ATB_ERR_ARG, "corrupt element record header");
+    }
+    DeviceGuard g(h->device);
+    int id = -1;
+    for (int i = 0; i < (int)h->lats.size(); ++i)
+        if (!h->lats[i].used) { id = i; break; }
+    if (id < 0) {
+        h->lats.emplace_back();
+        id = (int)h->lats.size() - 1;
+    }
+    Lattice& L = h->lats[id];
+    L.used = true;
+    L.nelem = nelem;
+    L.nwords = nwords;
+    L.off.assign(elem_off, elem_off + nelem + 1);
+    if (nelem == 0) L.off.assign(1, 0u);
+    size_t wbytes = (size_t)(nwords + 2) * 8;
+    if (L.words.ensure(wbytes) != cudaSuccess || L.doff.ensure(L.off.size() * 4) != cudaSuccess) {
+        L.used = false;
+        return fail(ATB_ERR_CUDA, "cudaMalloc(lattice) failed");
+    }
+    ATB_CUDA(cudaMemset(L.words.p, 0, wbytes));
+    if (nwords) ATB_CUDA(cudaMemcpy(L.words.p, words, nwords * 8, cudaMemcpyHostToDevice));
+    ATB_CUDA(cudaMemcpy(L.doff.p, L.off.data(), L.off.size() * 4, cudaMemcpyHostToDevice));
+    int rc = upload_plan(h, L);
+    if (rc) {
+        L.used = false;
+        return rc;
+    }
+    *lattice_id = id;
+    return ATB_OK;
+}
+
+int atb_lattice_update(atb_handle* h, int32_t id, const double* words, int64_t nwords) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Lattice* L = get_lat(h, id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    if (nwords != L->nwords) return fail(ATB_ERR_ARG, "table size changed");
+    DeviceGuard g(h->device);
+    ATB_CUDA(cudaStreamSynchronize(h->stream));
+    if (nwords) ATB_CUDA(cudaMemcpy(L->words.p, words, nwords * 8, cudaMemcpyHostToDevice));
+    return ATB_OK;
+}
+
+int atb_lattice_free(atb_handle* h, int32_t id) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Lattice* L = get_lat(h, id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    DeviceGuard g(h->device);
+    cudaStreamSynchronize(h->stream);
+    L->words.release();
+    L->doff.release();
+    L->dsegs.release();
+    L->used = false;
+    return ATB_OK;
+}
+
+int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns, int32_t turn0,
+              int32_t start_elem, int32_t end_elem, const uint32_t* refpts, int32_t nref,
+              double* rout, int32_t losses, uint8_t* islost, uint32_t* lturn, uint32_t* lelem,
+              double* lcoord, uint32_t* alive, double* moments, int32_t mode, int32_t flags) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Lattice* L = get_lat(h, id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    if (np < 0 || nturns < 0 || nref < 0) return fail(ATB_ERR_ARG, "negative size");
+    if (np > 0 && !rin) return fail(ATB_ERR_ARG, "rin is NULL");
+    if (nref > 0 && (!refpts || (!rout && np > 0))) return fail(ATB_ERR_ARG, "refpts/rout missing");
+    if (losses && np > 0 && (!islost || !lturn || !lelem || !lcoord))
+        return fail(ATB_ERR_ARG, "loss map buffers missing");
+    if (mode != ATB_MODE_EXACT && mode != ATB_MODE_FAST) return fail(ATB_ERR_ARG, "bad mode");
+    const int nelem = L->nelem;
+    if (nelem > 0) {
+        if (start_elem < 0 || start_elem >= nelem || end_elem < 0 || end_elem > nelem ||
+            start_elem > end_elem)
+            return fail(ATB_ERR_ARG, "start_elem/end_elem out of range");
+    } else {
+        start_elem = end_elem = 0;
+    }
+    if (np == 0 || nturns == 0) return ATB_OK;
+    DeviceGuard g(h->device);
+    cudaStream_t st = h->stream;
+
+    /* device buffers */
+    const size_t rbytes = (size_t)np * 48;
+    if (h->r.ensure(rbytes) != cudaSuccess) return fail(ATB_ERR_NOMEM, "cudaMalloc(particles) failed");
+    ATB_CUDA(cudaMemcpyAsync(h->r.p, rin, rbytes, cudaMemcpyHostToDevice, st));
+    if (losses) {
+        if (h->lost.ensure(np) != cudaSuccess || h->lturn.ensure(np * 4) != cudaSuccess ||
+            h->lelem.ensure(np * 4) != cudaSuccess || h->lcoord.ensure(rbytes) != cudaSuccess)
+            return fail(ATB_ERR_NOMEM, "cudaMalloc(loss map) failed");
+        ATB_CUDA(cudaMemsetAsync(h->lost.p, 0, np, st));
+        ATB_CUDA(cudaMemsetAsync(h->lturn.p, 0, np * 4, st));
+        ATB_CUDA(cudaMemsetAsync(h->lelem.p, 0, np * 4, st));
+        ATB_CUDA(cudaMemsetAsync(h->lcoord.p, 0, rbytes, st));
+    }
+    if (alive || moments) {
+        if (h->alive.ensure((size_t)nturns * 4) != cudaSuccess ||
+            h->moments.ensure((size_t)nturns * 96) != cudaSuccess)
+            return fail(ATB_ERR_NOMEM, "cudaMalloc(statistics) failed");
+        ATB_CUDA(cudaMemsetAsync(h->alive.p, 0, (size_t)nturns * 4, st));
+        ATB_CUDA(cudaMemsetAsync(h->moments.p, 0, (size_t)nturns * 96, st));
+    }
+    if (nref > 0) {
+        if (h->refpts.ensure((size_t)nref * 4) != cudaSuccess)
+            return fail(ATB_ERR_NOMEM, "cudaMalloc(refpts) failed");
+        ATB_CUDA(cudaMemcpyAsync(h->refpts.p, refpts, (size_t)nref * 4, cudaMemcpyHostToDevice, st));
+    }
+
+    /* turn chunks bounded by the snapshot budget */
+    const int64_t rec_first = nref ? count_records(refpts, nref, start_elem, end_elem, nelem) : 0;
+    const int64_t rec_turn = nref ? count_records(refpts, nref, 0, end_elem, nelem) : 0;
+    const int64_t slot_bytes = (int64_t)np * 48;
+    int64_t turns_per_chunk = nturns;
+    if (nref > 0 && rec_turn > 0) {
+        int64_t per_turn = rec_turn * slot_bytes;
+        turns_per_chunk = std::max<int64_t>(1, h->rout_budget / std::max<int64_t>(per_turn, 1));
+        if (std::max(rec_first, rec_turn) * slot_bytes > h->rout_budget)
+            return fail(ATB_ERR_NOMEM, "one turn of refpts snapshots exceeds the device budget");
+    }
+    const int64_t max_slots = nref ? std::max<int64_t>(rec_first, 0) +
+                                         (turns_per_chunk - 1) * rec_turn + rec_turn
+                                   : 0;
+    if (nref > 0 && max_slots > 0) {
+        if (h->rout.ensure((size_t)(max_slots * slot_bytes)) != cudaSuccess)
+            return fail(ATB_ERR_NOMEM, "cudaMalloc(refpts snapshots) failed");
+    }
+
+    std::vector<const Lattice*> lats{L};
+    int smem = 0, grid_max = 0;
+    int rc = kernel_config(h, lats, mode, &smem, &grid_max);
+    if (rc) return rc;
+
+    int64_t slot_done = 0;
+    for (int64_t t0 = 0; t0 < nturns; t0 += turns_per_chunk) {
+        const int nt = (int)std::min<int64_t>(turns_per_chunk, nturns - t0);
+        AtbJob J;
+        std::memset(&J, 0, sizeof(J));
+        fill_job_lattice(J, *L, t0 == 0 ? start_elem : 0, end_elem);
+        J.check_loss = (flags & ATB_FLAG_ELEMENT) ? 0 : 1;
+        J.r = h->r.as<double>();
+        J.np = np;
+        J.turn0 = turn0 + (int32_t)t0;
+        J.nturns = nt;
+        J.refpts = h->refpts.as<uint32_t>();
+        J.nref = nref;
+        J.losses = losses ? 1 : 0;
+        J.rout = nref ? h->rout.as<double>() : nullptr;
+        J.rout_slot0 = 0;
+        J.lost = h->lost.as<uint8_t>();
+        J.lturn = h->lturn.as<uint32_t>();
+        J.lelem = h->lelem.as<uint32_t>();
+        J.lcoord = h->lcoord.as<double>();
+        J.alive = (alive || moments) ? h->alive.as<uint32_t>() + t0 : nullptr;
+        J.moments = (alive || moments) ? h->moments.as<double>() + 12 * t0 : nullptr;
+        std::vector<AtbJob> jobs{J};
+        h->h_tiles.clear();
+        make_tiles(h->h_tiles, 0, np, h->threads);
+        rc = launch(h, jobs, h->h_tiles, smem, grid_max, mode, st);
+        if (rc) return rc;
+        if (nref) {
+            int64_t slots = (t0 == 0 ? rec_first : rec_turn) + (int64_t)(nt - 1) * rec_turn;
+            if (slots > 0)
+                ATB_CUDA(cudaMemcpyAsync(rout + slot_done * (slot_bytes / 8), h->rout.p,
+                                         (size_t)(slots * slot_bytes), cudaMemcpyDeviceToHost, st));
+            slot_done += slots;
+        }
+        /* the job/tile lists are host vectors reused next chunk: make sure
+           the copies above have consumed them */
+        ATB_CUDA(cudaStreamSynchronize(st));
+    }
+    ATB_CUDA(cudaMemcpyAsync(rin, h->r.p, rbytes, cudaMemcpyDeviceToHost, st));
+    if (losses) {
+        ATB_CUDA(cudaMemcpyAsync(islost, h->lost.p, np, cudaMemcpyDeviceToHost, st));
+        ATB_CUDA(cudaMemcpyAsync(lturn, h->lturn.p, np * 4, cudaMemcpyDeviceToHost, st));
+        ATB_CUDA(cudaMemcpyAsync(lelem, h->lelem.p, np * 4, cudaMemcpyDeviceToHost, st));
+        ATB_CUDA(cudaMemcpyAsync(lcoord, h->lcoord.p, rbytes, cudaMemcpyDeviceToHost, st));
+    }
+    if (alive) ATB_CUDA(cudaMemcpyAsync(alive, h->alive.p, (size_t)nturns * 4, cudaMemcpyDeviceToHost, st));
+    if (moments)
+        ATB_CUDA(cudaMemcpyAsync(moments, h->moments.p, (size_t)nturns * 96, cudaMemcpyDeviceToHost, st));
+    return check_status(h, st);
+}
+
+int atb_track_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t nturns,
+                     int32_t turn0, int32_t losses, uint8_t* islost, uint32_t* lturn,
+                     uint32_t* lelem, double* lcoord, uint32_t* alive, double* moments,
+                     int32_t mode, void* stream) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Lattice* L = get_lat(h, id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    if (np < 0 || nturns < 0) return fail(ATB_ERR_ARG, "negative size");
+    if (np > 0 && !r) return fail(ATB_ERR_ARG, "r is NULL");
+    if (losses && np > 0 && (!islost || !lturn || !lelem || !lcoord))
+        return fail(ATB_ERR_ARG, "loss map buffers missing");
+    if (mode != ATB_MODE_EXACT && mode != ATB_MODE_FAST) return fail(ATB_ERR_ARG, "bad mode");
+    if (np == 0 || nturns == 0) return ATB_OK;
+    DeviceGuard g(h->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    std::vector<const Lattice*> lats{L};
+    int smem = 0, grid_max = 0;
+    int rc = kernel_config(h, lats, mode, &smem, &grid_max);
+    if (rc) return rc;
+    AtbJob J;
+    std::memset(&J, 0, sizeof(J));
+    fill_job_lattice(J, *L, 0, L->nelem);
+    J.check_loss = 1;
+    J.r = r;
+    J.np = np;
+    J.turn0 = turn0;
+    J.nturns = nturns;
+    J.losses = losses ? 1 : 0;
+    J.lost = islost;
+    J.lturn = lturn;
+    J.lelem = lelem;
+    J.lcoord = lcoord;
+    J.alive = alive;
+    J.moments = moments;
+    std::vector<AtbJob> jobs{J};
+    h->h_tiles.clear();
+    make_tiles(h->h_tiles, 0, np, h->threads);
+    /* pageable-source copies of the launch lists are staged before
+       cudaMemcpyAsync returns, so the host vectors may be reused at once */
+    return launch(h, jobs, h->h_tiles, smem, grid_max, mode, st);
+}
+
+int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,
+                    void* stream) {
+    if (!h || (njobs > 0 && !jobs)) return fail(ATB_ERR_ARG, "NULL argument");
+    if (mode != ATB_MODE_EXACT && mode != ATB_MODE_FAST) return fail(ATB_ERR_ARG, "bad mode");
+    if (njobs <= 0) return ATB_OK;
+    DeviceGuard g(h->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    std::vector<const Lattice*> lats;
+    std::vector<AtbJob> J(njobs);
+    for (int j = 0; j < njobs; ++j) {
+        const atb_job_desc& d = jobs[j];
+        Lattice* L = get_lat(h, d.lattice_id);
+        if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id in batch");
+        if (d.np < 0 || d.nturns < 0 || (d.np > 0 && !d.r))
+            return fail(ATB_ERR_ARG, "invalid batch job");
+        if (d.losses && d.np > 0 && (!d.islost || !d.lturn || !d.lelem || !d.lcoord))
+            return fail(ATB_ERR_ARG, "loss map buffers missing in batch job");
+        lats.push_back(L);
+        std::memset(&J[j], 0, sizeof(AtbJob));
+        fill_job_lattice(J[j], *L, 0, L->nelem);
+        J[j].check_loss = 1;
+        J[j].r = d.r;
+        J[j].np = d.np;
+        J[j].turn0 = d.turn0;
+        J[j].nturns = d.nturns;
+        J[j].losses = d.losses ? 1 : 0;
+        J[j].lost = d.islost;
+        J[j].lturn = d.lturn;
+        J[j].lelem = d.lelem;
+        J[j].lcoord = d.lcoord;
+    }
+    int smem = 0, grid_max = 0;
+    int rc = kernel_config(h, lats, mode, &smem, &grid_max);
+    if (rc) return rc;
+    /* longest-processing-time first: order jobs by turns x elements */
+    std::vector<int> order(njobs);
+    for (int j = 0; j < njobs; ++j) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        double ca = (double)J[a].nturns * (lats[a]->nwords + 1);
+        double cb = (double)J[b].nturns * (lats[b]->nwords + 1);
+        return ca > cb;
+    });
+    h->h_tiles.clear();
+    for (int j : order)
+        if (J[j].nturns > 0) make_tiles(h->h_tiles, j, J[j].np, h->threads);
+    return launch(h, J, h->h_tiles, smem, grid_max, mode, st);
+}
+
+int atb_fp64_peak(int device, double* tflops, double* seconds) {
+    if (!tflops) return fail(ATB_ERR_ARG, "tflops is NULL");
+    DeviceGuard g(device);
+    cudaDeviceProp p;
+    ATB_CUDA(cudaGetDeviceProperties(&p, device));
+    const int threads = 256, blocks = p.multiProcessorCount * 8, iters = 4096;
+    double* out = nullptr;
+    ATB_CUDA(cudaMalloc(&out, sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    atb_dfma_probe<<<blocks, threads>>>(out, 64, 0.999999, 1e-7);   /* warm-up */
+    cudaEventRecord(e0);
+    atb_dfma_probe<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+    cudaEventRecord(e1);
+    cudaError_t err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (err != cudaSuccess) return fail(ATB_ERR_CUDA, cudaGetErrorString(err));
+    const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    if (seconds) *seconds = ms * 1e-3;
+    return ATB_OK;
+}
+
+int atb_sync(atb_handle* h, void* stream) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    DeviceGuard g(h->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    return check_status(h, st);
+}
+
+}  // extern "C"

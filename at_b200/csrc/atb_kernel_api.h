@@ -1,0 +1,64 @@
+/*
+ * Launch-side data structures of the tracking kernel (device and host).
+ *
+ * A launch processes a list of tiles; each tile is a contiguous run of at
+ * most blockDim particles of one job.  A job is one (lattice, particle set,
+ * turn range) triple with its output buffers, so the same kernel serves the
+ * plain drop-in call (one job), batched lattice variants (one job per
+ * variant) and the serving loop (one job per admitted request).
+ */
+#ifndef ATB_KERNEL_API_H
+#define ATB_KERNEL_API_H
+
+#include <stdint.h>
+
+#define ATB_MAX_THREADS 512
+/* bounded mbarrier wait: 1 s, then the kernel reports and returns */
+#define ATB_WAIT_NS 1000000000ULL
+#define ATB_STATUS_WAIT_TIMEOUT 1
+
+/* one staged lattice segment: consecutive element records */
+typedef struct AtbSeg {
+    int32_t first_elem;
+    int32_t nelem;
+    int64_t word0;     /* first word in the table (16-byte aligned)        */
+    int32_t nwords;    /* words copied (even)                              */
+    int32_t pad;
+} AtbSeg;
+
+typedef struct AtbJob {
+    const double* table;        /* element table words                      */
+    const AtbSeg* segs;         /* segment list                             */
+    const uint32_t* elem_off;   /* word offset of every element (+ end)     */
+    int32_t nelem;
+    int32_t resident;           /* whole table in one buffer                */
+    int32_t seg_first0;         /* first segment of the first turn          */
+    int32_t nseg_first;         /* segments visited in the first turn       */
+    int32_t nseg_turn;          /* segments visited in later turns          */
+    int32_t check_loss;         /* 0 for single-element tracking            */
+    double* r;                  /* (6, np) Fortran-order state              */
+    int64_t np;
+    int32_t turn0;              /* absolute turn number of the first turn   */
+    int32_t nturns;
+    int32_t start_elem;         /* first element of the first turn          */
+    int32_t end_elem;           /* one past the last element of every turn  */
+    const uint32_t* refpts;
+    int32_t nref;
+    int32_t losses;             /* 1: loss map (checkiflost), 0: setlost    */
+    double* rout;               /* (6, np, slots) snapshots                 */
+    int64_t rout_slot0;
+    uint8_t* lost;              /* loss map (losses == 1)                   */
+    uint32_t* lturn;
+    uint32_t* lelem;
+    double* lcoord;
+    uint32_t* alive;            /* optional: survivors after each turn     */
+    double* moments;            /* optional: 12 sums per turn              */
+} AtbJob;
+
+typedef struct AtbTile {
+    int32_t job;
+    int32_t count;
+    int64_t first;
+} AtbTile;
+
+#endif /* ATB_KERNEL_API_H */

@@ -1,0 +1,404 @@
+/*
+ * Per-particle integrators of the accelerated pass methods, as device
+ * functions over a register-resident 6-vector.
+ *
+ * Two arithmetic modes are compiled from this one source:
+ *   FAST == false  "exact": the reference's expression trees in the
+ *                  reference's evaluation order, compiled without FMA
+ *                  contraction (-fmad=false), IEEE division.  On the
+ *                  +,-,*,/ path this reproduces the reference C build bit for
+ *                  bit; only sin/tan go through CUDA's libdevice.
+ *   FAST == true   "fast": FMA contraction plus algebraic rewrites that drop
+ *                  divisions where the reference recomputes the same
+ *                  reciprocal (1/(1+delta) is carried through a slice, and
+ *                  x/p_norm becomes x*(1+delta)).  Each rewrite changes a
+ *                  result by at most a few ulp.
+ *
+ * Each function cites the reference routine it restates.
+ */
+#ifndef ATB_PHYSICS_CUH
+#define ATB_PHYSICS_CUH
+
+#include "atb_table.h"
+
+namespace atb {
+
+struct P6 {
+    double x, px, y, py, dp, ct;
+};
+
+#define ATB_C0 2.99792458e8
+
+__device__ __forceinline__ double inf_d() { return __longlong_as_double(0x7ff0000000000000LL); }
+__device__ __forceinline__ double nan_d() { return __longlong_as_double(0x7ff8000000000000LL); }
+
+__device__ __forceinline__ bool all_finite(const P6& r) {
+    return isfinite(r.x) && isfinite(r.px) && isfinite(r.y) && isfinite(r.py) &&
+           isfinite(r.dp) && isfinite(r.ct);
+}
+
+/* atlalib.c:50-57 ATaddvv */
+__device__ __forceinline__ void add_t(P6& r, const double* t) {
+    r.x += t[0]; r.px += t[1]; r.y += t[2]; r.py += t[3]; r.dp += t[4]; r.ct += t[5];
+}
+
+/* atlalib.c:17-32 ATmultmv: temp[i] = 0 + sum_j A[i+6j]*r[j], j ascending */
+__device__ __forceinline__ void mult_dense(P6& r, const double* A) {
+    const double r0 = r.x, r1 = r.px, r2 = r.y, r3 = r.py, r4 = r.dp, r5 = r.ct;
+    double t[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double s = 0.0;
+        s += A[i] * r0;
+        s += A[i + 6] * r1;
+        s += A[i + 12] * r2;
+        s += A[i + 18] * r3;
+        s += A[i + 24] * r4;
+        s += A[i + 30] * r5;
+        t[i] = s;
+    }
+    r.x = t[0]; r.px = t[1]; r.y = t[2]; r.py = t[3]; r.dp = t[4]; r.ct = t[5];
+}
+
+/* ATmultmv for a matrix that only rotates the x/y planes: the dense sum with
+ * its zero terms dropped, which is value-identical for finite coordinates.
+ * A non-finite coordinate takes the dense path so 0*inf -> NaN propagates as
+ * in the reference. */
+__device__ __forceinline__ void mult_tilt(P6& r, const double* m) {
+    if (!all_finite(r)) {
+        double A[36];
+#pragma unroll
+        for (int k = 0; k < 36; ++k) A[k] = 0.0;
+        A[0 + 6 * 0] = m[0]; A[0 + 6 * 2] = m[1];
+        A[1 + 6 * 1] = m[2]; A[1 + 6 * 3] = m[3];
+        A[2 + 6 * 0] = m[4]; A[2 + 6 * 2] = m[5];
+        A[3 + 6 * 1] = m[6]; A[3 + 6 * 3] = m[7];
+        A[4 + 6 * 4] = 1.0; A[5 + 6 * 5] = 1.0;
+        mult_dense(r, A);
+        return;
+    }
+    const double x = r.x, px = r.px, y = r.y, py = r.py;
+    r.x = m[0] * x + m[1] * y;
+    r.px = m[2] * px + m[3] * py;
+    r.y = m[4] * x + m[5] * y;
+    r.py = m[6] * px + m[7] * py;
+}
+
+__device__ __forceinline__ void mult_r(P6& r, const double* blk, bool dense) {
+    if (dense) mult_dense(r, blk); else mult_tilt(r, blk);
+}
+
+/* atlalib.c:169-175 checkiflostRectangularAp */
+__device__ __forceinline__ void check_rect(P6& r, const double* lim) {
+    if (r.x < lim[0] || r.x > lim[1]) r.ct = inf_d();
+    else if (r.y < lim[2] || r.y > lim[3]) r.ct = inf_d();
+}
+
+/* atlalib.c:185-190 checkiflostEllipticalAp */
+__device__ __forceinline__ void check_ellip(P6& r, const double* ax) {
+    double xn = r.x / ax[0];
+    double zn = r.y / ax[1];
+    if ((xn * xn + zn * zn) >= 1) r.ct = inf_d();
+}
+
+/* atlalib.c:70-75 ATChangePRef */
+template <bool FAST>
+__device__ __forceinline__ void change_pref(P6& r, double s) {
+    r.px /= s;
+    r.py /= s;
+    r.dp = (r.dp + 1.0 - s) / s;
+}
+
+/* atlalib.c:59-68 ATdrift6 == driftkickrad.c:36-45 drift6 == diff_drift.c:30-43
+ * (without the diffusion-matrix branch) */
+template <bool FAST>
+__device__ __forceinline__ void drift6(P6& r, double L) {
+    if (FAST) {
+        double pn = 1.0 / (1.0 + r.dp);
+        double nl = L * pn;
+        r.x += nl * r.px;
+        r.y += nl * r.py;
+        r.ct += (0.5 * nl * pn) * (r.px * r.px + r.py * r.py);
+    } else {
+        double pn = 1 / (1 + r.dp);
+        double nl = L * pn;
+        r.x += nl * r.px;
+        r.y += nl * r.py;
+        r.ct += nl * pn * (r.px * r.px + r.py * r.py) / 2;
+    }
+}
+
+/* driftkick.c:37-48 fastdrift.  FAST: c2 = NormL/(2(1+delta)) precomputed. */
+template <bool FAST>
+__device__ __forceinline__ void fastdrift(P6& r, double nl, double c2) {
+    r.x += nl * r.px;
+    r.y += nl * r.py;
+    if (FAST) r.ct += c2 * (r.px * r.px + r.py * r.py);
+    else r.ct += nl * (r.px * r.px + r.py * r.py) / (2 * (1 + r.dp));
+}
+
+/* The Horner recursion shared by every multipole kick
+ * (driftkick.c:51-115, diff_str_kick.c:33-40, diff_bnd_kick.c:40-47):
+ * Re + i Im = sum_n (B_n + i A_n)(x + i y)^n, highest order first. */
+template <int MO>
+__device__ __forceinline__ void horner_fixed(const double* A, const double* B, double x, double y,
+                                             double& re, double& im) {
+    re = B[MO];
+    im = A[MO];
+#pragma unroll
+    for (int i = MO - 1; i >= 0; --i) {
+        double ret = re * x - im * y + B[i];
+        im = im * x + re * y + A[i];
+        re = ret;
+    }
+}
+
+__device__ __forceinline__ void horner_dyn(const double* A, const double* B, int mo, double x,
+                                           double y, double& re, double& im) {
+    re = B[mo];
+    im = A[mo];
+    for (int i = mo - 1; i >= 0; --i) {
+        double ret = re * x - im * y + B[i];
+        im = im * x + re * y + A[i];
+        re = ret;
+    }
+}
+
+/* Coefficient holder: for MO >= 0 the coefficients are copied into
+ * registers once per element; MO < 0 reads them (broadcast) from the staged
+ * table on every kick. */
+template <int MO>
+struct Poly {
+    double a[MO + 1], b[MO + 1];
+    __device__ __forceinline__ void load(const double* A, const double* B, int) {
+#pragma unroll
+        for (int i = 0; i <= MO; ++i) { a[i] = A[i]; b[i] = B[i]; }
+    }
+    __device__ __forceinline__ void field(double x, double y, double& re, double& im) const {
+        horner_fixed<MO>(a, b, x, y, re, im);
+    }
+};
+
+template <>
+struct Poly<-1> {
+    const double* a;
+    const double* b;
+    int mo;
+    __device__ __forceinline__ void load(const double* A, const double* B, int m) {
+        a = A; b = B; mo = m;
+    }
+    __device__ __forceinline__ void field(double x, double y, double& re, double& im) const {
+        horner_dyn(a, b, mo, x, y, re, im);
+    }
+};
+
+/* driftkick.c:92-115 strthinkick */
+template <class PL>
+__device__ __forceinline__ void strthinkick(P6& r, const PL& pl, double L) {
+    double re, im;
+    pl.field(r.x, r.y, re, im);
+    r.px -= L * re;
+    r.py += L * im;
+}
+
+/* driftkick.c:51-89 bndthinkick; lirho = L*irho folded on the host */
+template <class PL>
+__device__ __forceinline__ void bndthinkick(P6& r, const PL& pl, double L, double irho,
+                                            double lirho) {
+    double re, im;
+    pl.field(r.x, r.y, re, im);
+    r.px -= L * (re - (r.dp - r.x * irho) * irho);
+    r.py += L * im;
+    r.ct += lirho * r.x;
+}
+
+/* Radiating kicks.  ``pn`` carries 1/(1+delta) between steps in FAST mode. */
+
+/* diff_str_kick.c:19-83 with B2perp of diff_str_kick.c:1-17 (bdiff == NULL) */
+template <bool FAST, class PL>
+__device__ __forceinline__ void str_kick_rad(P6& r, const PL& pl, double L, double radc,
+                                             double& pn) {
+    double re, im;
+    pl.field(r.x, r.y, re, im);
+    if (FAST) {
+        double xpr = r.px * pn;
+        double ypr = r.py * pn;
+        double s = xpr * xpr + ypr * ypr;
+        double vn = 1.0 / (1.0 + s);
+        double cr = im * ypr - re * xpr;
+        double b2p = (re * re + im * im + cr * cr) * vn;
+        double opd = 1.0 + r.dp;
+        double factor = (1.0 + 0.5 * s) * (opd * opd) * L;
+        r.dp -= radc * b2p * factor;
+        opd = 1.0 + r.dp;
+        pn = 1.0 / opd;
+        r.px = xpr * opd - L * re;
+        r.py = ypr * opd + L * im;
+    } else {
+        double p_norm = 1.0 / (1.0 + r.dp);
+        double xpr = r.px * p_norm;
+        double ypr = r.py * p_norm;
+        double v_norm2 = 1.0 / (1.0 + xpr * xpr + ypr * ypr);
+        double bx = im, by = re;
+        double b2p = (by * by + bx * bx + (bx * ypr - by * xpr) * (bx * ypr - by * xpr)) * v_norm2;
+        double factor = (1.0 + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
+        r.dp -= radc * b2p * factor;
+        p_norm = 1.0 / (1.0 + r.dp);
+        r.px = xpr / p_norm;
+        r.py = ypr / p_norm;
+        r.px -= L * re;
+        r.py += L * im;
+    }
+}
+
+/* diff_bnd_kick.c:101-174 with its B2perp (:85-99), bdiff == NULL */
+template <bool FAST, class PL>
+__device__ __forceinline__ void bnd_kick_rad(P6& r, const PL& pl, double L, double irho,
+                                             double lirho, double radc, double& pn) {
+    double re, im;
+    pl.field(r.x, r.y, re, im);
+    if (FAST) {
+        double xpr = r.px * pn;
+        double ypr = r.py * pn;
+        double hx = 1.0 + r.x * irho;
+        double s = xpr * xpr + ypr * ypr;
+        double vn = 1.0 / (hx * hx + s);
+        double by = re + irho;
+        double cr = im * ypr - by * xpr;
+        double b2p = ((by * by + im * im) * (hx * hx) + cr * cr) * vn;
+        double opd = 1.0 + r.dp;
+        double factor = (hx + 0.5 * s) * (opd * opd) * L;
+        double dp0 = r.dp;
+        r.dp -= radc * b2p * factor;
+        opd = 1.0 + r.dp;
+        pn = 1.0 / opd;
+        r.px = xpr * opd - L * (re - (dp0 - r.x * irho) * irho);
+        r.py = ypr * opd + L * im;
+        r.ct += lirho * r.x;
+    } else {
+        double p_norm = 1.0 / (1.0 + r.dp);
+        double x = r.x;
+        double xpr = r.px * p_norm;
+        double ypr = r.py * p_norm;
+        double bx = im, by = re + irho;
+        double v_norm2 = 1.0 / ((1.0 + x * irho) * (1.0 + x * irho) + xpr * xpr + ypr * ypr);
+        double b2p = ((by * (1 + x * irho)) * (by * (1 + x * irho)) +
+                      (bx * (1 + x * irho)) * (bx * (1 + x * irho)) +
+                      (bx * ypr - by * xpr) * (bx * ypr - by * xpr)) * v_norm2;
+        double factor = (1.0 + x * irho + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
+        double dp_0 = r.dp;
+        r.dp -= radc * b2p * factor;
+        p_norm = 1.0 / (1.0 + r.dp);
+        r.px = xpr / p_norm;
+        r.py = ypr / p_norm;
+        r.px -= L * (re - (dp_0 - r.x * irho) * irho);
+        r.py += L * im;
+        r.ct += lirho * r.x;
+    }
+}
+
+/* diff_drift.c:30-43 inside a radiating magnet; FAST reuses pn = 1/(1+delta) */
+template <bool FAST>
+__device__ __forceinline__ void diff_drift(P6& r, double L, double pn) {
+    if (FAST) {
+        double nl = L * pn;
+        r.x += nl * r.px;
+        r.y += nl * r.py;
+        r.ct += (0.5 * nl * pn) * (r.px * r.px + r.py * r.py);
+    } else {
+        double p_norm = 1.0 / (1.0 + r.dp);
+        double NormL = L * p_norm;
+        r.x += NormL * r.px;
+        r.y += NormL * r.py;
+        r.ct += NormL * p_norm * (r.px * r.px + r.py * r.py) / 2.0;
+    }
+}
+
+/* quadfringe.c:3-51 QuadFringePassP (sign=+1) / QuadFringePassN (sign=-1) */
+template <bool FAST>
+__device__ __forceinline__ void quad_fringe(P6& r, double b2, bool entrance) {
+    double u = b2 / (12.0 * (1.0 + r.dp));
+    double x2 = r.x * r.x;
+    double z2 = r.y * r.y;
+    double xz = r.x * r.y;
+    double gx = u * (x2 + 3 * z2) * r.x;
+    double gz = u * (z2 + 3 * x2) * r.y;
+    double r1tmp = 3 * u * (2 * xz * r.py - (x2 + z2) * r.px);
+    double r3tmp = 3 * u * (2 * xz * r.px - (x2 + z2) * r.py);
+    double dct = (gz * r.py - gx * r.px) / (1 + r.dp);
+    if (entrance) {
+        r.x += gx;
+        r.y -= gz;
+        r.ct -= dct;
+        r.px += r1tmp;
+        r.py -= r3tmp;
+    } else {
+        r.x -= gx;
+        r.y += gz;
+        r.ct += dct;
+        r.px -= r1tmp;
+        r.py += r3tmp;
+    }
+}
+
+/* one linear map of quadfringe.c:45-112 (x and y 2x2 blocks) */
+__device__ __forceinline__ void lin_fringe_map(P6& r, const double* m) {
+    const double x = r.x, px = r.px, y = r.y, py = r.py;
+    r.x = m[0] * x + m[1] * px;
+    r.px = m[2] * x + m[3] * px;
+    r.y = m[4] * y + m[5] * py;
+    r.py = m[6] * y + m[7] * py;
+}
+
+/* Edge focusing of BndMPoleSymplectic4Pass: atphyslib.c:15-79
+ * (edge_fringe_entrance / edge_fringe_exit).  sgn = +1 entrance, -1 exit.
+ * fy_c = irho*tan(edge) is used whenever the tangent's argument is exactly
+ * the edge angle (fringecorr == 0), as the reference then evaluates the same
+ * tan(edge_angle). */
+template <bool FAST>
+__device__ __forceinline__ void edge_fringe(P6& r, double irho, double edge, double fc,
+                                            double fx, double fy_c, int method, bool fc0,
+                                            double sgn) {
+    double fy;
+    if (method == ATB_BM_3) {
+        double q = r.px / (1 + r.dp);
+        fy = irho * tan(sgn > 0 ? (edge - fc + q) : (edge - fc - q));
+    } else {
+        double t;
+        if (FAST && fc0) {
+            fy = (method == ATB_BM_2) ? fy_c / (1 + r.dp) : fy_c;
+        } else {
+            t = edge - fc / (1 + r.dp);
+            double tn = (t == edge) ? fy_c : irho * tan(t);
+            fy = (method == ATB_BM_2) ? tn / (1 + r.dp) : tn;
+        }
+    }
+    r.px += r.x * fx;
+    r.py -= r.y * fy;
+}
+
+/* diff_bend_fringe.c:1-52 (bdiff == NULL) for the radiating bend */
+template <bool FAST>
+__device__ __forceinline__ void edge_fringe_rad(P6& r, double irho, double edge, double psi,
+                                                double fx, double fy_c, int method, bool fc0,
+                                                double sgn) {
+    double p_norm = 1.0 / (1.0 + r.dp);
+    double fy;
+    if (method == ATB_BM_3) {
+        fy = irho * tan(edge - psi + sgn * r.px * p_norm);
+    } else {
+        if (FAST && fc0) {
+            fy = (method == ATB_BM_2) ? fy_c * p_norm : fy_c;
+        } else {
+            double t = edge - psi * p_norm;
+            double tn = (t == edge) ? fy_c : irho * tan(t);
+            fy = (method == ATB_BM_2) ? tn * p_norm : tn;
+        }
+    }
+    r.px += r.x * fx;
+    r.py -= r.y * fy;
+}
+
+}  // namespace atb
+
+#endif  // ATB_PHYSICS_CUH

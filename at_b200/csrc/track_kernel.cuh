@@ -1,0 +1,580 @@
+/*
+ * The persistent multi-turn tracking kernel.
+ *
+ * One thread owns one particle's (x, px, y, py, delta, ct) in registers for
+ * all the turns of a launch.  A block walks the lattice program (the flat
+ * element table of atb_table.h) segment by segment: each segment is copied
+ * from global memory into shared memory by the bulk-copy (TMA) engine,
+ * double-buffered behind an mbarrier, and every element's parameters are then
+ * read from shared memory as warp-uniform broadcasts.  When the whole table
+ * fits in one buffer it is loaded once per block and stays resident.
+ *
+ * The turn/element loop, the refpts snapshots and the loss rule restate the
+ * reference engine (pyat/at.c:596-654, checkiflost :115-139, setlost
+ * :142-161); the per-element bodies restate the pass methods (see
+ * atb_physics.cuh).  This header is compiled twice, once per arithmetic mode
+ * (ATB_FAST = 0 / 1), into distinct kernel symbols.
+ */
+#ifndef ATB_TRACK_KERNEL_CUH
+#define ATB_TRACK_KERNEL_CUH
+
+#include <cstdint>
+#include "atb_physics.cuh"
+#include "atb_kernel_api.h"
+
+#ifndef ATB_FAST
+#error "define ATB_FAST to 0 or 1"
+#endif
+
+#define ATB_CAT2(a, b) a##b
+#define ATB_CAT(a, b) ATB_CAT2(a, b)
+#if ATB_FAST
+#define ATB_KSUFFIX _fast
+#else
+#define ATB_KSUFFIX _exact
+#endif
+
+namespace atb {
+
+constexpr bool kFast = (ATB_FAST != 0);
+
+/* ---------------- shared-memory staging (bulk copy + mbarrier) ---------- */
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile(
+        "mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+        "r"(bytes)
+        : "memory");
+}
+
+/* global -> shared bulk copy, completion signalled on the mbarrier
+ * (no multicast: the source is always this GPU's own memory) */
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+/* Bounded wait: gives up after ATB_WAIT_NS nanoseconds and reports it. */
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > ATB_WAIT_NS) return false;
+    }
+}
+
+/* ---------------- record access ------------------------------------------ */
+
+struct Rec {
+    const double* p;
+    uint64_t hdr;
+    uint64_t opt;
+    __device__ __forceinline__ int op() const { return (int)((hdr >> ATB_H_OP_SHIFT) & ATB_H_OP_MASK); }
+    __device__ __forceinline__ int mo() const { return (int)((hdr >> ATB_H_MO_SHIFT) & ATB_H_MO_MASK); }
+    __device__ __forceinline__ uint32_t flags() const { return (uint32_t)((hdr >> ATB_H_FL_SHIFT) & ATB_H_FL_MASK); }
+    __device__ __forceinline__ int nsteps() const { return (int)((hdr >> ATB_H_NS_SHIFT) & ATB_H_NS_MASK); }
+    __device__ __forceinline__ int len() const { return (int)((hdr >> ATB_H_LEN_SHIFT) & ATB_H_LEN_MASK); }
+    __device__ __forceinline__ const double* blk(int slot) const {
+        uint32_t o = (uint32_t)((opt >> (slot * ATB_OPT_BITS)) & ATB_OPT_MASK);
+        return o ? p + o : nullptr;
+    }
+    __device__ __forceinline__ double f(int w) const { return p[w]; }
+};
+
+/* ---------------- misalignment / aperture wrappers ----------------------- */
+
+__device__ __forceinline__ void entrance_misalign(P6& r, const Rec& e) {
+    const uint32_t fl = e.flags();
+    if (const double* t1 = e.blk(ATB_OPT_T1)) add_t(r, t1);
+    if (const double* r1 = e.blk(ATB_OPT_R1)) mult_r(r, r1, fl & ATB_F_R1_DENSE);
+}
+
+__device__ __forceinline__ void apertures(P6& r, const Rec& e) {
+    if (const double* ra = e.blk(ATB_OPT_RAP)) check_rect(r, ra);
+    if (const double* ea = e.blk(ATB_OPT_EAP)) check_ellip(r, ea);
+}
+
+__device__ __forceinline__ void exit_misalign(P6& r, const Rec& e) {
+    const uint32_t fl = e.flags();
+    if (const double* r2 = e.blk(ATB_OPT_R2)) mult_r(r, r2, fl & ATB_F_R2_DENSE);
+    if (const double* t2 = e.blk(ATB_OPT_T2)) add_t(r, t2);
+}
+
+/* ---------------- pass methods ------------------------------------------- */
+
+/* StrMPoleSymplectic4Pass.c:29-109, BndMPoleSymplectic4Pass.c:38-129,
+ * StrMPoleSymplectic4RadPass.c:30-115, BndMPoleSymplectic4RadPass.c:39-128 */
+template <int MO, bool BEND, bool RAD>
+__device__ __forceinline__ void pass_multipole(P6& r, const Rec& e) {
+    const uint32_t fl = e.flags();
+    const double L1 = e.f(ATB_SM_L1), L2 = e.f(ATB_SM_L2);
+    const double K1 = e.f(ATB_SM_K1), K2 = e.f(ATB_SM_K2);
+    const int mo = e.mo();
+    const double* A = e.p + (BEND ? ATB_BM_POLY : ATB_SM_POLY);
+    const double* B = A + mo + 1;
+    Poly<MO> pl;
+    pl.load(A, B, mo);
+
+    if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_SM_SCALE));
+    double nl1 = 0.0, nl2 = 0.0;
+    if (!RAD) {
+        double p_norm = 1.0 / (1.0 + r.dp);
+        nl1 = L1 * p_norm;
+        nl2 = L2 * p_norm;
+    }
+    entrance_misalign(r, e);
+    apertures(r, e);
+    double irho = 0.0, k1i = 0.0, k2i = 0.0;
+    if (BEND) {
+        irho = e.f(ATB_BM_IRHO);
+        k1i = e.f(ATB_BM_K1IRHO);
+        k2i = e.f(ATB_BM_K2IRHO);
+        const int m_in = (int)((fl >> ATB_F_BM_IN_SHIFT) & ATB_F_BM_MASK);
+        if (RAD)
+            edge_fringe_rad<kFast>(r, irho, e.f(ATB_BM_EIN), e.f(ATB_BM_FCIN), e.f(ATB_BM_FXIN),
+                                   e.f(ATB_BM_FYIN), m_in, fl & ATB_F_FC0_IN, 1.0);
+        else
+            edge_fringe<kFast>(r, irho, e.f(ATB_BM_EIN), e.f(ATB_BM_FCIN), e.f(ATB_BM_FXIN),
+                               e.f(ATB_BM_FYIN), m_in, fl & ATB_F_FC0_IN, 1.0);
+    }
+    if (fl & ATB_F_FQ_IN) {
+        const double b1 = e.f(ATB_SM_B1);
+        if (fl & ATB_F_FQ_IN_LIN) {
+            const double* fm = e.blk(ATB_OPT_FRINGE);
+            lin_fringe_map(r, fm);
+            quad_fringe<kFast>(r, b1, true);
+            lin_fringe_map(r, fm + 8);
+        } else {
+            quad_fringe<kFast>(r, b1, true);
+        }
+    }
+    const int ns = e.nsteps();
+    if (RAD) {
+        const double radc = e.f(ATB_SM_RADC);
+        double pn = kFast ? 1.0 / (1.0 + r.dp) : 0.0;
+        for (int m = 0; m < ns; ++m) {
+            diff_drift<kFast>(r, L1, pn);
+            if (BEND) bnd_kick_rad<kFast>(r, pl, K1, irho, k1i, radc, pn);
+            else str_kick_rad<kFast>(r, pl, K1, radc, pn);
+            diff_drift<kFast>(r, L2, pn);
+            if (BEND) bnd_kick_rad<kFast>(r, pl, K2, irho, k2i, radc, pn);
+            else str_kick_rad<kFast>(r, pl, K2, radc, pn);
+            diff_drift<kFast>(r, L2, pn);
+            if (BEND) bnd_kick_rad<kFast>(r, pl, K1, irho, k1i, radc, pn);
+            else str_kick_rad<kFast>(r, pl, K1, radc, pn);
+            diff_drift<kFast>(r, L1, pn);
+        }
+    } else {
+        double c1 = 0.0, c2 = 0.0;
+        if (kFast) {
+            double h = 0.5 / (1.0 + r.dp);
+            c1 = nl1 * h;
+            c2 = nl2 * h;
+        }
+        for (int m = 0; m < ns; ++m) {
+            fastdrift<kFast>(r, nl1, c1);
+            if (BEND) bndthinkick(r, pl, K1, irho, k1i); else strthinkick(r, pl, K1);
+            fastdrift<kFast>(r, nl2, c2);
+            if (BEND) bndthinkick(r, pl, K2, irho, k2i); else strthinkick(r, pl, K2);
+            fastdrift<kFast>(r, nl2, c2);
+            if (BEND) bndthinkick(r, pl, K1, irho, k1i); else strthinkick(r, pl, K1);
+            fastdrift<kFast>(r, nl1, c1);
+        }
+    }
+    if (fl & ATB_F_FQ_OUT) {
+        const double b1 = e.f(ATB_SM_B1);
+        if (fl & ATB_F_FQ_OUT_LIN) {
+            const double* fm = e.blk(ATB_OPT_FRINGE);
+            lin_fringe_map(r, fm + 16);
+            quad_fringe<kFast>(r, b1, false);
+            lin_fringe_map(r, fm + 24);
+        } else {
+            quad_fringe<kFast>(r, b1, false);
+        }
+    }
+    if (BEND) {
+        const int m_out = (int)((fl >> ATB_F_BM_OUT_SHIFT) & ATB_F_BM_MASK);
+        if (RAD)
+            edge_fringe_rad<kFast>(r, irho, e.f(ATB_BM_EOUT), e.f(ATB_BM_FCOUT), e.f(ATB_BM_FXOUT),
+                                   e.f(ATB_BM_FYOUT), m_out, fl & ATB_F_FC0_OUT, -1.0);
+        else
+            edge_fringe<kFast>(r, irho, e.f(ATB_BM_EOUT), e.f(ATB_BM_FCOUT), e.f(ATB_BM_FXOUT),
+                               e.f(ATB_BM_FYOUT), m_out, fl & ATB_F_FC0_OUT, -1.0);
+    }
+    apertures(r, e);
+    exit_misalign(r, e);
+    if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_SM_ISCALE));
+}
+
+template <bool BEND, bool RAD>
+__device__ __forceinline__ void pass_multipole_dispatch(P6& r, const Rec& e) {
+    switch (e.mo()) {
+        case 0: pass_multipole<0, BEND, RAD>(r, e); break;
+        case 1: pass_multipole<1, BEND, RAD>(r, e); break;
+        case 2: pass_multipole<2, BEND, RAD>(r, e); break;
+        case 3: pass_multipole<3, BEND, RAD>(r, e); break;
+        default: pass_multipole<-1, BEND, RAD>(r, e); break;
+    }
+}
+
+/* DriftPass.c:16-48 */
+__device__ __forceinline__ void pass_drift(P6& r, const Rec& e) {
+    entrance_misalign(r, e);
+    apertures(r, e);
+    drift6<kFast>(r, e.f(ATB_DR_LE));
+    apertures(r, e);
+    exit_misalign(r, e);
+}
+
+/* IdentityPass.c:20-43 */
+__device__ __forceinline__ void pass_identity(P6& r, const Rec& e) {
+    entrance_misalign(r, e);
+    apertures(r, e);
+    exit_misalign(r, e);
+}
+
+/* ThinMPolePass.c:28-70 */
+__device__ __forceinline__ void pass_thinmpole(P6& r, const Rec& e) {
+    const uint32_t fl = e.flags();
+    const int mo = e.mo();
+    const double* A = e.p + ATB_TM_POLY;
+    const double* B = A + mo + 1;
+    Poly<-1> pl;
+    pl.load(A, B, mo);
+    const double bax = e.f(ATB_TM_BAX), bay = e.f(ATB_TM_BAY);
+    if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_TM_SCALE));
+    entrance_misalign(r, e);
+    apertures(r, e);
+    strthinkick(r, pl, 1.0);
+    r.px += bax * r.dp;
+    r.py -= bay * r.dp;
+    r.ct -= bax * r.x - bay * r.y;
+    exit_misalign(r, e);
+    if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_TM_ISCALE));
+}
+
+/* RFCavityPass.c:23-68 -> attrackfunc.c:5-42 (trackRFCavity) */
+__device__ __forceinline__ void rf_kick(P6& r, const Rec& e, int nturn) {
+    const double nv = e.f(ATB_RF_NV), tf = e.f(ATB_RF_TF), lag = e.f(ATB_RF_LAG);
+    const double ht = e.f(ATB_RF_HT), phi = e.f(ATB_RF_PHI);
+    r.dp += -nv * sin(tf * ((r.ct - lag) / ATB_C0 - ht * (double)nturn) - phi);
+}
+
+__device__ __forceinline__ void pass_rfcavity(P6& r, const Rec& e, int nturn) {
+    const uint32_t fl = e.flags();
+    if (!(fl & ATB_F_THICK)) {
+        if (fl & ATB_F_NV) rf_kick(r, e, nturn);
+    } else {
+        const double half = e.f(ATB_RF_HALF);
+        drift6<kFast>(r, half);
+        if (fl & ATB_F_NV) rf_kick(r, e, nturn);
+        drift6<kFast>(r, half);
+    }
+}
+
+/* CorrectorPass.c:25-90 */
+__device__ __forceinline__ void pass_corrector(P6& r, const Rec& e) {
+    const uint32_t fl = e.flags();
+    const double xk = e.f(ATB_CO_XK), yk = e.f(ATB_CO_YK);
+    if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_CO_SCALE));
+    if (!(fl & ATB_F_THICK)) {
+        entrance_misalign(r, e);
+        apertures(r, e);
+        r.px += xk;
+        r.py += yk;
+    } else {
+        const double le = e.f(ATB_CO_LE);
+        double p_norm = 1.0 / (1.0 + r.dp);
+        double nl = le * p_norm;
+        entrance_misalign(r, e);
+        apertures(r, e);
+        r.ct += nl * p_norm * (e.f(ATB_CO_K2) + r.px * r.px + r.py * r.py + r.px * xk + r.py * yk) / 2;
+        r.x += nl * (r.px + e.f(ATB_CO_HX));
+        r.px += xk;
+        r.y += nl * (r.py + e.f(ATB_CO_HY));
+        r.py += yk;
+        apertures(r, e);
+    }
+    exit_misalign(r, e);
+    if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_CO_ISCALE));
+}
+
+/* One element on one particle; lost particles (x is NaN) are skipped as every
+ * reference pass method does (e.g. StrMPoleSymplectic4Pass.c:59). */
+__device__ __forceinline__ void track_element(P6& r, const Rec& e, int nturn) {
+    if (isnan(r.x)) return;
+    switch (e.op()) {
+        case ATB_OP_IDENTITY: pass_identity(r, e); break;
+        case ATB_OP_DRIFT: pass_drift(r, e); break;
+        case ATB_OP_STRMPOLE: pass_multipole_dispatch<false, false>(r, e); break;
+        case ATB_OP_STRMPOLE_RAD: pass_multipole_dispatch<false, true>(r, e); break;
+        case ATB_OP_BNDMPOLE: pass_multipole_dispatch<true, false>(r, e); break;
+        case ATB_OP_BNDMPOLE_RAD: pass_multipole_dispatch<true, true>(r, e); break;
+        case ATB_OP_THINMPOLE: pass_thinmpole(r, e); break;
+        case ATB_OP_RFCAVITY: pass_rfcavity(r, e, nturn); break;
+        case ATB_OP_CORRECTOR: pass_corrector(r, e); break;
+        case ATB_OP_APERTURE: check_rect(r, e.p + ATB_AP_LIM); break;
+        default: break;
+    }
+}
+
+/* pyat/at.c:123: lost if any coordinate is non-finite or |r_n| > 1, n < 5 */
+__device__ __forceinline__ bool is_bad(const P6& r) {
+    return !all_finite(r) || fabs(r.x) > 1.0 || fabs(r.px) > 1.0 || fabs(r.y) > 1.0 ||
+           fabs(r.py) > 1.0 || fabs(r.dp) > 1.0;
+}
+
+__device__ __forceinline__ void load6(const double* src, P6& r) {
+    const double2* s = reinterpret_cast<const double2*>(src);
+    double2 a = s[0], b = s[1], c = s[2];
+    r.x = a.x; r.px = a.y; r.y = b.x; r.py = b.y; r.dp = c.x; r.ct = c.y;
+}
+
+__device__ __forceinline__ void store6(double* dst, const P6& r) {
+    double2* d = reinterpret_cast<double2*>(dst);
+    d[0] = make_double2(r.x, r.px);
+    d[1] = make_double2(r.y, r.py);
+    d[2] = make_double2(r.dp, r.ct);
+}
+
+/* segment index of the q-th segment visited by this launch */
+__device__ __forceinline__ int seg_at(const AtbJob& J, long long q) {
+    if (q < J.nseg_first) return J.seg_first0 + (int)q;
+    return (int)((q - J.nseg_first) % J.nseg_turn);
+}
+
+/* ---------------- the kernel --------------------------------------------- */
+
+extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
+ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
+                                       const AtbTile* __restrict__ tiles, int ntiles,
+                                       int* __restrict__ tile_counter,
+                                       int* __restrict__ status, int smem_cap_words) {
+    extern __shared__ __align__(128) double smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ int s_tile;
+    double* buf0 = smem;
+    double* buf1 = smem + smem_cap_words;
+    uint32_t use_count[2] = {0u, 0u};
+    const int tid = threadIdx.x;
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    int resident_job = -1;   /* job whose whole table sits in buf0 */
+
+    while (true) {
+        if (tid == 0) s_tile = atomicAdd(tile_counter, 1);
+        __syncthreads();
+        const int t = s_tile;
+        __syncthreads();
+        if (t >= ntiles) break;
+        const AtbTile tile = tiles[t];
+        const AtbJob& J = jobs[tile.job];
+        const long long p = tile.first + tid;
+        const bool active = (tid < tile.count);
+        const bool resident = (J.resident != 0);
+
+        P6 r;
+        bool lost = false;
+        if (active) {
+            load6(J.r + 6 * p, r);
+            if (J.losses) lost = J.lost[p] != 0;
+        } else {
+            r.x = nan_d(); r.px = r.py = r.y = r.dp = r.ct = 0.0;
+            lost = true;
+        }
+
+        /* staging pipeline state for this tile */
+        const long long nq = (J.nturns <= 0) ? 0
+                             : (long long)J.nseg_first + (long long)(J.nturns - 1) * J.nseg_turn;
+        bool timed_out = false;
+        if (resident) {
+            if (resident_job != tile.job) {
+                if (tid == 0) {
+                    const uint32_t bytes = (uint32_t)(J.segs[0].nwords * 8);
+                    mbar_expect_tx(&bars[0], bytes);
+                    bulk_g2s(buf0, J.table + J.segs[0].word0, bytes, &bars[0]);
+                }
+                bool ok = mbar_wait_bounded(&bars[0], use_count[0] & 1u);
+                use_count[0]++;
+                timed_out = __syncthreads_or(!ok);
+                resident_job = tile.job;
+            }
+        } else {
+            resident_job = -1;
+            if (tid == 0) {
+                for (int b = 0; b < 2 && b < nq; ++b) {
+                    const AtbSeg sg = J.segs[seg_at(J, b)];
+                    const uint32_t bytes = (uint32_t)(sg.nwords * 8);
+                    mbar_expect_tx(&bars[b], bytes);
+                    bulk_g2s(b ? buf1 : buf0, J.table + sg.word0, bytes, &bars[b]);
+                }
+            }
+        }
+        if (timed_out) {
+            if (tid == 0) atomicOr(status, ATB_STATUS_WAIT_TIMEOUT);
+            break;
+        }
+
+        long long slot = J.rout_slot0;
+        long long q = 0;
+        for (int tt = 0; tt < J.nturns && !timed_out; ++tt) {
+            const int nturn = J.turn0 + tt;
+            const int estart = (tt == 0) ? J.start_elem : 0;
+            const int eend = J.end_elem;
+            int nri = 0;
+            unsigned nextref = (nri < J.nref) ? J.refpts[nri++] : 0xffffffffu;
+            const int nseg_this = (tt == 0) ? J.nseg_first : J.nseg_turn;
+            for (int si = 0; si < nseg_this; ++si, ++q) {
+                const int b = resident ? 0 : (int)(q & 1);
+                const AtbSeg sg = J.segs[resident ? 0 : seg_at(J, q)];
+                const double* base = b ? buf1 : buf0;
+                if (!resident) {
+                    bool ok = mbar_wait_bounded(&bars[b], use_count[b] & 1u);
+                    use_count[b]++;
+                    if (__syncthreads_or(!ok)) { timed_out = true; break; }
+                }
+                /* elements of this segment */
+                int e_lo = resident ? estart : sg.first_elem;
+                int e_hi = resident ? eend : sg.first_elem + sg.nelem;
+                if (e_lo < estart) e_lo = estart;
+                if (e_hi > eend) e_hi = eend;
+                int w = 0;
+                if (resident) {
+                    w = J.elem_off[e_lo] - J.elem_off[0];
+                } else {
+                    w = J.elem_off[e_lo] - J.elem_off[sg.first_elem];
+                }
+                for (int ei = e_lo; ei < e_hi; ++ei) {
+                    Rec e;
+                    e.p = base + w;
+                    const uint64_t* hp = reinterpret_cast<const uint64_t*>(e.p);
+                    e.hdr = hp[0];
+                    e.opt = hp[1];
+                    if ((unsigned)ei == nextref) {
+                        if (active) store6(J.rout + 6 * (p + J.np * slot), r);
+                        ++slot;
+                        nextref = (nri < J.nref) ? J.refpts[nri++] : 0xffffffffu;
+                    }
+                    track_element(r, e, nturn);
+                    if (J.check_loss) {
+                        if (J.losses) {
+                            if (!lost && is_bad(r)) {
+                                lost = true;
+                                if (active) {
+                                    J.lturn[p] = (unsigned)nturn;
+                                    J.lelem[p] = (unsigned)ei;
+                                    store6(J.lcoord + 6 * p, r);
+                                }
+                                r.x = nan_d(); r.px = 0.0; r.y = 0.0; r.py = 0.0; r.dp = 0.0; r.ct = 0.0;
+                            }
+                        } else if (isfinite(r.x) && is_bad(r)) {
+                            r.x = nan_d(); r.px = 0.0; r.y = 0.0; r.py = 0.0; r.dp = 0.0; r.ct = 0.0;
+                        }
+                    }
+                    w += e.len();
+                }
+                if (!resident) {
+                    __syncthreads();   /* every thread is done with buffer b */
+                    if (tid == 0 && q + 2 < nq) {
+                        const AtbSeg nx = J.segs[seg_at(J, q + 2)];
+                        const uint32_t bytes = (uint32_t)(nx.nwords * 8);
+                        mbar_expect_tx(&bars[b], bytes);
+                        bulk_g2s(b ? buf1 : buf0, J.table + nx.word0, bytes, &bars[b]);
+                    }
+                }
+            }
+            if (timed_out) break;
+            if ((unsigned)J.nelem == nextref) {
+                if (active) store6(J.rout + 6 * (p + J.np * slot), r);
+                ++slot;
+            }
+            if (J.alive) {
+                /* per-turn survivors and first/second moments: warp ballot
+                 * and shuffle reductions, one atomic per warp */
+                const bool alive = active && !isnan(r.x) && !(J.losses && lost);
+                const unsigned m = __ballot_sync(0xffffffffu, alive);
+                double v[12];
+                v[0] = alive ? r.x : 0.0; v[1] = alive ? r.px : 0.0; v[2] = alive ? r.y : 0.0;
+                v[3] = alive ? r.py : 0.0; v[4] = alive ? r.dp : 0.0; v[5] = alive ? r.ct : 0.0;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) v[6 + k] = v[k] * v[k];
+#pragma unroll
+                for (int k = 0; k < 12; ++k) {
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+                }
+                if ((tid & 31) == 0) {
+                    atomicAdd(&J.alive[tt], (unsigned)__popc(m));
+                    if (J.moments) {
+#pragma unroll
+                        for (int k = 0; k < 12; ++k) atomicAdd(&J.moments[12 * tt + k], v[k]);
+                    }
+                }
+            }
+        }
+        if (timed_out) {
+            /* drain our own copies still in flight before leaving */
+            if (!resident) {
+                for (int b = 0; b < 2; ++b) {
+                    if (use_count[b] < (uint32_t)((nq + 1 - b) / 2)) {
+                        mbar_wait_bounded(&bars[b], use_count[b] & 1u);
+                    }
+                }
+            }
+            if (tid == 0) atomicOr(status, ATB_STATUS_WAIT_TIMEOUT);
+            break;
+        }
+        if (active) {
+            store6(J.r + 6 * p, r);
+            if (J.losses) J.lost[p] = lost ? 1 : 0;
+        }
+        /* all threads must be past the last segment before the buffers are
+           re-filled by the next tile */
+        __syncthreads();
+    }
+}
+
+}  // namespace atb
+
+#endif  // ATB_TRACK_KERNEL_CUH

@@ -1,0 +1,156 @@
+"""Per-device engine objects over the C ABI (include/atb200.h)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib, ptr
+from .lattice import CompiledLattice
+
+_engines: dict[int, "Engine"] = {}
+_elock = threading.Lock()
+
+
+def default_mode() -> int:
+    m = os.environ.get("AT_B200_MODE", "fast").lower()
+    if m not in ("fast", "exact"):
+        raise ValueError("AT_B200_MODE must be 'fast' or 'exact'")
+    return _lib.MODE_FAST if m == "fast" else _lib.MODE_EXACT
+
+
+def mode_code(mode) -> int:
+    if mode is None:
+        return default_mode()
+    if isinstance(mode, str):
+        if mode not in ("fast", "exact"):
+            raise ValueError("mode must be 'fast' or 'exact'")
+        return _lib.MODE_FAST if mode == "fast" else _lib.MODE_EXACT
+    return int(mode)
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    rc = lib().atb_device_count(C.byref(n))
+    return n.value if rc == 0 else 0
+
+
+def device_info(dev: int):
+    name = C.create_string_buffer(256)
+    ma, mi, sm = C.c_int(), C.c_int(), C.c_int()
+    mem = C.c_uint64()
+    check(lib().atb_device_info(dev, name, 256, C.byref(ma), C.byref(mi), C.byref(sm), C.byref(mem)))
+    return name.value.decode(), ma.value, mi.value, sm.value, mem.value
+
+
+class Engine:
+    """One CUDA engine (handle, stream, buffers) bound to a device."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().atb_create(int(device), C.byref(h)))
+        self.h = h
+        self.device = int(device)
+        self.lock = threading.Lock()
+
+    @classmethod
+    def get(cls, device: int = 0) -> "Engine":
+        with _elock:
+            e = _engines.get(device)
+            if e is None:
+                e = cls(device)
+                _engines[device] = e
+            return e
+
+    def close(self):
+        if self.h:
+            lib().atb_destroy(self.h)
+            self.h = None
+
+    # -- launch tuning ------------------------------------------------------
+    def set_launch(self, threads: int = 0, seg_cap_words: int = 0, resident_max_words: int = 0,
+                   rout_budget_bytes: int = 0):
+        check(lib().atb_set_launch(self.h, int(threads), int(seg_cap_words),
+                                   int(resident_max_words), int(rout_budget_bytes)))
+
+    # -- lattices -----------------------------------------------------------
+    def upload(self, cl: CompiledLattice) -> int:
+        lid = C.c_int32(-1)
+        words = np.ascontiguousarray(cl.words, dtype=np.float64)
+        off = np.ascontiguousarray(cl.offsets, dtype=np.uint32)
+        check(lib().atb_lattice_upload(self.h, ptr(words) if words.size else None,
+                                       int(words.size), ptr(off), int(cl.nelem), C.byref(lid)))
+        return lid.value
+
+    def update(self, lid: int, cl: CompiledLattice):
+        words = np.ascontiguousarray(cl.words, dtype=np.float64)
+        check(lib().atb_lattice_update(self.h, int(lid), ptr(words) if words.size else None,
+                                       int(words.size)))
+
+    def free(self, lid: int):
+        check(lib().atb_lattice_free(self.h, int(lid)))
+
+    # -- tracking -----------------------------------------------------------
+    def track(self, lid: int, r: np.ndarray, nturns: int, turn0: int = 0, start_elem: int = 0,
+              end_elem: int = 0, refpts: np.ndarray | None = None, losses: bool = False,
+              stats: bool = False, mode=None, element: bool = False):
+        """Track the (6, N) Fortran-ordered array ``r`` in place.
+
+        Returns ``(rout, loss_dict or None, (alive, moments) or None)``."""
+        npart = r.size // 6
+        nref = 0 if refpts is None else int(refpts.size)
+        rout = np.empty((6, npart, nref, nturns), dtype=np.float64, order="F")
+        ld = None
+        islost = lturn = lelem = lcoord = None
+        if losses:
+            islost = np.zeros(npart, dtype=np.bool_)
+            lturn = np.zeros(npart, dtype=np.uint32)
+            lelem = np.zeros(npart, dtype=np.uint32)
+            lcoord = np.zeros((6, npart), dtype=np.float64, order="F")
+        alive = moments = None
+        if stats:
+            alive = np.zeros(nturns, dtype=np.uint32)
+            moments = np.zeros((nturns, 12), dtype=np.float64)
+        refs = None if refpts is None else np.ascontiguousarray(refpts, dtype=np.uint32)
+        with self.lock:
+            check(lib().atb_track(
+                self.h, int(lid), ptr(r), npart, int(nturns), int(turn0), int(start_elem),
+                int(end_elem), ptr(refs) if nref else None, nref,
+                ptr(rout) if (nref and npart) else None, 1 if losses else 0, ptr(islost),
+                ptr(lturn), ptr(lelem), ptr(lcoord), ptr(alive), ptr(moments), mode_code(mode),
+                _lib.FLAG_ELEMENT if element else 0))
+        if losses:
+            ld = {"islost": islost, "turn": lturn, "elem": lelem, "coord": lcoord}
+        return rout, ld, ((alive, moments) if stats else None)
+
+    def track_device(self, lid: int, r_ptr: int, npart: int, nturns: int, turn0: int = 0,
+                     losses=None, alive_ptr: int | None = None, moments_ptr: int | None = None,
+                     mode=None, stream: int | None = None):
+        """Enqueue tracking of a device-resident (6, N) array (no host copies).
+
+        ``losses`` is ``None`` or a tuple of device pointers
+        (islost, lturn, lelem, lcoord)."""
+        lp = losses if losses is not None else (None, None, None, None)
+        check(lib().atb_track_device(self.h, int(lid), r_ptr, int(npart), int(nturns), int(turn0),
+                                     1 if losses is not None else 0, lp[0], lp[1], lp[2], lp[3],
+                                     alive_ptr, moments_ptr, mode_code(mode), stream))
+
+    def track_batch(self, jobs: list[dict], mode=None, stream: int | None = None):
+        arr = (_lib.AtbJobDesc * len(jobs))()
+        for a, j in zip(arr, jobs):
+            a.lattice_id = j["lattice_id"]
+            a.nturns = j["nturns"]
+            a.turn0 = j.get("turn0", 0)
+            lp = j.get("losses")
+            a.losses = 1 if lp is not None else 0
+            a.r = j["r"]
+            a.np = j["np"]
+            if lp is not None:
+                a.islost, a.lturn, a.lelem, a.lcoord = lp
+        check(lib().atb_track_batch(self.h, arr, len(jobs), mode_code(mode), stream))
+
+    def sync(self, stream: int | None = None):
+        check(lib().atb_sync(self.h, stream))

@@ -1,0 +1,395 @@
+"""Benchmark: particle-turns/s of the FP64 tracking path on B200.
+
+Workload (default): the radiating large ring (``at_b200.rings.large_ring``,
+1954 elements, misaligned, 3 GeV electrons) with a 1,000,000-particle
+Gaussian bunch around its closed orbit per GPU.  One step tracks the bunch
+for ``--turns-per-step`` turns (default 10); the bunch keeps evolving from
+step to step with the absolute turn counter advancing, so K steps are K*T
+consecutive turns of the 10,000-turn run.
+
+Arms:
+  default            this engine.  ``value``: device time (CUDA events on the
+                     launching stream, L2 flushed between steps) with the
+                     particles resident in HBM; ``e2e``: the drop-in call
+                     ``at_b200.gpupass`` on pinned host arrays (host->device
+                     and device->host copies of the bunch and loss map inside
+                     the timed region).
+  --impl reference   the reference's own compiled C engine (pyat/at.c +
+                     atintegrators, built by oracle/build_ref.py) through its
+                     atpass entry, OpenMP over all host cores, on a bounded
+                     sample of the same workload each step.
+
+Multi-GPU (torchrun): one process per GPU, each tracks its own bunch (weak
+scaling, particles are independent: no collective on the data path); the
+step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "particle-turns/s FP64 vs FP64 peak; served p50/p99 latency vs plain drop-in"
+UNIT = "particle-turns/s"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="large", choices=["large", "fodo"])
+    ap.add_argument("--particles", type=int, default=None)
+    ap.add_argument("--turns-per-step", type=int, default=None)
+    ap.add_argument("--mode", default="fast", choices=["fast", "exact"])
+    ap.add_argument("--threads", type=int, default=0, help="threads per block (0: default)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _defaults(a):
+    if a.particles is None:
+        a.particles = 1_000_000 if a.workload == "large" else 10_000
+    if a.turns_per_step is None:
+        a.turns_per_step = 10 if a.workload == "large" else 100
+    return a
+
+
+def _ring(workload):
+    from at_b200 import rings
+    if workload == "large":
+        return rings.large_ring()
+    return rings.fodo_ring()
+
+
+def _bunch(workload, n, seed):
+    from at_b200 import rings
+    if workload == "large":
+        return rings.large_ring_bunch(n, seed=seed)
+    return rings.gaussian(n, seed=seed)
+
+
+def _config(a, ring):
+    return {"workload": "%s ring, %d particles/GPU, %d turns/step" % (
+                "radiating large (1954 elements)" if a.workload == "large" else "FODO (385 elements)",
+                a.particles, a.turns_per_step),
+            "elements": len(ring), "particles_per_gpu": a.particles,
+            "turns_per_step": a.turns_per_step, "arithmetic": a.mode,
+            "losses": True, "l2": "flushed between timed steps",
+            "parallelism": "particle shards, one per GPU"}
+
+
+# --------------------------------------------------------------------------- #
+# reference (CPU) runs                                                         #
+# --------------------------------------------------------------------------- #
+def _ref_sample(workload, particles, turns, threads):
+    """Time the reference engine once in a subprocess; returns the JSON dict."""
+    from oracle import ref_runner
+    if not ref_runner.available():
+        return None
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    cmd = [sys.executable, os.path.join(REPO, "oracle", "ref_runner.py"), workload,
+           "--particles", str(particles), "--turns", str(turns), "--threads", str(threads)]
+    out = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=900)
+    if out.returncode != 0:
+        raise RuntimeError("reference run failed: %s" % out.stderr[-2000:])
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def _port_sample(workload, particles, turns, threads):
+    """The oracle restatement (when the reference build is absent)."""
+    from oracle import oracle
+    ring = _ring(workload)
+    r = _bunch(workload, particles, 0)
+    t0 = time.perf_counter()
+    oracle.track(ring, r, turns, energy=ring.energy, rest_energy=ring.particle.rest_energy,
+                 losses=True, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return {"particle_turns": particles * turns, "seconds": dt, "rate": particles * turns / dt,
+            "threads": threads, "sample": "%d particles x %d turns" % (particles, turns)}
+
+
+def cpu_rate(workload, target_s=15.0, threads=None):
+    """A bounded sample (about target_s of CPU work) of the workload."""
+    threads = threads or os.cpu_count() or 1
+    kind = "reference"
+    fn = _ref_sample
+    from oracle import ref_runner
+    if not ref_runner.available():
+        kind, fn = "port", _port_sample
+    probe = fn(workload, max(64, 8 * threads), 1, threads)
+    n = int(max(64, min(200_000, probe["rate"] * target_s)))
+    res = fn(workload, n, 1, threads)
+    res["kind"] = kind
+    return res
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    ring_len = len(_ring(a.workload))
+    threads = os.cpu_count() or 1
+    kind = "reference"
+    from oracle import ref_runner
+    fn = _ref_sample
+    if not ref_runner.available():
+        kind, fn = "port", _port_sample
+    probe = fn(a.workload, max(64, 8 * threads), 1, threads)
+    # each step: about 10 s of CPU work, so K+W steps stay within minutes
+    n = int(max(64, min(200_000, probe["rate"] * 10.0)))
+    for _ in range(a.warmup):
+        fn(a.workload, max(64, n // 10), 1, threads)
+    rates, secs = [], []
+    for _ in range(a.steps):
+        res = fn(a.workload, n, 1, threads)
+        rates.append(res["rate"])
+        secs.append(res["seconds"])
+    value = a.steps * n / sum(secs)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sum(secs) / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": dict(_config(a, range(ring_len)), sample="%d particles x 1 turn per step" % n),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": "%d particles x 1 turn per step, %d steps" % (n, a.steps)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- #
+# GPU arm                                                                      #
+# --------------------------------------------------------------------------- #
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def run_b200(a):
+    import torch
+    import torch.distributed as dist
+
+    from at_b200 import _lib, flops
+    from at_b200.engine import Engine
+    from at_b200.lattice import compile_lattice
+    from at_b200 import tracking
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+
+    ring = _ring(a.workload)
+    cl = compile_lattice(ring, ring.energy, ring.particle.rest_energy)
+    fpt, ntrans = flops.flops_per_particle_turn(cl)
+    eng = Engine.get(local)
+    if a.threads:
+        eng.set_launch(threads=a.threads)
+    lid = eng.upload(cl)
+    mode = a.mode
+    N, T = a.particles, a.turns_per_step
+
+    # FP64 peak of this GPU, measured live
+    import ctypes as C
+    pk, pks = C.c_double(), C.c_double()
+    _lib.check(_lib.lib().atb_fp64_peak(local, C.byref(pk), C.byref(pks)))
+    fp64_peak = pk.value
+
+    # particles resident in HBM: (6, N) Fortran order == torch (N, 6) row-major
+    r0 = _bunch(a.workload, N, seed=rank)
+    rd = torch.from_numpy(np.ascontiguousarray(r0.T)).to(dev)
+    lost = torch.zeros(N, dtype=torch.uint8, device=dev)
+    lturn = torch.zeros(N, dtype=torch.int32, device=dev)
+    lelem = torch.zeros(N, dtype=torch.int32, device=dev)
+    lcoord = torch.zeros((N, 6), dtype=torch.float64, device=dev)
+    alive = torch.zeros(T, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+    lp = (lost.data_ptr(), lturn.data_ptr(), lelem.data_ptr(), lcoord.data_ptr())
+
+    def step(turn0, with_alive):
+        if with_alive:
+            alive.zero_()
+        eng.track_device(lid, rd.data_ptr(), N, T, turn0, losses=lp,
+                         alive_ptr=alive.data_ptr() if with_alive else None, mode=mode,
+                         stream=sptr)
+
+    turn = 0
+    for _ in range(a.warmup):
+        step(turn, False)
+        turn += T
+    torch.cuda.synchronize()
+    eng.sync(sptr)
+
+    clocks = Clocks(local) if rank == 0 else None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    times = []
+    survivors = 0
+    for _ in range(a.steps):
+        flush.fill_(1.0)                      # evict the particle state from L2
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step(turn, True)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) * 1e-3)
+        survivors += int(alive.sum().item())
+        turn += T
+    torch.cuda.synchronize()
+    eng.sync(sptr)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+    tot = torch.tensor([sum(times)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    t_max = float(tot.item())
+    value = world * N * T * a.steps / t_max
+    # roofline of the tracking kernel: algorithmic flops of the particle-turns
+    # actually tracked (survivors per turn) over its event-timed duration
+    achieved = fpt * survivors / sum(times) / 1e12
+
+    # end to end through the drop-in entry point on pinned host buffers
+    e2e = None
+    if not a.no_e2e:
+        hb = torch.empty((N, 6), dtype=torch.float64).pin_memory()
+        hb.copy_(torch.from_numpy(np.ascontiguousarray(r0.T)))
+        rh = hb.numpy().T                      # (6, N) Fortran view, pinned
+        assert rh.flags.f_contiguous
+        line = list(ring)
+        line_obj = type(ring)(line, energy=ring.energy, particle=ring.particle)
+        tracking.gpupass(line_obj, rh, 1, losses=True, mode=mode, gpu_pool=[local])
+        etimes = []
+        if world > 1:
+            dist.barrier()
+        for k in range(a.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            tracking.gpupass(line_obj, rh, T, losses=True, reuse=True, keep_counter=True,
+                             mode=mode, gpu_pool=[local])
+            etimes.append(time.perf_counter() - t0)
+        et = torch.tensor([sum(etimes)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * N * T * a.steps / float(et.item()), "unit": UNIT,
+               "h2d_bytes_per_step": N * 48,
+               "d2h_bytes_per_step": N * 48 + N * (1 + 4 + 4 + 48),
+               "api": "at_b200.gpupass (reference gpupass/atpass signature), pinned host arrays"}
+
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline:
+        try:
+            c = cpu_rate(a.workload)
+            cpu = {"value": c["rate"], "unit": UNIT, "cores": c["threads"], "kind": c["kind"],
+                   "sample": c["sample"] + " of the same workload, OpenMP over all host cores"}
+        except Exception as exc:  # noqa: BLE001
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": "failed: %s" % str(exc)[:200]}
+
+    traffic = None
+    prof = os.path.join(REPO, "profiles", "traffic_%s.json" % a.workload)
+    if os.path.exists(prof):
+        with open(prof) as f:
+            tp = json.load(f)
+        traffic = tp.get("bytes_per_particle_turn", 0.0) * N * T
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * t_max / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded lattice and Gaussian bunch)",
+            "config": _config(a, ring),
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic,
+                         "peak_source": "measured live: atb_fp64_peak DFMA chains on this GPU",
+                         "flops_per_particle_turn": fpt, "survivor_particle_turns": survivors},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = _defaults(_args())
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_b200(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,144 @@
+/*
+ * atb200 -- C ABI of the B200 particle-tracking engine.
+ *
+ * Plain C types only (pointers, sizes, status codes); no Python, NumPy or
+ * torch types cross this boundary.  Every entry point returns ATB_OK (0) or a
+ * negative ATB_ERR_* code and never aborts; atb_last_error() gives the
+ * message of the calling thread's last failure.
+ *
+ * What each entry point replaces in the reference (atcollab/at):
+ *   atb_lattice_upload   the lattice cache that pyat/at.c builds on a
+ *                        non-reuse call (pyat/at.c:445-512) and the per-element
+ *                        `struct elem` set-up of every trackFunction
+ *                        (atintegrators/atelem.c:373-374, e.g.
+ *                        StrMPoleSymplectic4Pass.c:112-166): the host compiles
+ *                        the elements into one flat table (atb_table.h) and
+ *                        this call makes it device-resident.
+ *   atb_track            at_atpass (pyat/at.c:340-681) / at_gpupass
+ *                        (atgpu/PyInterface.cpp:132-402): multi-turn tracking
+ *                        of a 6xN Fortran-ordered particle array, in place,
+ *                        with refpts snapshots (6,N,R,T) and the loss map.
+ *                        With ATB_FLAG_ELEMENT it is at_elempass
+ *                        (pyat/at.c:683-753): one pass, no loss marking.
+ *   atb_device_count /   at_gpuinfo (atgpu/PyInterface.cpp:95-129).
+ *   atb_device_info
+ */
+#ifndef ATB200_H
+#define ATB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ATB_OK 0
+#define ATB_ERR_ARG (-1)      /* invalid argument                          */
+#define ATB_ERR_CUDA (-2)     /* CUDA runtime error                        */
+#define ATB_ERR_TIMEOUT (-3)  /* a bounded in-kernel wait gave up          */
+#define ATB_ERR_NOMEM (-4)    /* device memory budget exceeded             */
+#define ATB_ERR_NOLAT (-5)    /* unknown lattice id                        */
+
+#define ATB_MODE_EXACT 0      /* reference operation order, no FMA         */
+#define ATB_MODE_FAST 1       /* FMA + reciprocal reuse (default)          */
+
+#define ATB_FLAG_ELEMENT 1    /* single-element pass: no loss marking      */
+
+typedef struct atb_handle atb_handle;
+
+/* One job of a batched launch (lattice variant x particle set). Device
+ * pointers.  rout/refpts are not supported in batches. */
+typedef struct atb_job_desc {
+    int32_t lattice_id;
+    int32_t nturns;
+    int32_t turn0;
+    int32_t losses;
+    double* r;            /* (6, np) Fortran order, device                */
+    int64_t np;
+    uint8_t* islost;      /* device, np (losses == 1)                      */
+    uint32_t* lturn;
+    uint32_t* lelem;
+    double* lcoord;       /* device, 6*np                                  */
+} atb_job_desc;
+
+/* library version (major*10000 + minor*100 + patch) */
+int atb_version(void);
+
+/* message of the calling thread's last failing call ("" if none) */
+const char* atb_last_error(void);
+
+/* at_gpuinfo (atgpu/PyInterface.cpp:95-129): device count and properties */
+int atb_device_count(int* count);
+int atb_device_info(int device, char* name, int name_len, int* cc_major, int* cc_minor,
+                    int* sm_count, uint64_t* total_mem);
+
+/* An engine bound to one device, with its own stream and buffers.  Not
+ * re-entrant: one host thread at a time per handle (the reference's atpass
+ * keeps static state too, pyat/at.c:62-75). */
+int atb_create(int device, atb_handle** out);
+int atb_destroy(atb_handle* h);
+
+/* Launch tuning: threads per block (32..512, multiple of 32), shared-memory
+ * segment capacity in 8-byte words, largest table kept resident in shared
+ * memory, and the device-memory budget for refpts snapshots.  0 keeps the
+ * current value. */
+int atb_set_launch(atb_handle* h, int threads_per_block, int seg_cap_words,
+                   int resident_max_words, int64_t rout_budget_bytes);
+
+/* Make a compiled lattice (flat table of atb_table.h: `nwords` words, element
+ * i at words [elem_off[i], elem_off[i+1])) device-resident.  Replaces the
+ * reference's lattice cache (pyat/at.c:445-512). */
+int atb_lattice_upload(atb_handle* h, const double* words, int64_t nwords,
+                       const uint32_t* elem_off, int32_t nelem, int32_t* lattice_id);
+
+/* Overwrite the words of an uploaded lattice (same layout), e.g. after the
+ * energy-dependent fields were refreshed for a new ring energy. */
+int atb_lattice_update(atb_handle* h, int32_t lattice_id, const double* words, int64_t nwords);
+
+int atb_lattice_free(atb_handle* h, int32_t lattice_id);
+
+/* at_atpass / at_gpupass.  All pointers are HOST memory:
+ *   rin     (6, np) Fortran order, updated in place (pyat/at.c:555,633)
+ *   refpts  nref uint32 element indices (sorted, as get_uint32_index gives)
+ *   rout    (6, np, nref, nturns) Fortran order, or NULL when nref == 0
+ *   losses  1: fill islost/lturn/lelem/lcoord (pyat/at.c:574-594,664-677)
+ *   alive   optional (nturns) survivors after each turn, or NULL
+ *   moments optional (nturns, 12): sums of the 6 coordinates and of their
+ *           squares over survivors after each turn, or NULL
+ * turn0 is the reference's param.nturn at the first turn (the `turn` or kept
+ * counter, pyat/at.c:428-431); start_elem/end_elem as pyat/at.c:514-536.
+ * Blocks until the results are back in host memory. */
+int atb_track(atb_handle* h, int32_t lattice_id, double* rin, int64_t np, int32_t nturns,
+              int32_t turn0, int32_t start_elem, int32_t end_elem, const uint32_t* refpts,
+              int32_t nref, double* rout, int32_t losses, uint8_t* islost, uint32_t* lturn,
+              uint32_t* lelem, double* lcoord, uint32_t* alive, double* moments, int32_t mode,
+              int32_t flags);
+
+/* The same with DEVICE pointers (particles already resident in HBM), enqueued
+ * on `stream` (NULL: the handle's stream) without host synchronisation; no
+ * refpts.  Kernel status is reported by the next atb_sync(). */
+int atb_track_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np, int32_t nturns,
+                     int32_t turn0, int32_t losses, uint8_t* islost, uint32_t* lturn,
+                     uint32_t* lelem, double* lcoord, uint32_t* alive, double* moments,
+                     int32_t mode, void* stream);
+
+/* Many lattice variants and particle sets in one persistent launch (device
+ * pointers); the tiles of the longest jobs are scheduled first. */
+int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,
+                    void* stream);
+
+/* Measurement helper with no counterpart in the reference: the FP64 FMA
+ * throughput of `device` (TFLOP/s, one FMA = 2 flops) from independent DFMA
+ * chains in registers, the denominator of the tracking kernel's roofline. */
+int atb_fp64_peak(int device, double* tflops, double* seconds);
+
+/* Wait for all work enqueued by this handle and return the kernels' status
+ * (ATB_ERR_TIMEOUT if a bounded wait gave up). */
+int atb_sync(atb_handle* h, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ATB200_H */

@@ -1,0 +1,579 @@
+/*
+ * ORACLE -- test infrastructure only.
+ *
+ * A plain-C restatement of the reference tracking path (atcollab/at: the
+ * pyat/at.c turn/element engine and the atintegrators pass methods on the
+ * accelerated path), used as the checker of the CUDA engine in tests/ and as
+ * the "port" CPU baseline.  It is never linked into the product.
+ *
+ * Every function names the reference routine it restates.  Arithmetic keeps
+ * the reference's expression trees and evaluation order and is compiled with
+ * -ffp-contract=off, so on the +,-,*,/ path it is bit-identical to the
+ * reference C build (checked against oracle/_ref and the golden fixtures).
+ * Particles are independent, so the loop runs particle-outermost (one OpenMP
+ * iteration per particle through all turns); the per-particle sequence of
+ * operations is the reference's element-by-element sequence.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* pass methods (must match oracle.py) */
+enum {
+    O_IDENTITY = 0, O_DRIFT, O_STRMPOLE, O_STRMPOLE_RAD, O_BNDMPOLE, O_BNDMPOLE_RAD,
+    O_THINMPOLE, O_RFCAVITY, O_CORRECTOR, O_APERTURE
+};
+
+typedef struct {
+    int32_t pass;
+    int32_t MaxOrder;
+    int32_t NumIntSteps;
+    int32_t FringeBendEntrance;
+    int32_t FringeBendExit;
+    int32_t FringeQuadEntrance;
+    int32_t FringeQuadExit;
+    int32_t pad;
+    double Length, BendingAngle, EntranceAngle, ExitAngle;
+    double FringeInt1, FringeInt2, FullGap, Scaling;
+    double Voltage, Frequency, TimeLag, PhaseLag;
+    double bax, bay;
+    const double *PolynomA, *PolynomB, *fringeIntM0, *fringeIntP0;
+    const double *R1, *R2, *T1, *T2, *RApertures, *EApertures, *KickAngle, *Limits;
+} OElem;
+
+/* ---- constants: atintegrators/atconstants.h:16-31, pyat/at.c:52-53 ----- */
+#define O_PI 3.14159265358979323846
+#define O_THIRD_ROOT_2 1.25992104989487316477
+static const double O_TWOPI = 2.0 * O_PI;
+static const double O_DRIFT1 = 1.0 / (2.0 * (2.0 - O_THIRD_ROOT_2));
+static const double O_DRIFT2 = 0.5 - (1.0 / (2.0 * (2.0 - O_THIRD_ROOT_2)));
+static const double O_KICK1 = 1.0 / (2.0 - O_THIRD_ROOT_2);
+static const double O_KICK2 = 1.0 - 2.0 / (2.0 - O_THIRD_ROOT_2);
+static const double O_C0 = 2.99792458e8;
+#define O_RE 2.8179403205e-15
+#define O_E0 510.99895069e-6
+static const double O_RAD_CONST = 2.0 / 3.0 * O_RE;
+
+/* ---- small vector helpers ---------------------------------------------- */
+
+/* atlalib.c:50-57 */
+static void o_addv(double *r, const double *d) {
+    for (int i = 0; i < 6; i++) r[i] += d[i];
+}
+
+/* atlalib.c:17-32: column-major 6x6 times vector, accumulated from 0 */
+static void o_mulmv(double *r, const double *m) {
+    double out[6];
+    for (int i = 0; i < 6; i++) {
+        double acc = 0;
+        for (int j = 0; j < 6; j++) acc += m[i + j * 6] * r[j];
+        out[i] = acc;
+    }
+    memcpy(r, out, sizeof(out));
+}
+
+/* atlalib.c:169-175 */
+static void o_rect_ap(double *r, const double *lim) {
+    if (r[0] < lim[0] || r[0] > lim[1]) r[5] = INFINITY;
+    else if (r[2] < lim[2] || r[2] > lim[3]) r[5] = INFINITY;
+}
+
+/* atlalib.c:185-190 */
+static void o_ellip_ap(double *r, const double *ax) {
+    double u = r[0] / ax[0];
+    double v = r[2] / ax[1];
+    if ((u * u + v * v) >= 1) r[5] = INFINITY;
+}
+
+/* atlalib.c:70-75 */
+static void o_pref(double *r, double s) {
+    r[1] /= s;
+    r[3] /= s;
+    r[4] = (r[4] + 1.0 - s) / s;
+}
+
+/* atlalib.c:59-68 (== driftkickrad.c drift6 and diff_drift without bdiff) */
+static void o_drift6(double *r, double L) {
+    double pn = 1 / (1 + r[4]);
+    double nl = L * pn;
+    r[0] += nl * r[1];
+    r[2] += nl * r[3];
+    r[5] += nl * pn * (r[1] * r[1] + r[3] * r[3]) / 2;
+}
+
+/* diff_drift.c:30-43 (its literal constants are 1.0 and 2.0) */
+static void o_ddrift(double *r, double L) {
+    double pn = 1.0 / (1.0 + r[4]);
+    double nl = L * pn;
+    r[0] += nl * r[1];
+    r[2] += nl * r[3];
+    r[5] += nl * pn * (r[1] * r[1] + r[3] * r[3]) / 2.0;
+}
+
+/* driftkick.c:37-48 */
+static void o_fastdrift(double *r, double nl) {
+    r[0] += nl * r[1];
+    r[2] += nl * r[3];
+    r[5] += nl * (r[1] * r[1] + r[3] * r[3]) / (2 * (1 + r[4]));
+}
+
+/* the multipole field, highest order first (driftkick.c:92-115 et al.) */
+static void o_field(const double *r, const double *A, const double *B, int n,
+                    double *re, double *im) {
+    double a = B[n], b = A[n];
+    for (int k = n - 1; k >= 0; k--) {
+        double t = a * r[0] - b * r[2] + B[k];
+        b = b * r[0] + a * r[2] + A[k];
+        a = t;
+    }
+    *re = a;
+    *im = b;
+}
+
+/* driftkick.c:92-115 strthinkick */
+static void o_strkick(double *r, const double *A, const double *B, double L, int n) {
+    double re, im;
+    o_field(r, A, B, n, &re, &im);
+    r[1] -= L * re;
+    r[3] += L * im;
+}
+
+/* driftkick.c:51-89 bndthinkick */
+static void o_bndkick(double *r, const double *A, const double *B, double L, double h, int n) {
+    double re, im;
+    o_field(r, A, B, n, &re, &im);
+    r[1] -= L * (re - (r[4] - r[0] * h) * h);
+    r[3] += L * im;
+    r[5] += L * h * r[0];
+}
+
+/* diff_str_kick.c:19-83 (bdiff == NULL) */
+static void o_strkick_rad(double *r, const double *A, const double *B, int n, double L,
+                          double radc) {
+    double re, im;
+    o_field(r, A, B, n, &re, &im);
+    double pn = 1.0 / (1.0 + r[4]);
+    double xp = r[1] * pn, yp = r[3] * pn;
+    double bx = im, by = re;
+    double vn = 1.0 / (1.0 + xp * xp + yp * yp);
+    double b2 = (by * by + bx * bx + (bx * yp - by * xp) * (bx * yp - by * xp)) * vn;
+    double f = (1.0 + (xp * xp + yp * yp) / 2.0) / (pn * pn) * L;
+    r[4] -= radc * b2 * f;
+    pn = 1.0 / (1.0 + r[4]);
+    r[1] = xp / pn;
+    r[3] = yp / pn;
+    r[1] -= L * re;
+    r[3] += L * im;
+}
+
+/* diff_bnd_kick.c:101-174 with its B2perp (:85-99), bdiff == NULL */
+static void o_bndkick_rad(double *r, const double *A, const double *B, int n, double L,
+                          double h, double radc) {
+    double re, im;
+    o_field(r, A, B, n, &re, &im);
+    double pn = 1.0 / (1.0 + r[4]);
+    double x = r[0];
+    double xp = r[1] * pn, yp = r[3] * pn;
+    double bx = im, by = re + h;
+    double vn = 1.0 / ((1.0 + x * h) * (1.0 + x * h) + xp * xp + yp * yp);
+    double b2 = ((by * (1 + x * h)) * (by * (1 + x * h)) + (bx * (1 + x * h)) * (bx * (1 + x * h)) +
+                 (bx * yp - by * xp) * (bx * yp - by * xp)) * vn;
+    double f = (1.0 + x * h + (xp * xp + yp * yp) / 2.0) / (pn * pn) * L;
+    double d0 = r[4];
+    r[4] -= radc * b2 * f;
+    pn = 1.0 / (1.0 + r[4]);
+    r[1] = xp / pn;
+    r[3] = yp / pn;
+    r[1] -= L * (re - (d0 - r[0] * h) * h);
+    r[3] += L * im;
+    r[5] += L * h * r[0];
+}
+
+/* quadfringe.c:3-51: sgn = +1 (QuadFringePassP) or -1 (QuadFringePassN) */
+static void o_quad_fringe(double *r, double b2, int sgn) {
+    double u = b2 / (12.0 * (1.0 + r[4]));
+    double x2 = r[0] * r[0], z2 = r[2] * r[2], xz = r[0] * r[2];
+    double gx = u * (x2 + 3 * z2) * r[0];
+    double gz = u * (z2 + 3 * x2) * r[2];
+    double t1 = 3 * u * (2 * xz * r[3] - (x2 + z2) * r[1]);
+    double t3 = 3 * u * (2 * xz * r[1] - (x2 + z2) * r[3]);
+    double dc = (gz * r[3] - gx * r[1]) / (1 + r[4]);
+    if (sgn > 0) {
+        r[0] += gx; r[2] -= gz; r[5] -= dc; r[1] += t1; r[3] -= t3;
+    } else {
+        r[0] -= gx; r[2] += gz; r[5] += dc; r[1] -= t1; r[3] += t3;
+    }
+}
+
+/* quadfringe.c: quadPartialFringeMatrix, 2x2 blocks (m[0..3] x, m[4..7] y) */
+static void o_fringe_matrix(double K1, const double *fi, int part, double *m) {
+    double in = 1.0, k2 = K1 * K1, j1x, j2x, j3x, j1y, j2y, j3y;
+    if (part == 1) {
+        j1x = in * (K1 * fi[1] - 2 * k2 * fi[3] / 3. - k2 * fi[0] * fi[2] / 2);
+        j2x = in * K1 * fi[2];
+        j3x = in * k2 * (fi[2] + fi[4] + fi[0] * fi[1]);
+        j1y = in * (-K1 * fi[1] - 2 * k2 * fi[3] / 3. - k2 * fi[0] * fi[2] / 2);
+    } else {
+        j1x = in * (K1 * fi[1] + k2 * fi[0] * fi[2] / 2);
+        j2x = in * K1 * fi[2];
+        j3x = in * k2 * (fi[4] - fi[0] * fi[1]);
+        j1y = in * (-K1 * fi[1] + k2 * fi[0] * fi[2] / 2);
+    }
+    j2y = -j2x;
+    j3y = j3x;
+    double ex = exp(j1x), ey = exp(j1y);
+    m[0] = ex; m[1] = j2x / ex; m[2] = ex * j3x; m[3] = (1 + j2x * j3x) / ex;
+    m[4] = ey; m[5] = j2y / ey; m[6] = ey * j3y; m[7] = (1 + j2y * j3y) / ey;
+}
+
+static void o_apply22(double *r, const double *m) {
+    double x = r[0], px = r[1], y = r[2], py = r[3];
+    r[0] = m[0] * x + m[1] * px;
+    r[1] = m[2] * x + m[3] * px;
+    r[2] = m[4] * y + m[5] * py;
+    r[3] = m[6] * y + m[7] * py;
+}
+
+/* quadfringe.c:45-112 linearQuadFringeElegantEntrance/Exit */
+static void o_lin_fringe(double *r, double b2, const double *fm, const double *fp, int entrance) {
+    double m[8], s;
+    if (entrance) {
+        o_fringe_matrix(b2, fp, 2, m);
+        s = m[0]; m[0] = m[3]; m[3] = s;
+        s = m[4]; m[4] = m[7]; m[7] = s;
+        o_apply22(r, m);
+        o_quad_fringe(r, b2, +1);
+        o_fringe_matrix(b2, fm, 1, m);
+        s = m[0]; m[0] = m[3]; m[3] = s;
+        s = m[4]; m[4] = m[7]; m[7] = s;
+        o_apply22(r, m);
+    } else {
+        o_fringe_matrix(b2, fm, 1, m);
+        o_apply22(r, m);
+        o_quad_fringe(r, b2, -1);
+        o_fringe_matrix(b2, fp, 2, m);
+        o_apply22(r, m);
+    }
+}
+
+/* atphyslib.c:15-79 edge_fringe_entrance/exit; sgn +1 entrance, -1 exit */
+static void o_edge(double *r, double h, double edge, double fint, double gap, int method,
+                   int sgn) {
+    double fc = 0.0, fy;
+    if (!((fint == 0.0) || (gap == 0.0) || (method == 0))) {
+        double se = sin(edge), ce = cos(edge);
+        fc = h * gap * fint * (1 + se * se) / ce;
+    }
+    double fx = h * tan(edge);
+    if (method == 2)
+        fy = h * tan(edge - fc / (1 + r[4])) / (1 + r[4]);
+    else if (method == 3)
+        fy = (sgn > 0) ? h * tan(edge - fc + r[1] / (1 + r[4]))
+                       : h * tan(edge - fc - r[1] / (1 + r[4]));
+    else
+        fy = h * tan(edge - fc / (1 + r[4]));
+    r[1] += r[0] * fx;
+    r[3] -= r[2] * fy;
+}
+
+/* diff_bend_fringe.c:1-52 (bdiff == NULL) */
+static void o_edge_rad(double *r, double h, double edge, double fint, double gap, int method,
+                       double sgn) {
+    double pn = 1.0 / (1.0 + r[4]);
+    double psi = 0.0, fy;
+    if (!((fint == 0.0) || (gap == 0.0) || (method == 0))) {
+        double se = sin(edge), ce = cos(edge);
+        psi = h * gap * fint * (1.0 + se * se) / ce;
+    }
+    double fx = h * tan(edge);
+    if (method == 2)
+        fy = h * tan(edge - psi * pn) * pn;
+    else if (method == 3)
+        fy = h * tan(edge - psi + sgn * r[1] * pn);
+    else
+        fy = h * tan(edge - psi * pn);
+    r[1] += r[0] * fx;
+    r[3] -= r[2] * fy;
+}
+
+/* ---- pass methods -------------------------------------------------------- */
+
+static double o_gamma(double energy, double rest) {
+    /* atelem.c:364-371 */
+    return (rest == 0.0) ? 1.0E-9 * energy / O_E0 : energy / rest;
+}
+
+/* StrMPole/BndMPole (Rad) Symplectic4: StrMPoleSymplectic4Pass.c:29-109,
+ * BndMPoleSymplectic4Pass.c:38-129, StrMPoleSymplectic4RadPass.c:30-115,
+ * BndMPoleSymplectic4RadPass.c:39-128 */
+static void o_multipole(double *r, const OElem *e, const double *A, const double *B, int bend,
+                        int rad, double radc) {
+    double le = e->Length;
+    double SL = le / e->NumIntSteps;
+    double L1 = SL * O_DRIFT1, L2 = SL * O_DRIFT2, K1 = SL * O_KICK1, K2 = SL * O_KICK2;
+    int n = e->MaxOrder;
+    double h = bend ? e->BendingAngle / e->Length : 0.0;
+    int lin_in = (e->fringeIntM0 && e->fringeIntP0 && e->FringeQuadEntrance == 2);
+    int lin_out = (e->fringeIntM0 && e->fringeIntP0 && e->FringeQuadExit == 2);
+    double s = e->Scaling;
+    double nl1 = 0, nl2 = 0;
+    if (s != 1.0) o_pref(r, s);
+    if (!rad) {
+        double pn = 1.0 / (1.0 + r[4]);
+        nl1 = L1 * pn;
+        nl2 = L2 * pn;
+    }
+    if (e->T1) o_addv(r, e->T1);
+    if (e->R1) o_mulmv(r, e->R1);
+    if (e->RApertures) o_rect_ap(r, e->RApertures);
+    if (e->EApertures) o_ellip_ap(r, e->EApertures);
+    if (bend) {
+        if (rad) o_edge_rad(r, h, e->EntranceAngle, e->FringeInt1, e->FullGap, e->FringeBendEntrance, 1.0);
+        else o_edge(r, h, e->EntranceAngle, e->FringeInt1, e->FullGap, e->FringeBendEntrance, 1);
+    }
+    if (e->FringeQuadEntrance && B[1] != 0) {
+        if (lin_in) o_lin_fringe(r, B[1], e->fringeIntM0, e->fringeIntP0, 1);
+        else o_quad_fringe(r, B[1], +1);
+    }
+    for (int m = 0; m < e->NumIntSteps; m++) {
+        if (rad) {
+            o_ddrift(r, L1);
+            if (bend) o_bndkick_rad(r, A, B, n, K1, h, radc); else o_strkick_rad(r, A, B, n, K1, radc);
+            o_ddrift(r, L2);
+            if (bend) o_bndkick_rad(r, A, B, n, K2, h, radc); else o_strkick_rad(r, A, B, n, K2, radc);
+            o_ddrift(r, L2);
+            if (bend) o_bndkick_rad(r, A, B, n, K1, h, radc); else o_strkick_rad(r, A, B, n, K1, radc);
+            o_ddrift(r, L1);
+        } else {
+            o_fastdrift(r, nl1);
+            if (bend) o_bndkick(r, A, B, K1, h, n); else o_strkick(r, A, B, K1, n);
+            o_fastdrift(r, nl2);
+            if (bend) o_bndkick(r, A, B, K2, h, n); else o_strkick(r, A, B, K2, n);
+            o_fastdrift(r, nl2);
+            if (bend) o_bndkick(r, A, B, K1, h, n); else o_strkick(r, A, B, K1, n);
+            o_fastdrift(r, nl1);
+        }
+    }
+    if (e->FringeQuadExit && B[1] != 0) {
+        if (lin_out) o_lin_fringe(r, B[1], e->fringeIntM0, e->fringeIntP0, 0);
+        else o_quad_fringe(r, B[1], -1);
+    }
+    if (bend) {
+        if (rad) o_edge_rad(r, h, e->ExitAngle, e->FringeInt2, e->FullGap, e->FringeBendExit, -1.0);
+        else o_edge(r, h, e->ExitAngle, e->FringeInt2, e->FullGap, e->FringeBendExit, -1);
+    }
+    if (e->RApertures) o_rect_ap(r, e->RApertures);
+    if (e->EApertures) o_ellip_ap(r, e->EApertures);
+    if (e->R2) o_mulmv(r, e->R2);
+    if (e->T2) o_addv(r, e->T2);
+    if (s != 1.0) o_pref(r, 1.0 / s);
+}
+
+/* ThinMPolePass.c:28-70 */
+static void o_thin(double *r, const OElem *e, const double *A, const double *B) {
+    double s = e->Scaling;
+    if (s != 1.0) o_pref(r, s);
+    if (e->T1) o_addv(r, e->T1);
+    if (e->R1) o_mulmv(r, e->R1);
+    if (e->RApertures) o_rect_ap(r, e->RApertures);
+    if (e->EApertures) o_ellip_ap(r, e->EApertures);
+    o_strkick(r, A, B, 1.0, e->MaxOrder);
+    r[1] += e->bax * r[4];
+    r[3] -= e->bay * r[4];
+    r[5] -= e->bax * r[0] - e->bay * r[2];
+    if (e->R2) o_mulmv(r, e->R2);
+    if (e->T2) o_addv(r, e->T2);
+    if (s != 1.0) o_pref(r, 1.0 / s);
+}
+
+/* attrackfunc.c:5-42 trackRFCavity, via RFCavityPass.c:359-392 */
+static void o_rf(double *r, const OElem *e, double nv, double hn, int nturn, double T0) {
+    double le = e->Length, f = e->Frequency, lag = e->TimeLag, phi = e->PhaseLag;
+    if (le == 0) {
+        if (nv != 0)
+            r[4] += -nv * sin(O_TWOPI * f * ((r[5] - lag) / O_C0 - (hn / f - T0) * nturn) - phi);
+    } else {
+        double half = le / 2;
+        o_drift6(r, half);
+        if (nv != 0.0)
+            r[4] += -nv * sin(O_TWOPI * f * ((r[5] - lag) / O_C0 - (hn / f - T0) * nturn) - phi);
+        o_drift6(r, half);
+    }
+}
+
+/* CorrectorPass.c:25-90 */
+static void o_corr(double *r, const OElem *e) {
+    double xk = e->KickAngle[0], yk = e->KickAngle[1], le = e->Length, s = e->Scaling;
+    if (s != 1.0) o_pref(r, s);
+    if (le == 0.0) {
+        if (e->T1) o_addv(r, e->T1);
+        if (e->R1) o_mulmv(r, e->R1);
+        if (e->RApertures) o_rect_ap(r, e->RApertures);
+        if (e->EApertures) o_ellip_ap(r, e->EApertures);
+        r[1] += xk;
+        r[3] += yk;
+    } else {
+        double pn = 1.0 / (1.0 + r[4]);
+        double nl = le * pn;
+        if (e->T1) o_addv(r, e->T1);
+        if (e->R1) o_mulmv(r, e->R1);
+        if (e->RApertures) o_rect_ap(r, e->RApertures);
+        if (e->EApertures) o_ellip_ap(r, e->EApertures);
+        r[5] += nl * pn * (xk * xk / 3 + yk * yk / 3 + r[1] * r[1] + r[3] * r[3] + r[1] * xk + r[3] * yk) / 2;
+        r[0] += nl * (r[1] + xk / 2);
+        r[1] += xk;
+        r[2] += nl * (r[3] + yk / 2);
+        r[3] += yk;
+        if (e->RApertures) o_rect_ap(r, e->RApertures);
+        if (e->EApertures) o_ellip_ap(r, e->EApertures);
+    }
+    if (e->R2) o_mulmv(r, e->R2);
+    if (e->T2) o_addv(r, e->T2);
+    if (s != 1.0) o_pref(r, 1.0 / s);
+}
+
+/* DriftPass.c:16-48 */
+static void o_driftpass(double *r, const OElem *e) {
+    if (e->T1) o_addv(r, e->T1);
+    if (e->R1) o_mulmv(r, e->R1);
+    if (e->RApertures) o_rect_ap(r, e->RApertures);
+    if (e->EApertures) o_ellip_ap(r, e->EApertures);
+    o_drift6(r, e->Length);
+    if (e->RApertures) o_rect_ap(r, e->RApertures);
+    if (e->EApertures) o_ellip_ap(r, e->EApertures);
+    if (e->R2) o_mulmv(r, e->R2);
+    if (e->T2) o_addv(r, e->T2);
+}
+
+/* IdentityPass.c:20-43 */
+static void o_identity(double *r, const OElem *e) {
+    if (e->T1) o_addv(r, e->T1);
+    if (e->R1) o_mulmv(r, e->R1);
+    if (e->RApertures) o_rect_ap(r, e->RApertures);
+    if (e->EApertures) o_ellip_ap(r, e->EApertures);
+    if (e->R2) o_mulmv(r, e->R2);
+    if (e->T2) o_addv(r, e->T2);
+}
+
+/* Per-element constants the reference derives once per call or per cached
+ * element: KickAngle folded into the dipole terms (the reference writes it
+ * into the coefficient arrays and restores them afterwards), the RF harmonic
+ * number round(F*T0) and the normalised voltage. */
+typedef struct {
+    double A[64], B[64];
+    double nv, hn, radc;
+} OPrep;
+
+static void o_prepare(const OElem *e, OPrep *p, double energy, double rest, double T0) {
+    int n = e->MaxOrder;
+    if (e->pass == O_STRMPOLE || e->pass == O_STRMPOLE_RAD || e->pass == O_BNDMPOLE ||
+        e->pass == O_BNDMPOLE_RAD || e->pass == O_THINMPOLE) {
+        for (int k = 0; k <= n && k < 64; k++) {
+            p->A[k] = e->PolynomA[k];
+            p->B[k] = e->PolynomB[k];
+        }
+        if (e->KickAngle) {
+            if (e->pass == O_THINMPOLE) {
+                p->B[0] -= e->KickAngle[0];
+                p->A[0] += e->KickAngle[1];
+            } else {
+                p->B[0] -= sin(e->KickAngle[0]) / e->Length;
+                p->A[0] += sin(e->KickAngle[1]) / e->Length;
+            }
+        }
+    }
+    if (e->pass == O_STRMPOLE_RAD || e->pass == O_BNDMPOLE_RAD)
+        p->radc = O_RAD_CONST * pow(o_gamma(energy, rest), 3);
+    if (e->pass == O_RFCAVITY) {
+        p->hn = round(e->Frequency * T0);
+        p->nv = e->Voltage / energy;
+    }
+}
+
+static void o_element(double *r, const OElem *e, const OPrep *p, int nturn, double T0) {
+    if (isnan(r[0])) return;
+    switch (e->pass) {
+        case O_IDENTITY: o_identity(r, e); break;
+        case O_DRIFT: o_driftpass(r, e); break;
+        case O_STRMPOLE: o_multipole(r, e, p->A, p->B, 0, 0, 0.0); break;
+        case O_STRMPOLE_RAD: o_multipole(r, e, p->A, p->B, 0, 1, p->radc); break;
+        case O_BNDMPOLE: o_multipole(r, e, p->A, p->B, 1, 0, 0.0); break;
+        case O_BNDMPOLE_RAD: o_multipole(r, e, p->A, p->B, 1, 1, p->radc); break;
+        case O_THINMPOLE: o_thin(r, e, p->A, p->B); break;
+        case O_RFCAVITY: o_rf(r, e, p->nv, p->hn, nturn, T0); break;
+        case O_CORRECTOR: o_corr(r, e); break;
+        case O_APERTURE: o_rect_ap(r, e->Limits); break;
+        default: break;
+    }
+}
+
+/* pyat/at.c:123 */
+static int o_bad(const double *r) {
+    for (int k = 0; k < 6; k++)
+        if (!isfinite(r[k]) || (fabs(r[k]) > 1 && k < 5)) return 1;
+    return 0;
+}
+
+/* The engine of pyat/at.c:596-654 for one particle; returns 0. */
+static void o_particle(double *r, const OElem *el, const OPrep *pp, int nelem, int nturns,
+                       int turn0, int start, int end, const uint32_t *refs, int nref,
+                       int losses, int check, double T0, double *rout, int64_t np, int64_t p,
+                       uint8_t *lost, uint32_t *lturn, uint32_t *lelem, double *lcoord) {
+    int64_t slot = 0;
+    int is_lost = losses ? (lost[p] != 0) : 0;
+    for (int t = 0; t < nturns; t++) {
+        int nturn = turn0 + t;
+        int s0 = (t == 0) ? start : 0;
+        int ri = 0;
+        uint32_t next = (ri < nref) ? refs[ri++] : 0x7fffffffu;
+        for (int i = s0; i < end; i++) {
+            if ((uint32_t)i == next) {
+                if (rout) memcpy(rout + 6 * (p + np * slot), r, 6 * sizeof(double));
+                slot++;
+                next = (ri < nref) ? refs[ri++] : 0x7fffffffu;
+            }
+            o_element(r, &el[i], &pp[i], nturn, T0);
+            if (!check) continue;
+            if (losses) {
+                if (!is_lost && o_bad(r)) {
+                    is_lost = 1;
+                    lturn[p] = (uint32_t)nturn;
+                    lelem[p] = (uint32_t)i;
+                    memcpy(lcoord + 6 * p, r, 6 * sizeof(double));
+                    r[0] = NAN; r[1] = 0; r[2] = 0; r[3] = 0; r[4] = 0; r[5] = 0;
+                }
+            } else if (isfinite(r[0]) && o_bad(r)) {
+                r[0] = NAN; r[1] = 0; r[2] = 0; r[3] = 0; r[4] = 0; r[5] = 0;
+            }
+        }
+        if ((uint32_t)nelem == next) {
+            if (rout) memcpy(rout + 6 * (p + np * slot), r, 6 * sizeof(double));
+            slot++;
+        }
+    }
+    if (losses) lost[p] = (uint8_t)is_lost;
+}
+
+/* Track np particles (6, np Fortran order) in place.  Mirrors at_atpass. */
+int oracle_track(const OElem *el, int nelem, double *r, int64_t np, int nturns, int turn0,
+                 int start, int end, const uint32_t *refs, int nref, int losses, int check,
+                 double energy, double rest, double T0, double *rout, uint8_t *lost,
+                 uint32_t *lturn, uint32_t *lelem, double *lcoord, int nthreads) {
+    OPrep *pp = (OPrep *)calloc((size_t)(nelem > 0 ? nelem : 1), sizeof(OPrep));
+    if (!pp) return -1;
+    for (int i = 0; i < nelem; i++) o_prepare(&el[i], &pp[i], energy, rest, T0);
+    if (losses) {
+        memset(lost, 0, (size_t)np);
+        memset(lturn, 0, (size_t)np * 4);
+        memset(lelem, 0, (size_t)np * 4);
+        memset(lcoord, 0, (size_t)np * 48);
+    }
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads > 0 ? nthreads : 1)
+    for (int64_t p = 0; p < np; p++) {
+        o_particle(r + 6 * p, el, pp, nelem, nturns, turn0, start, end, refs, nref, losses, check,
+                   T0, rout, np, p, lost, lturn, lelem, lcoord);
+    }
+    free(pp);
+    return 0;
+}

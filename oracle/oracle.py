@@ -1,0 +1,169 @@
+"""ORACLE -- test infrastructure only.
+
+Python front of the C restatement in ``oracle/oracle.c`` of the reference
+tracking path (``pyat/at.c`` engine + the ``atintegrators`` pass methods on
+the accelerated path).  It reads elements by attribute, as the reference's
+integrators do (``atintegrators/atelem.c:219-352``), independently of the
+product's lattice compiler, and calls the C engine through ctypes.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg use this module, and only as the checker; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sysconfig
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "oracle.c")
+LIB = os.path.join(HERE, "liboracle.so")
+
+PASSES = {
+    "IdentityPass": 0, "DriftPass": 1, "StrMPoleSymplectic4Pass": 2,
+    "StrMPoleSymplectic4RadPass": 3, "BndMPoleSymplectic4Pass": 4,
+    "BndMPoleSymplectic4RadPass": 5, "ThinMPolePass": 6, "RFCavityPass": 7,
+    "CorrectorPass": 8, "AperturePass": 9,
+}
+C0 = 2.99792458e8
+
+_dp = C.POINTER(C.c_double)
+
+
+class OElem(C.Structure):
+    _fields_ = [
+        ("pass_", C.c_int32), ("MaxOrder", C.c_int32), ("NumIntSteps", C.c_int32),
+        ("FringeBendEntrance", C.c_int32), ("FringeBendExit", C.c_int32),
+        ("FringeQuadEntrance", C.c_int32), ("FringeQuadExit", C.c_int32), ("pad", C.c_int32),
+        ("Length", C.c_double), ("BendingAngle", C.c_double), ("EntranceAngle", C.c_double),
+        ("ExitAngle", C.c_double), ("FringeInt1", C.c_double), ("FringeInt2", C.c_double),
+        ("FullGap", C.c_double), ("Scaling", C.c_double), ("Voltage", C.c_double),
+        ("Frequency", C.c_double), ("TimeLag", C.c_double), ("PhaseLag", C.c_double),
+        ("bax", C.c_double), ("bay", C.c_double),
+        ("PolynomA", _dp), ("PolynomB", _dp), ("fringeIntM0", _dp), ("fringeIntP0", _dp),
+        ("R1", _dp), ("R2", _dp), ("T1", _dp), ("T2", _dp), ("RApertures", _dp),
+        ("EApertures", _dp), ("KickAngle", _dp), ("Limits", _dp),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile the C restatement (ISO C99, no FMA contraction, OpenMP)."""
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+        cmd = ["gcc", "-O2", "-std=c99", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
+               "-fPIC", "-shared", SRC, "-o", LIB + ".tmp", "-lm"]
+        subprocess.run(cmd, check=True)
+        os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB)
+        f = L.oracle_track
+        f.argtypes = [C.POINTER(OElem), C.c_int, C.c_void_p, C.c_int64, C.c_int, C.c_int,
+                      C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                      C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                      C.c_void_p, C.c_int]
+        f.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _arr(el, name, keep):
+    a = getattr(el, name, None)
+    if a is None:
+        return None
+    a = np.asarray(a, dtype=np.float64).ravel(order="F").copy()
+    keep.append(a)
+    return a.ctypes.data_as(_dp)
+
+
+def _elements(line, keep):
+    arr = (OElem * max(len(line), 1))()
+    for o, el in zip(arr, line):
+        pm = el.PassMethod
+        if pm not in PASSES:
+            raise RuntimeError("PassMethod %s: library, module or trackFunction not found" % pm)
+        o.pass_ = PASSES[pm]
+        o.Length = float(getattr(el, "Length", 0.0))
+        o.MaxOrder = int(getattr(el, "MaxOrder", 0))
+        o.NumIntSteps = int(getattr(el, "NumIntSteps", 0))
+        o.BendingAngle = float(getattr(el, "BendingAngle", 0.0)) if pm.startswith("Bnd") else 0.0
+        o.EntranceAngle = float(getattr(el, "EntranceAngle", 0.0))
+        o.ExitAngle = float(getattr(el, "ExitAngle", 0.0))
+        o.FringeBendEntrance = int(getattr(el, "FringeBendEntrance", 1))
+        o.FringeBendExit = int(getattr(el, "FringeBendExit", 1))
+        o.FringeInt1 = float(getattr(el, "FringeInt1", 0.0))
+        o.FringeInt2 = float(getattr(el, "FringeInt2", 0.0))
+        o.FullGap = float(getattr(el, "FullGap", 0.0))
+        o.Scaling = float(getattr(el, "FieldScaling", 1.0))
+        o.FringeQuadEntrance = int(getattr(el, "FringeQuadEntrance", 0))
+        o.FringeQuadExit = int(getattr(el, "FringeQuadExit", 0))
+        o.Voltage = float(getattr(el, "Voltage", 0.0))
+        o.Frequency = float(getattr(el, "Frequency", 0.0))
+        o.TimeLag = float(getattr(el, "TimeLag", 0.0))
+        o.PhaseLag = float(getattr(el, "PhaseLag", 0.0))
+        if pm == "ThinMPolePass" and getattr(el, "BendingAngle", None) is not None:
+            # ThinMPolePass.c:219-224 with atelem.c:312-315: size dims[0]*dims[1],
+            # where dims[1] counts as 0 for a 1-D array
+            ba = np.asarray(el.BendingAngle, dtype=np.float64)
+            sz = ba.shape[0] * ba.shape[1] if ba.ndim >= 2 else 0
+            flat = ba.ravel(order="F")
+            o.bax = float(flat[0]) if sz >= 1 else 0.0
+            o.bay = float(flat[1]) if sz >= 2 else 0.0
+        for name in ("PolynomA", "PolynomB", "fringeIntM0", "fringeIntP0", "R1", "R2", "T1",
+                     "T2", "RApertures", "EApertures", "KickAngle", "Limits"):
+            setattr(o, name, _arr(el, name, keep))
+    return arr
+
+
+def track(line, r, nturns, refpts=None, turn=0, energy=0.0, rest_energy=0.0, losses=False,
+          start_elem=0, end_elem=None, nthreads=None, t0=None, element=False):
+    """Track the (6, N) Fortran-ordered ``r`` in place with the C oracle.
+
+    Returns ``(rout, lossdict or None)`` with the reference's layouts."""
+    lib = _load()
+    keep: list = []
+    els = _elements(line, keep)
+    nelem = len(line)
+    ring_length = sum(float(getattr(e, "Length", 0.0)) for e in line)
+    T0 = ring_length / C0 if t0 is None else t0
+    if end_elem is None or end_elem == 0:
+        end_elem = nelem
+    npart = r.size // 6
+    refs = np.ascontiguousarray(refpts if refpts is not None else [], dtype=np.uint32)
+    rout = np.zeros((6, npart, refs.size, nturns), dtype=np.float64, order="F")
+    ld = None
+    lost = lturn = lelem = lcoord = None
+    if losses:
+        lost = np.zeros(npart, dtype=np.uint8)
+        lturn = np.zeros(npart, dtype=np.uint32)
+        lelem = np.zeros(npart, dtype=np.uint32)
+        lcoord = np.zeros((6, npart), dtype=np.float64, order="F")
+    if nthreads is None:
+        nthreads = os.cpu_count() or 1
+    rc = lib.oracle_track(els, nelem, r.ctypes.data, npart, nturns, turn, start_elem, end_elem,
+                          refs.ctypes.data if refs.size else None, refs.size,
+                          1 if losses else 0, 0 if element else 1, energy, rest_energy, T0,
+                          rout.ctypes.data if refs.size else None,
+                          None if lost is None else lost.ctypes.data,
+                          None if lturn is None else lturn.ctypes.data,
+                          None if lelem is None else lelem.ctypes.data,
+                          None if lcoord is None else lcoord.ctypes.data, nthreads)
+    if rc != 0:
+        raise MemoryError("oracle allocation failed")
+    if losses:
+        ld = {"islost": lost.astype(bool), "turn": lturn, "elem": lelem, "coord": lcoord}
+    return rout, ld
+
+
+def ext_suffix() -> str:
+    return sysconfig.get_config_var("EXT_SUFFIX") or ".so"

@@ -1,0 +1,187 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Runs the reference pyat (atcollab/at: its C engine ``pyat/at.c`` and its
+``atintegrators``), built from the reference sources by
+``oracle/build_ref.py --full`` into ``oracle/_ref/pyat_full``, on the seeded
+cases of ``tests/golden/cases.py`` and on the reference's own machine file
+``hmba.mat``, and stores inputs and outputs as small ``.npz`` files.  Only
+this script touches the reference; the tests read the fixtures.
+
+    python oracle/build_ref.py --full && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "oracle", "_ref", "pyat_full"))
+sys.path.insert(0, HERE)
+
+import at  # noqa: E402  (the reference, built from its sources)
+from at.tracking.atpass import atpass, elempass  # noqa: E402
+
+import cases  # noqa: E402
+
+ARRAY_ATTRS = {"PolynomA", "PolynomB", "KickAngle", "T1", "T2", "R1", "R2", "RApertures",
+               "EApertures", "Limits", "fringeIntM0", "fringeIntP0", "BendingAngle"}
+
+
+def ref_element(d):
+    kw = {}
+    late = {}
+    for k, v in d.items():
+        if k in ("FamName",):
+            continue
+        if k in ARRAY_ATTRS and not (k == "BendingAngle" and np.isscalar(v)):
+            a = np.asfortranarray(np.asarray(v, dtype=np.float64))
+            if k == "BendingAngle":
+                late[k] = a            # a thin multipole's (bax, bay) array
+            else:
+                kw[k] = a
+        else:
+            kw[k] = v
+    el = at.Element(d.get("FamName", "E"), **kw)
+    for k, v in late.items():
+        object.__setattr__(el, k, v)
+    # pyat's base Element keeps the values as given; make sure the integer
+    # attributes are Python ints as the integrators read them with PyLong
+    for k in ("MaxOrder", "NumIntSteps", "FringeBendEntrance", "FringeBendExit",
+              "FringeQuadEntrance", "FringeQuadExit"):
+        if hasattr(el, k):
+            setattr(el, k, int(getattr(el, k)))
+    return el
+
+
+def spec_json(d):
+    out = {}
+    for k, v in d.items():
+        if isinstance(v, np.ndarray):
+            out[k] = {"shape": list(v.shape), "data": v.ravel(order="F").tolist()}
+        else:
+            out[k] = v
+    return out
+
+
+def element_fixtures():
+    electron = at.Particle("electron")
+    res = {}
+    meta = {}
+    for name, d in cases.element_cases():
+        r0 = cases.element_particles()
+        if d["PassMethod"] == "AperturePass":
+            r0[0, 5] = 5e-3
+        r = r0.copy(order="F")
+        el = ref_element(d)
+        rad = "Rad" in d["PassMethod"] or d["PassMethod"] == "RFCavityPass"
+        kw = dict(energy=6e9, particle=electron) if rad else {}
+        elempass(el, r, **kw)
+        res[name + "/in"] = r0
+        res[name + "/out"] = r
+        meta[name] = spec_json(d)
+    np.savez_compressed(os.path.join(HERE, "elements.npz"), **res)
+    with open(os.path.join(HERE, "elements.json"), "w") as f:
+        json.dump(meta, f, indent=0, sort_keys=True)
+
+
+def fodo_fixture():
+    sys.path.insert(0, REPO)
+    from at_b200 import rings
+    ring = rings.fodo_ring()
+    line = [ref_element(vars_of(e)) for e in ring]
+    r0 = rings.gaussian(10000)[:, ::40].copy(order="F")       # 250 particles
+    r0[:, :50] *= 4.0                                         # some to be lost
+    r = r0.copy(order="F")
+    rout, ld = atpass(line, r, 200, energy=3e9, particle=at.Particle("electron"), losses=True)
+    np.savez_compressed(os.path.join(HERE, "fodo_200turns.npz"), rin=r0, rout_final=r,
+                        islost=ld["islost"], lturn=ld["turn"], lelem=ld["elem"],
+                        lcoord=ld["coord"])
+    # refpts snapshots: 64 particles, 30 turns
+    r0 = r0[:, 20:84].copy(order="F")
+    r = r0.copy(order="F")
+    refs = np.array([0, 100, 385], dtype=np.uint32)
+    rout, ld = atpass(line, r, 30, refpts=refs, energy=3e9, particle=at.Particle("electron"),
+                      losses=True)
+    np.savez_compressed(os.path.join(HERE, "fodo_refpts.npz"), rin=r0, rout_final=r,
+                        rout=rout, refpts=refs, islost=ld["islost"], lturn=ld["turn"],
+                        lelem=ld["elem"], lcoord=ld["coord"])
+    # radiating copy, 20 turns
+    rr = rings.radiating(ring)
+    line = [ref_element(vars_of(e)) for e in rr]
+    r0 = rings.gaussian(64, seed=3)
+    r = r0.copy(order="F")
+    atpass(line, r, 20, energy=3e9, particle=at.Particle("electron"))
+    np.savez_compressed(os.path.join(HERE, "fodo_rad_20turns.npz"), rin=r0, rout_final=r)
+
+
+def vars_of(e):
+    d = {}
+    for k, v in vars(e).items():
+        d[k] = v
+    return d
+
+
+def sink_fixture():
+    line = [ref_element(d) for d in cases.kitchen_sink()]
+    r0 = cases.element_particles(96, seed=21, scale=0.4)
+    r = r0.copy(order="F")
+    refs = np.array([0, 3, 7, 12, len(line)], dtype=np.uint32)
+    rout, ld = atpass(line, r, 3, refpts=refs, turn=5, energy=6e9,
+                      particle=at.Particle("electron"), losses=True)
+    np.savez_compressed(os.path.join(HERE, "sink_3turns.npz"), rin=r0, rout_final=r, rout=rout,
+                        refpts=refs, islost=ld["islost"], lturn=ld["turn"], lelem=ld["elem"],
+                        lcoord=ld["coord"])
+    # partial turn: start at element 4, refpts before the start are skipped
+    r = r0.copy(order="F")
+    rout, ld = atpass(line, r, 1, refpts=refs, start_elem=4, end_elem=15, energy=6e9,
+                      particle=at.Particle("electron"), losses=True)
+    np.savez_compressed(os.path.join(HERE, "sink_partial.npz"), rin=r0, rout_final=r,
+                        rout=rout, refpts=refs, islost=ld["islost"], lturn=ld["turn"],
+                        lelem=ld["elem"], lcoord=ld["coord"])
+
+
+def hmba_fixture():
+    path = os.path.join(REPO, "oracle", "_ref", "pyat_full", "machine_data", "hmba.mat")
+    ring = at.load_lattice(path)
+    out = {}
+    for tag, lat in (("off", ring.radiation_off(copy=True)), ("6d", ring.enable_6d(copy=True))):
+        specs = []
+        for e in lat:
+            d = {"FamName": e.FamName, "PassMethod": e.PassMethod}
+            for k in ("Length", "PolynomA", "PolynomB", "MaxOrder", "NumIntSteps", "BendingAngle",
+                      "EntranceAngle", "ExitAngle", "FringeQuadEntrance", "FringeQuadExit",
+                      "Voltage", "Frequency", "HarmNumber", "TimeLag", "Energy",
+                      "FringeBendEntrance", "FringeBendExit", "FullGap", "FringeInt1",
+                      "FringeInt2"):
+                if hasattr(e, k):
+                    v = getattr(e, k)
+                    d[k] = np.asarray(v).tolist() if isinstance(v, np.ndarray) else v
+            specs.append(d)
+        line = [ref_element(d) for d in specs]
+        r0 = np.asfortranarray(np.random.default_rng(5).standard_normal((6, 32)) *
+                               np.array([1e-4, 1e-5, 1e-5, 1e-6, 1e-3, 1e-3])[:, None])
+        r = r0.copy(order="F")
+        atpass(line, r, 1, energy=float(ring.energy), particle=ring.particle)
+        out[tag] = dict(specs=specs, energy=float(ring.energy))
+        np.savez_compressed(os.path.join(HERE, "hmba_%s.npz" % tag), rin=r0, rout_final=r)
+        if tag == "off":
+            # the reference test's partial-turn cases (test_atpass.py:157-171)
+            for s, e in ((100, 0), (100, 110)):
+                r1 = np.array([0, 1e-6, 0, 0, 0, 0], dtype=np.float64)
+                atpass(line, r1, 1, start_elem=s, end_elem=e, energy=float(ring.energy))
+                out[tag]["partial_%d_%d" % (s, e)] = r1.tolist()
+    with open(os.path.join(HERE, "hmba.json"), "w") as f:
+        json.dump(out, f)
+
+
+if __name__ == "__main__":
+    element_fixtures()
+    fodo_fixture()
+    sink_fixture()
+    hmba_fixture()
+    print("golden fixtures written to", HERE)

@@ -1,0 +1,202 @@
+"""CUDA engine against the oracle, on the same seeded inputs.
+
+Tolerances (stated per test):
+  * exact mode: bit-identical wherever the path has no sin/tan; where the
+    RF cavity's sin or a bend's per-particle tan is involved, CUDA's libdevice
+    and glibc may differ by an ulp, so a scale-relative 1e-14 is allowed;
+  * fast mode (FMA, reciprocal reuse): scale-relative 1e-13 after one turn,
+    1e-9 after 1000 turns on particles that survive in both, and the same
+    lost set except for particles within 1e-9 of a loss boundary at the loss
+    element.
+"Scale-relative" divides each coordinate's largest difference by that
+coordinate's largest magnitude over the particles (conftest.scale_rel_diff).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from at_b200 import elements as E
+from at_b200 import rings
+from at_b200.engine import Engine
+from at_b200.lattice import compile_lattice
+from oracle import oracle
+
+from conftest import ELECTRON_REST, GOLDEN, scale_rel_diff
+
+pytestmark = pytest.mark.gpu
+
+TRANSCENDENTAL = ("rf_", "bend_fringe", "bend_full", "thin_ba")
+
+
+def _gpu_track(line, r, nturns, energy, rest, mode, element=False, **kw):
+    eng = Engine.get(0)
+    cl = compile_lattice(line, energy, rest, t0=0.0 if element else None)
+    lid = eng.upload(cl)
+    try:
+        out = eng.track(lid, r, nturns, kw.pop("turn", 0), kw.pop("start_elem", 0),
+                        kw.pop("end_elem", cl.nelem), mode=mode, element=element, **kw)
+    finally:
+        eng.free(lid)
+    return out
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+@pytest.mark.parametrize("name,spec", cases.element_cases(), ids=[c[0] for c in cases.element_cases()])
+def test_element_vs_oracle(name, spec, mode):
+    el = cases.make_element(spec, E.Element)
+    r0 = cases.element_particles(256, seed=3)
+    rad = "Rad" in spec["PassMethod"] or spec["PassMethod"] == "RFCavityPass"
+    en, rest = (6e9, ELECTRON_REST) if rad else (0.0, 0.0)
+    ro = r0.copy(order="F")
+    oracle.track([el], ro, 1, energy=en, rest_energy=rest, element=True, t0=0.0)
+    rg = r0.copy(order="F")
+    _gpu_track([el], rg, 1, en, rest, mode, element=True)
+    np.testing.assert_array_equal(np.isnan(rg), np.isnan(ro))
+    if mode == "exact" and not name.startswith(TRANSCENDENTAL):
+        np.testing.assert_array_equal(rg, ro)
+    else:
+        tol = 1e-14 if mode == "exact" else 1e-13
+        assert scale_rel_diff(rg, ro) <= tol
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_element_golden_fixture(golden, mode):
+    """The engine against the reference's own outputs (tests/golden)."""
+    g = golden("elements.npz")
+    for name, spec in cases.element_cases():
+        el = cases.make_element(spec, E.Element)
+        r = g[name + "/in"].copy(order="F")
+        rad = "Rad" in spec["PassMethod"] or spec["PassMethod"] == "RFCavityPass"
+        _gpu_track([el], r, 1, 6e9 if rad else 0.0, ELECTRON_REST if rad else 0.0, mode,
+                   element=True)
+        ref = g[name + "/out"]
+        np.testing.assert_array_equal(np.isnan(r), np.isnan(ref), err_msg=name)
+        assert scale_rel_diff(r, ref) <= (1e-14 if mode == "exact" else 1e-13), name
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_fodo_one_turn(mode):
+    ring = rings.fodo_ring()
+    r0 = rings.gaussian(4096)
+    ro = r0.copy(order="F")
+    oracle.track(ring, ro, 1, energy=3e9, rest_energy=ELECTRON_REST)
+    rg = r0.copy(order="F")
+    _gpu_track(ring, rg, 1, 3e9, ELECTRON_REST, mode)
+    assert scale_rel_diff(rg, ro) <= (1e-14 if mode == "exact" else 1e-13)
+
+
+def _near_boundary(coord):
+    """Lost coordinates within 1e-9 (relative) of the amplitude limit."""
+    c = np.abs(np.asarray(coord)[:5])
+    return np.any(np.abs(c - 1.0) <= 1e-9, axis=0)
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_fodo_1000_turns(mode):
+    """The plain-tracking workload at reduced particle count: 2048 particles,
+    1000 turns, losses on."""
+    ring = rings.fodo_ring()
+    r0 = rings.gaussian(10000)[:, :2048].copy(order="F")
+    ro = r0.copy(order="F")
+    _, lo = oracle.track(ring, ro, 1000, energy=3e9, rest_energy=ELECTRON_REST, losses=True)
+    rg = r0.copy(order="F")
+    _, lg, _ = _gpu_track(ring, rg, 1000, 3e9, ELECTRON_REST, mode, losses=True)
+    flip = lo["islost"] != lg["islost"]
+    # a particle may flip only if its loss coordinate sat on the boundary
+    nb = _near_boundary(np.where(lo["islost"], lo["coord"], lg["coord"]))
+    assert np.all(nb[flip]), "lost sets differ away from the boundary: %d" % flip.sum()
+    both = ~lo["islost"] & ~lg["islost"]
+    assert scale_rel_diff(rg[:, both], ro[:, both]) <= 1e-9
+    same = lo["islost"] & lg["islost"]
+    assert np.mean(lo["turn"][same] == lg["turn"][same]) > 0.99
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_golden_lattices(golden, mode):
+    tol = 1e-14 if mode == "exact" else 1e-13
+    ring = rings.fodo_ring()
+    g = golden("fodo_refpts.npz")
+    r = g["rin"].copy(order="F")
+    rout, ld, _ = _gpu_track(ring, r, 30, 3e9, ELECTRON_REST, mode, refpts=g["refpts"],
+                             losses=True)
+    assert scale_rel_diff(r, g["rout_final"]) <= 1e-11
+    assert scale_rel_diff(rout[:, :, :, 0], g["rout"][:, :, :, 0]) <= tol
+    np.testing.assert_array_equal(ld["islost"], g["islost"])
+    g = golden("fodo_rad_20turns.npz")
+    r = g["rin"].copy(order="F")
+    _gpu_track(rings.radiating(ring), r, 20, 3e9, ELECTRON_REST, mode)
+    assert scale_rel_diff(r, g["rout_final"]) <= 1e-11
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_kitchen_sink_losses_refpts(golden, mode):
+    g = golden("sink_3turns.npz")
+    line = [cases.make_element(s, E.Element) for s in cases.kitchen_sink()]
+    r = g["rin"].copy(order="F")
+    rout, ld, _ = _gpu_track(line, r, 3, 6e9, ELECTRON_REST, mode, refpts=g["refpts"],
+                             losses=True, turn=5)
+    np.testing.assert_array_equal(ld["islost"], g["islost"])
+    np.testing.assert_array_equal(ld["turn"], g["lturn"])
+    np.testing.assert_array_equal(ld["elem"], g["lelem"])
+    np.testing.assert_array_equal(np.isnan(r), np.isnan(g["rout_final"]))
+    assert scale_rel_diff(ld["coord"], g["lcoord"]) <= 1e-12
+    assert scale_rel_diff(rout[..., 0], g["rout"][..., 0]) <= 1e-12
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_partial_turn(golden, mode):
+    g = golden("sink_partial.npz")
+    line = [cases.make_element(s, E.Element) for s in cases.kitchen_sink()]
+    r = g["rin"].copy(order="F")
+    _, ld, _ = _gpu_track(line, r, 1, 6e9, ELECTRON_REST, mode, refpts=g["refpts"], losses=True,
+                          start_elem=4, end_elem=15)
+    np.testing.assert_array_equal(ld["islost"], g["islost"])
+    assert scale_rel_diff(r, g["rout_final"]) <= 1e-12
+
+
+@pytest.mark.parametrize("tag", ["off", "6d"])
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_hmba(golden, tag, mode):
+    with open(os.path.join(GOLDEN, "hmba.json")) as f:
+        data = json.load(f)[tag]
+    line = [cases.make_element(d, E.Element) for d in data["specs"]]
+    g = golden("hmba_%s.npz" % tag)
+    r = g["rin"].copy(order="F")
+    _gpu_track(line, r, 1, data["energy"], 0.0, mode)
+    assert scale_rel_diff(r, g["rout_final"]) <= (1e-14 if mode == "exact" else 1e-13)
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_pipelined_segments_match_resident(mode):
+    """A table too large for one shared-memory buffer streams through the
+    double-buffered bulk-copy pipeline; the result must not depend on it."""
+    ring = rings.radiating(rings.fodo_ring())
+    r0 = rings.gaussian(1000, seed=4)
+    eng = Engine.get(0)
+    cl = compile_lattice(ring, 3e9, ELECTRON_REST)
+    lid = eng.upload(cl)
+    ra = r0.copy(order="F")
+    eng.track(lid, ra, 5, mode=mode)
+    eng.set_launch(seg_cap_words=1024, resident_max_words=512)
+    try:
+        rb = r0.copy(order="F")
+        eng.track(lid, rb, 5, mode=mode)
+    finally:
+        eng.set_launch(seg_cap_words=6144, resident_max_words=14336)
+        eng.free(lid)
+    np.testing.assert_array_equal(ra, rb)
+
+
+def test_large_ring_one_turn():
+    """The radiating large ring (misaligned, ~2000 elements) against the oracle."""
+    ring = rings.large_ring()
+    r0 = rings.large_ring_bunch(2048)
+    ro = r0.copy(order="F")
+    oracle.track(ring, ro, 1, energy=ring.energy, rest_energy=ring.particle.rest_energy)
+    for mode, tol in (("exact", 1e-14), ("fast", 1e-13)):
+        rg = r0.copy(order="F")
+        _gpu_track(ring, rg, 1, ring.energy, ring.particle.rest_energy, mode)
+        assert scale_rel_diff(rg, ro) <= tol, mode
