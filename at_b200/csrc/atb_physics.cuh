@@ -37,6 +37,19 @@ __device__ __forceinline__ bool all_finite(const P6& r) {
            isfinite(r.dp) && isfinite(r.ct);
 }
 
+/* Fast-mode reciprocal of a positive operand near 1: the hardware estimate
+ * (rcp.approx.ftz.f64) refined by two Newton-Raphson steps
+ * y <- y + y(1 - d y) (Markstein's iteration; each step squares the relative
+ * error), within an ulp of 1/d.  Only the "fast" kernels use it. */
+__device__ __forceinline__ double rcp_nr(double d) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+    double e = fma(-d, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-d, y, 1.0);
+    return fma(y, e, y);
+}
+
 /* atlalib.c:50-57 ATaddvv */
 __device__ __forceinline__ void add_t(P6& r, const double* t) {
     r.x += t[0]; r.px += t[1]; r.y += t[2]; r.py += t[3]; r.dp += t[4]; r.ct += t[5];
@@ -62,22 +75,20 @@ __device__ __forceinline__ void mult_dense(P6& r, const double* A) {
 
 /* ATmultmv for a matrix that only rotates the x/y planes: the dense sum with
  * its zero terms dropped, which is value-identical for finite coordinates.
- * A non-finite coordinate takes the dense path so 0*inf -> NaN propagates as
- * in the reference. */
+ * A non-finite coordinate takes the full sum with the zero entries written
+ * out, so 0*inf -> NaN propagates exactly as in the reference. */
 __device__ __forceinline__ void mult_tilt(P6& r, const double* m) {
+    const double x = r.x, px = r.px, y = r.y, py = r.py, d = r.dp, c = r.ct;
     if (!all_finite(r)) {
-        double A[36];
-#pragma unroll
-        for (int k = 0; k < 36; ++k) A[k] = 0.0;
-        A[0 + 6 * 0] = m[0]; A[0 + 6 * 2] = m[1];
-        A[1 + 6 * 1] = m[2]; A[1 + 6 * 3] = m[3];
-        A[2 + 6 * 0] = m[4]; A[2 + 6 * 2] = m[5];
-        A[3 + 6 * 1] = m[6]; A[3 + 6 * 3] = m[7];
-        A[4 + 6 * 4] = 1.0; A[5 + 6 * 5] = 1.0;
-        mult_dense(r, A);
+        const double z = 0.0;
+        r.x = 0.0 + m[0] * x + z * px + m[1] * y + z * py + z * d + z * c;
+        r.px = 0.0 + z * x + m[2] * px + z * y + m[3] * py + z * d + z * c;
+        r.y = 0.0 + m[4] * x + z * px + m[5] * y + z * py + z * d + z * c;
+        r.py = 0.0 + z * x + m[6] * px + z * y + m[7] * py + z * d + z * c;
+        r.dp = 0.0 + z * x + z * px + z * y + z * py + 1.0 * d + z * c;
+        r.ct = 0.0 + z * x + z * px + z * y + z * py + z * d + 1.0 * c;
         return;
     }
-    const double x = r.x, px = r.px, y = r.y, py = r.py;
     r.x = m[0] * x + m[1] * y;
     r.px = m[2] * px + m[3] * py;
     r.y = m[4] * x + m[5] * y;
@@ -224,14 +235,14 @@ __device__ __forceinline__ void str_kick_rad(P6& r, const PL& pl, double L, doub
         double xpr = r.px * pn;
         double ypr = r.py * pn;
         double s = xpr * xpr + ypr * ypr;
-        double vn = 1.0 / (1.0 + s);
+        double vn = rcp_nr(1.0 + s);
         double cr = im * ypr - re * xpr;
         double b2p = (re * re + im * im + cr * cr) * vn;
         double opd = 1.0 + r.dp;
         double factor = (1.0 + 0.5 * s) * (opd * opd) * L;
         r.dp -= radc * b2p * factor;
         opd = 1.0 + r.dp;
-        pn = 1.0 / opd;
+        pn = rcp_nr(opd);
         r.px = xpr * opd - L * re;
         r.py = ypr * opd + L * im;
     } else {
@@ -262,7 +273,7 @@ __device__ __forceinline__ void bnd_kick_rad(P6& r, const PL& pl, double L, doub
         double ypr = r.py * pn;
         double hx = 1.0 + r.x * irho;
         double s = xpr * xpr + ypr * ypr;
-        double vn = 1.0 / (hx * hx + s);
+        double vn = rcp_nr(hx * hx + s);
         double by = re + irho;
         double cr = im * ypr - by * xpr;
         double b2p = ((by * by + im * im) * (hx * hx) + cr * cr) * vn;
@@ -271,7 +282,7 @@ __device__ __forceinline__ void bnd_kick_rad(P6& r, const PL& pl, double L, doub
         double dp0 = r.dp;
         r.dp -= radc * b2p * factor;
         opd = 1.0 + r.dp;
-        pn = 1.0 / opd;
+        pn = rcp_nr(opd);
         r.px = xpr * opd - L * (re - (dp0 - r.x * irho) * irho);
         r.py = ypr * opd + L * im;
         r.ct += lirho * r.x;

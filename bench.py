@@ -270,8 +270,12 @@ def run_b200(a):
     lcoord = torch.zeros((N, 6), dtype=torch.float64, device=dev)
     alive = torch.zeros(T, dtype=torch.int32, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated stream: the engine launches on it and the events are
+    # recorded on it (the legacy default stream's handle would read as NULL)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
+    assert sptr != 0
     lp = (lost.data_ptr(), lturn.data_ptr(), lelem.data_ptr(), lcoord.data_ptr())
 
     def step(turn0, with_alive):

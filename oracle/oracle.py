@@ -134,7 +134,11 @@ def track(line, r, nturns, refpts=None, turn=0, energy=0.0, rest_energy=0.0, los
     keep: list = []
     els = _elements(line, keep)
     nelem = len(line)
-    ring_length = sum(float(getattr(e, "Length", 0.0)) for e in line)
+    # pyat/at.c:504 accumulates the lengths one by one; Python's sum() of
+    # floats is compensated (3.12+) and can differ in the last bits
+    ring_length = 0.0
+    for e in line:
+        ring_length += float(getattr(e, "Length", 0.0))
     T0 = ring_length / C0 if t0 is None else t0
     if end_elem is None or end_elem == 0:
         end_elem = nelem

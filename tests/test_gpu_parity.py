@@ -191,12 +191,40 @@ def test_pipelined_segments_match_resident(mode):
 
 
 def test_large_ring_one_turn():
-    """The radiating large ring (misaligned, ~2000 elements) against the oracle."""
+    """The radiating large ring (misaligned, 1954 elements) against the oracle.
+
+    exact: 1e-14.  fast: 2e-13 -- FMA contraction alone sets the floor here:
+    the oracle's own C source compiled with -ffp-contract=fast -mfma differs
+    from the reference order by 1.08e-13 (y) after one turn of this ring."""
     ring = rings.large_ring()
     r0 = rings.large_ring_bunch(2048)
     ro = r0.copy(order="F")
     oracle.track(ring, ro, 1, energy=ring.energy, rest_energy=ring.particle.rest_energy)
-    for mode, tol in (("exact", 1e-14), ("fast", 1e-13)):
+    for mode, tol in (("exact", 1e-14), ("fast", 2e-13)):
         rg = r0.copy(order="F")
         _gpu_track(ring, rg, 1, ring.energy, ring.particle.rest_energy, mode)
         assert scale_rel_diff(rg, ro) <= tol, mode
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_large_ring_100_turns(mode):
+    """100 turns of the large ring: survivors within 1e-9 (scale-relative), the
+    same lost set, and the closed orbit constant is a fixed point."""
+    ring = rings.large_ring()
+    r0 = rings.large_ring_bunch(1024, seed=3)
+    ro = r0.copy(order="F")
+    _, lo = oracle.track(ring, ro, 100, energy=ring.energy, rest_energy=ring.particle.rest_energy,
+                         losses=True)
+    rg = r0.copy(order="F")
+    _, lg, _ = _gpu_track(ring, rg, 100, ring.energy, ring.particle.rest_energy, mode,
+                          losses=True)
+    np.testing.assert_array_equal(lg["islost"], lo["islost"])
+    ok = ~lo["islost"]
+    assert scale_rel_diff(rg[:, ok], ro[:, ok]) <= 1e-9
+
+
+def test_find_orbit6_matches_constant():
+    from at_b200 import physics
+    ring = rings.large_ring()
+    orb = physics.find_orbit6(ring)
+    np.testing.assert_allclose(orb, rings.LARGE_ORBIT, rtol=0, atol=1e-12)
