@@ -367,7 +367,7 @@ def run_b200(a):
     if os.path.exists(prof):
         with open(prof) as f:
             tp = json.load(f)
-        traffic = tp.get("bytes_per_particle_turn", 0.0) * N * T
+        traffic = tp.get("bytes_per_particle_launch", 0.0) * N
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
