@@ -64,6 +64,8 @@ _SIGS = {
     "atb_track_batch": ([_vp, C.POINTER(AtbJobDesc), _i32, _i32, _vp], C.c_int),
     "atb_sync": ([_vp, _vp], C.c_int),
     "atb_fp64_peak": ([C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+    "atb_track_noalloc": ([_i32, _vp, _i64, _vp, _vp, _i32, _vp, _i64, _i32, _i32, _i32, _vp,
+                           _vp, _vp, _vp, _i32, _vp], C.c_int),
 }
 
 

@@ -24,6 +24,7 @@ UNITS = [
     ("track_exact.cu", ["-fmad=false"]),
     ("track_fast.cu", ["-fmad=true"]),
     ("atb200.cu", []),
+    ("atb_noalloc.cu", []),
 ]
 DEPS = ["atb_physics.cuh", "track_kernel.cuh", "atb_kernel_api.h", "atb_table.h"]
 

@@ -297,6 +297,10 @@ int check_status(atb_handle* h, cudaStream_t st) {
 
 }  // namespace
 
+/* lets the other translation units of the library report through
+   atb_last_error() */
+void atb_set_error_message(const char* msg) { g_err = msg ? msg : ""; }
+
 extern "C" {
 
 int atb_version(void) { return 10000; }

@@ -133,6 +133,37 @@ int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int3
  * chains in registers, the denominator of the tracking kernel's roofline. */
 int atb_fp64_peak(int device, double* tflops, double* seconds);
 
+/* No counterpart in the reference.  Tracking for callers that cannot
+ * allocate device memory on their call path: real-time loops (an online model
+ * in an orbit or tune feedback, where cudaMalloc/cudaFree would synchronise
+ * the device and add unbounded latency) and applications whose HBM is owned
+ * by another allocator (a pool that reserved it up front, where an extra
+ * cudaMalloc fails or fragments it).  Same tracking as atb_track_device (whole
+ * turns from element 0, no refpts), on caller-owned device buffers only:
+ * `table` (nwords words) and `elem_off` (nelem+1 offsets) are the compiled
+ * lattice on the device, `elem_off_host` the same offsets in host memory (to
+ * plan the shared-memory segments), `r` the (6, np) particles, and the four
+ * loss-map arrays when `losses` is 1.  Nothing is allocated: the launch lists
+ * live in one fixed array of ATB_NOALLOC_SCRATCH_BYTES inside the library,
+ * held by every GPU that loads it until the process exits.  Limits: at most
+ * ATB_NOALLOC_MAX_PARTICLES particles and ATB_NOALLOC_MAX_SEGS segments of 48 KB
+ * (a lattice table of up to about 48 MB); larger requests return ATB_ERR_ARG.
+ * The first call on a device looks up the array's device address and sets the
+ * kernels' shared-memory limit, so make it before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU (two host threads, or
+ * two streams) race, so serialise them.  Enqueued on `stream` (NULL: the
+ * legacy default stream); returns after the launch completed, with
+ * ATB_ERR_TIMEOUT if a bounded in-kernel wait gave up. */
+#define ATB_NOALLOC_SCRATCH_BYTES (576 * 1024)
+#define ATB_NOALLOC_MAX_TILES 32768
+#define ATB_NOALLOC_MAX_PARTICLES (ATB_NOALLOC_MAX_TILES * 256)
+#define ATB_NOALLOC_MAX_SEGS 1024
+int atb_track_noalloc(int32_t device, const double* table, int64_t nwords,
+                      const uint32_t* elem_off_host, const uint32_t* elem_off, int32_t nelem,
+                      double* r, int64_t np, int32_t nturns, int32_t turn0, int32_t losses,
+                      uint8_t* islost, uint32_t* lturn, uint32_t* lelem, double* lcoord,
+                      int32_t mode, void* stream);
+
 /* Wait for all work enqueued by this handle and return the kernels' status
  * (ATB_ERR_TIMEOUT if a bounded wait gave up). */
 int atb_sync(atb_handle* h, void* stream);
