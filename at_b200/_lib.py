@@ -63,6 +63,10 @@ _SIGS = {
                           _i32, _vp], C.c_int),
     "atb_track_batch": ([_vp, C.POINTER(AtbJobDesc), _i32, _i32, _vp], C.c_int),
     "atb_sync": ([_vp, _vp], C.c_int),
+    "atb_batch_prepare": ([_vp, C.POINTER(AtbJobDesc), _i32, _i32, C.POINTER(_i32)], C.c_int),
+    "atb_batch_capture": ([_vp, _i32], C.c_int),
+    "atb_batch_launch": ([_vp, _i32, _vp], C.c_int),
+    "atb_batch_free": ([_vp, _i32], C.c_int),
     "atb_fp64_peak": ([C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "atb_track_noalloc": ([_i32, _vp, _i64, _vp, _vp, _i32, _vp, _i64, _i32, _i32, _i32, _vp,
                            _vp, _vp, _vp, _i32, _vp], C.c_int),

@@ -1,0 +1,84 @@
+"""Launch-parameter autotuner for the tracking kernel.
+
+The kernel's throughput depends on the threads per block (occupancy versus
+per-block staging cost) and on the shared-memory segment capacity (how many
+blocks fit per SM versus how often a block re-stages the lattice).  The
+autotuner times each candidate on a short sample of the actual workload
+(copies of the particles, a couple of turns) and keeps the fastest; results
+are cached per device, table size and job count in a JSON file
+(``$AT_B200_TUNE_CACHE``, default ``~/.cache/at_b200/autotune.json``).
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+
+THREADS = (128, 256, 384, 512)
+SEG_CAPS = (3072, 4096, 6144)
+
+
+def cache_path() -> str:
+    return os.environ.get("AT_B200_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "at_b200",
+                                       "autotune.json"))
+
+
+def _load_cache() -> dict:
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store_cache(c: dict):
+    p = cache_path()
+    try:
+        os.makedirs(os.path.dirname(p), exist_ok=True)
+        with open(p + ".tmp", "w") as f:
+            json.dump(c, f, indent=1, sort_keys=True)
+        os.replace(p + ".tmp", p)
+    except OSError:
+        pass
+
+
+def cache_key(device_name: str, table_words: int, njobs: int, nparticles: int, mode) -> str:
+    # buckets keep the cache small: table size and particle count to powers of 2
+    tw = 1 << max(0, int(table_words).bit_length() - 1)
+    npb = 1 << max(0, int(nparticles).bit_length() - 1)
+    return "%s|words~%d|jobs=%d|np~%d|%s" % (device_name, tw, njobs, npb, mode)
+
+
+def tune(engine, run_sample, key: str | None = None, candidates=None, use_cache: bool = True):
+    """Pick (threads, seg_cap_words) for ``engine``.
+
+    ``run_sample()`` must launch a short, representative sample of the work
+    and return its device time in seconds (it is called once per candidate
+    after one warm-up call).  The winner is applied with ``engine.set_launch``
+    and returned with the per-candidate timings."""
+    cache = _load_cache() if (use_cache and key) else {}
+    if key and key in cache:
+        best = cache[key]
+        engine.set_launch(threads=best["threads"], seg_cap_words=best["seg_cap"])
+        return best["threads"], best["seg_cap"], {"cached": True}
+    cands = candidates or [(t, c) for t in THREADS for c in SEG_CAPS]
+    timings = {}
+    for t, c in cands:
+        try:
+            engine.set_launch(threads=t, seg_cap_words=c)
+            run_sample()
+            timings[(t, c)] = run_sample()
+        except Exception as exc:  # noqa: BLE001 - a candidate that cannot launch is skipped
+            timings[(t, c)] = float("inf")
+            last = exc
+    best = min(timings, key=timings.get)
+    if timings[best] == float("inf"):
+        raise RuntimeError("no launch configuration could run: %s" % last)
+    engine.set_launch(threads=best[0], seg_cap_words=best[1])
+    if key:
+        cache = _load_cache()
+        cache[key] = {"threads": best[0], "seg_cap": best[1], "seconds": timings[best],
+                      "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+        _store_cache(cache)
+    return best[0], best[1], {"%dx%d" % k: v for k, v in timings.items()}

@@ -76,6 +76,21 @@ struct DevBuf {
     T* as() const { return static_cast<T*>(p); }
 };
 
+/* A prepared batch: its launch lists stay on the device, so launching it is
+   one memset and one kernel, which can be captured in a CUDA graph. */
+struct Batch {
+    bool used = false;
+    int mode = 1;
+    int threads = 256;      /* launch shape fixed when the batch is prepared */
+    int seg_cap = 6144;
+    int smem = 0;
+    int grid = 0;
+    int ntiles = 0;
+    DevBuf jobs, tiles, counter;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
 struct Lattice {
     bool used = false;
     int nelem = 0;
@@ -102,6 +117,7 @@ struct atb_handle {
     DevBuf r, rout, lost, lturn, lelem, lcoord, refpts, jobs, tiles, counter, status, alive,
         moments;
     std::vector<AtbTile> h_tiles;
+    std::vector<struct Batch> batches;
 };
 
 namespace {
@@ -375,6 +391,13 @@ int atb_destroy(atb_handle* h) {
             L.doff.release();
             L.dsegs.release();
         }
+        for (Batch& B : h->batches) {
+            if (B.exec) cudaGraphExecDestroy(B.exec);
+            if (B.graph) cudaGraphDestroy(B.graph);
+            B.jobs.release();
+            B.tiles.release();
+            B.counter.release();
+        }
         for (DevBuf* b : {&h->r, &h->rout, &h->lost, &h->lturn, &h->lelem, &h->lcoord,
                           &h->refpts, &h->jobs, &h->tiles, &h->counter, &h->status, &h->alive,
                           &h->moments})
@@ -388,6 +411,8 @@ int atb_destroy(atb_handle* h) {
 int atb_set_launch(atb_handle* h, int threads, int seg_cap_words, int resident_max_words,
                    int64_t rout_budget_bytes) {
     if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    for (const Batch& B : h->batches)
+        if (B.used) return fail(ATB_ERR_ARG, "free the prepared batches before changing the launch shape");
     if (threads) {
         if (threads < 32 || threads > ATB_MAX_THREADS || threads % 32)
             return fail(ATB_ERR_ARG, "threads per block must be a multiple of 32 in [32, 512]");
@@ -405,8 +430,12 @@ int atb_set_launch(atb_handle* h, int threads, int seg_cap_words, int resident_m
         h->resident_max_words = resident_max_words;
     }
     if (rout_budget_bytes > 0) h->rout_budget = rout_budget_bytes;
-    /* re-plan every lattice for the new capacities */
+    /* re-plan every lattice for the new capacities; prepared batches hold
+       launch lists built on the current plans, so they must be freed first */
+    for (const Batch& B : h->batches)
+        if (B.used) return fail(ATB_ERR_ARG, "free the prepared batches before changing the launch shape");
     DeviceGuard g(h->device);
+    ATB_CUDA(cudaDeviceSynchronize());   /* no launch may still read the old plans */
     for (Lattice& L : h->lats)
         if (L.used) {
             int rc = upload_plan(h, L);
@@ -702,6 +731,154 @@ int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int3
     for (int j : order)
         if (J[j].nturns > 0) make_tiles(h->h_tiles, j, J[j].np, h->threads);
     return launch(h, J, h->h_tiles, smem, grid_max, mode, st);
+}
+
+int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,
+                      int32_t* batch_id) {
+    if (!h || !batch_id || (njobs > 0 && !jobs)) return fail(ATB_ERR_ARG, "NULL argument");
+    if (mode != ATB_MODE_EXACT && mode != ATB_MODE_FAST) return fail(ATB_ERR_ARG, "bad mode");
+    DeviceGuard g(h->device);
+    std::vector<const Lattice*> lats;
+    std::vector<AtbJob> J(njobs > 0 ? njobs : 0);
+    for (int j = 0; j < njobs; ++j) {
+        const atb_job_desc& d = jobs[j];
+        Lattice* L = get_lat(h, d.lattice_id);
+        if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id in batch");
+        if (d.np < 0 || d.nturns < 0 || (d.np > 0 && !d.r))
+            return fail(ATB_ERR_ARG, "invalid batch job");
+        if (d.losses && d.np > 0 && (!d.islost || !d.lturn || !d.lelem || !d.lcoord))
+            return fail(ATB_ERR_ARG, "loss map buffers missing in batch job");
+        lats.push_back(L);
+        std::memset(&J[j], 0, sizeof(AtbJob));
+        fill_job_lattice(J[j], *L, 0, L->nelem);
+        J[j].check_loss = 1;
+        J[j].r = d.r;
+        J[j].np = d.np;
+        J[j].turn0 = d.turn0;
+        J[j].nturns = d.nturns;
+        J[j].losses = d.losses ? 1 : 0;
+        J[j].lost = d.islost;
+        J[j].lturn = d.lturn;
+        J[j].lelem = d.lelem;
+        J[j].lcoord = d.lcoord;
+    }
+    int smem = 0, grid_max = 0;
+    if (!lats.empty()) {
+        int rc = kernel_config(h, lats, mode, &smem, &grid_max);
+        if (rc) return rc;
+    }
+    std::vector<int> order(J.size());
+    for (size_t j = 0; j < J.size(); ++j) order[j] = (int)j;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (double)J[a].nturns * (lats[a]->nwords + 1) * 1.0 >
+               (double)J[b].nturns * (lats[b]->nwords + 1) * 1.0;
+    });
+    std::vector<AtbTile> tiles;
+    for (int j : order)
+        if (J[j].nturns > 0) make_tiles(tiles, j, J[j].np, h->threads);
+    int id = -1;
+    for (int i = 0; i < (int)h->batches.size(); ++i)
+        if (!h->batches[i].used) { id = i; break; }
+    if (id < 0) {
+        h->batches.emplace_back();
+        id = (int)h->batches.size() - 1;
+    }
+    Batch& B = h->batches[id];
+    if (B.jobs.ensure(std::max<size_t>(1, J.size()) * sizeof(AtbJob)) != cudaSuccess ||
+        B.tiles.ensure(std::max<size_t>(1, tiles.size()) * sizeof(AtbTile)) != cudaSuccess ||
+        B.counter.ensure(sizeof(int)) != cudaSuccess)
+        return fail(ATB_ERR_NOMEM, "cudaMalloc(batch lists) failed");
+    if (!J.empty())
+        ATB_CUDA(cudaMemcpy(B.jobs.p, J.data(), J.size() * sizeof(AtbJob), cudaMemcpyHostToDevice));
+    if (!tiles.empty())
+        ATB_CUDA(cudaMemcpy(B.tiles.p, tiles.data(), tiles.size() * sizeof(AtbTile),
+                            cudaMemcpyHostToDevice));
+    B.used = true;
+    B.mode = mode;
+    B.threads = h->threads;
+    B.seg_cap = h->seg_cap_words;
+    B.smem = smem;
+    B.ntiles = (int)tiles.size();
+    B.grid = std::min<int64_t>((int64_t)tiles.size(), std::max(grid_max, 1));
+    *batch_id = id;
+    return ATB_OK;
+}
+
+static Batch* get_batch(atb_handle* h, int id) {
+    if (id < 0 || id >= (int)h->batches.size() || !h->batches[id].used) return nullptr;
+    return &h->batches[id];
+}
+
+static int batch_enqueue(atb_handle* h, Batch& B, cudaStream_t st) {
+    ATB_CUDA(cudaMemsetAsync(B.counter.p, 0, sizeof(int), st));
+    if (B.ntiles == 0) return ATB_OK;
+    if (B.mode == ATB_MODE_EXACT)
+        atb_track_kernel_exact<<<B.grid, B.threads, B.smem, st>>>(
+            B.jobs.as<AtbJob>(), B.tiles.as<AtbTile>(), B.ntiles, B.counter.as<int>(),
+            h->status.as<int>(), B.seg_cap);
+    else
+        atb_track_kernel_fast<<<B.grid, B.threads, B.smem, st>>>(
+            B.jobs.as<AtbJob>(), B.tiles.as<AtbTile>(), B.ntiles, B.counter.as<int>(),
+            h->status.as<int>(), B.seg_cap);
+    ATB_CUDA(cudaGetLastError());
+    return ATB_OK;
+}
+
+int atb_batch_capture(atb_handle* h, int32_t batch_id) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Batch* B = get_batch(h, batch_id);
+    if (!B) return fail(ATB_ERR_ARG, "unknown batch id");
+    DeviceGuard g(h->device);
+    if (B->exec) {
+        cudaGraphExecDestroy(B->exec);
+        B->exec = nullptr;
+    }
+    if (B->graph) {
+        cudaGraphDestroy(B->graph);
+        B->graph = nullptr;
+    }
+    ATB_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = batch_enqueue(h, *B, h->stream);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(ATB_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    B->graph = graph;
+    ATB_CUDA(cudaGraphInstantiate(&B->exec, graph, 0));
+    return ATB_OK;
+}
+
+int atb_batch_launch(atb_handle* h, int32_t batch_id, void* stream) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Batch* B = get_batch(h, batch_id);
+    if (!B) return fail(ATB_ERR_ARG, "unknown batch id");
+    DeviceGuard g(h->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    if (B->exec) {
+        ATB_CUDA(cudaGraphLaunch(B->exec, st));
+        return ATB_OK;
+    }
+    return batch_enqueue(h, *B, st);
+}
+
+int atb_batch_free(atb_handle* h, int32_t batch_id) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Batch* B = get_batch(h, batch_id);
+    if (!B) return fail(ATB_ERR_ARG, "unknown batch id");
+    DeviceGuard g(h->device);
+    cudaStreamSynchronize(h->stream);
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    B->exec = nullptr;
+    B->graph = nullptr;
+    B->jobs.release();
+    B->tiles.release();
+    B->counter.release();
+    B->used = false;
+    return ATB_OK;
 }
 
 int atb_fp64_peak(int device, double* tflops, double* seconds) {

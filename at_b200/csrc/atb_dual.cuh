@@ -1,0 +1,161 @@
+/*
+ * Forward-mode dual numbers for the tangent kernel: a value and K partial
+ * derivatives, with the arithmetic the integrators use (+, -, *, /, sin, tan,
+ * cos, exp).  The pass-method templates in atb_physics.cuh and
+ * track_kernel.cuh run unchanged on this type, which propagates the Jacobian
+ * of every operation exactly (no finite differences).
+ */
+#ifndef ATB_DUAL_CUH
+#define ATB_DUAL_CUH
+
+namespace atb {
+
+template <int K>
+struct Dual {
+    double v;
+    double d[K];
+    __device__ __forceinline__ Dual() {}
+    __device__ __forceinline__ Dual(double x) : v(x) {
+#pragma unroll
+        for (int i = 0; i < K; ++i) d[i] = 0.0;
+    }
+    __device__ __forceinline__ Dual& operator+=(const Dual& o) { return *this = *this + o; }
+    __device__ __forceinline__ Dual& operator-=(const Dual& o) { return *this = *this - o; }
+    __device__ __forceinline__ Dual& operator*=(const Dual& o) { return *this = *this * o; }
+    __device__ __forceinline__ Dual& operator/=(const Dual& o) { return *this = *this / o; }
+
+    friend __device__ __forceinline__ Dual operator+(const Dual& a, const Dual& b) {
+        Dual r;
+        r.v = a.v + b.v;
+#pragma unroll
+        for (int i = 0; i < K; ++i) r.d[i] = a.d[i] + b.d[i];
+        return r;
+    }
+    friend __device__ __forceinline__ Dual operator-(const Dual& a, const Dual& b) {
+        Dual r;
+        r.v = a.v - b.v;
+#pragma unroll
+        for (int i = 0; i < K; ++i) r.d[i] = a.d[i] - b.d[i];
+        return r;
+    }
+    friend __device__ __forceinline__ Dual operator-(const Dual& a) {
+        Dual r;
+        r.v = -a.v;
+#pragma unroll
+        for (int i = 0; i < K; ++i) r.d[i] = -a.d[i];
+        return r;
+    }
+    friend __device__ __forceinline__ Dual operator*(const Dual& a, const Dual& b) {
+        Dual r;
+        r.v = a.v * b.v;
+#pragma unroll
+        for (int i = 0; i < K; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+        return r;
+    }
+    friend __device__ __forceinline__ Dual operator/(const Dual& a, const Dual& b) {
+        Dual r;
+        r.v = a.v / b.v;
+        const double ib = 1.0 / b.v;
+#pragma unroll
+        for (int i = 0; i < K; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
+        return r;
+    }
+    /* mixed forms keep a constant operand from carrying zero derivatives */
+    friend __device__ __forceinline__ Dual operator+(const Dual& a, double b) {
+        Dual r = a;
+        r.v = a.v + b;
+        return r;
+    }
+    friend __device__ __forceinline__ Dual operator+(double a, const Dual& b) { return b + a; }
+    friend __device__ __forceinline__ Dual operator-(const Dual& a, double b) {
+        Dual r = a;
+        r.v = a.v - b;
+        return r;
+    }
+    friend __device__ __forceinline__ Dual operator-(double a, const Dual& b) {
+        Dual r;
+        r.v = a - b.v;
+#pragma unroll
+        for (int i = 0; i < K; ++i) r.d[i] = -b.d[i];
+        return r;
+    }
+    friend __device__ __forceinline__ Dual operator*(const Dual& a, double b) {
+        Dual r;
+        r.v = a.v * b;
+#pragma unroll
+        for (int i = 0; i < K; ++i) r.d[i] = a.d[i] * b;
+        return r;
+    }
+    friend __device__ __forceinline__ Dual operator*(double a, const Dual& b) { return b * a; }
+    friend __device__ __forceinline__ Dual operator/(const Dual& a, double b) {
+        Dual r;
+        r.v = a.v / b;
+        const double ib = 1.0 / b;
+#pragma unroll
+        for (int i = 0; i < K; ++i) r.d[i] = a.d[i] * ib;
+        return r;
+    }
+    friend __device__ __forceinline__ Dual operator/(double a, const Dual& b) {
+        Dual r;
+        r.v = a / b.v;
+        const double s = -r.v / b.v;
+#pragma unroll
+        for (int i = 0; i < K; ++i) r.d[i] = s * b.d[i];
+        return r;
+    }
+};
+
+template <int K>
+__device__ __forceinline__ Dual<K> sin(const Dual<K>& a) {
+    Dual<K> r;
+    double s, c;
+    ::sincos(a.v, &s, &c);
+    r.v = s;
+#pragma unroll
+    for (int i = 0; i < K; ++i) r.d[i] = c * a.d[i];
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ Dual<K> cos(const Dual<K>& a) {
+    Dual<K> r;
+    double s, c;
+    ::sincos(a.v, &s, &c);
+    r.v = c;
+#pragma unroll
+    for (int i = 0; i < K; ++i) r.d[i] = -s * a.d[i];
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ Dual<K> tan(const Dual<K>& a) {
+    Dual<K> r;
+    r.v = ::tan(a.v);
+    const double s = 1.0 + r.v * r.v;
+#pragma unroll
+    for (int i = 0; i < K; ++i) r.d[i] = s * a.d[i];
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ Dual<K> exp(const Dual<K>& a) {
+    Dual<K> r;
+    r.v = ::exp(a.v);
+#pragma unroll
+    for (int i = 0; i < K; ++i) r.d[i] = r.v * a.d[i];
+    return r;
+}
+
+/* the value of a scalar (for comparisons and loss tests) */
+__device__ __forceinline__ double val(double x) { return x; }
+template <int K>
+__device__ __forceinline__ double val(const Dual<K>& x) { return x.v; }
+
+template <class T>
+struct is_dual { static constexpr bool value = false; };
+template <int K>
+struct is_dual<Dual<K>> { static constexpr bool value = true; };
+
+}  // namespace atb
+
+#endif  // ATB_DUAL_CUH

@@ -139,7 +139,15 @@ class Engine:
                                      alive_ptr, moments_ptr, mode_code(mode), stream))
 
     def track_batch(self, jobs: list[dict], mode=None, stream: int | None = None):
-        arr = (_lib.AtbJobDesc * len(jobs))()
+        """One persistent launch over many jobs (dicts with lattice_id, r, np,
+        nturns, optional turn0 and losses=(islost, lturn, lelem, lcoord)
+        device pointers)."""
+        check(lib().atb_track_batch(self.h, self._descs(jobs), len(jobs), mode_code(mode),
+                                    stream))
+
+    @staticmethod
+    def _descs(jobs: list[dict]):
+        arr = (_lib.AtbJobDesc * max(1, len(jobs)))()
         for a, j in zip(arr, jobs):
             a.lattice_id = j["lattice_id"]
             a.nturns = j["nturns"]
@@ -150,7 +158,22 @@ class Engine:
             a.np = j["np"]
             if lp is not None:
                 a.islost, a.lturn, a.lelem, a.lcoord = lp
-        check(lib().atb_track_batch(self.h, arr, len(jobs), mode_code(mode), stream))
+        return arr
+
+    def batch_prepare(self, jobs: list[dict], mode=None) -> int:
+        bid = C.c_int32(-1)
+        check(lib().atb_batch_prepare(self.h, self._descs(jobs), len(jobs), mode_code(mode),
+                                      C.byref(bid)))
+        return bid.value
+
+    def batch_capture(self, bid: int):
+        check(lib().atb_batch_capture(self.h, int(bid)))
+
+    def batch_launch(self, bid: int, stream: int | None = None):
+        check(lib().atb_batch_launch(self.h, int(bid), stream))
+
+    def batch_free(self, bid: int):
+        check(lib().atb_batch_free(self.h, int(bid)))
 
     def sync(self, stream: int | None = None):
         check(lib().atb_sync(self.h, stream))

@@ -192,3 +192,95 @@ def large_ring_bunch(n: int, seed: int = 0) -> np.ndarray:
     """The large-ring bunch: a 6-D Gaussian (sigma = 100 um, 10 urad, 10 um,
     1 urad, 1e-3, 1 mm) around the closed orbit, Fortran-ordered (6, n)."""
     return gaussian(n, LARGE_SIGMA, seed=seed, centre=LARGE_ORBIT)
+
+
+# ---------------------------------------------------------------------------
+# batched variants of the large ring (dynamic-aperture scans)
+# ---------------------------------------------------------------------------
+def large_ring_variant(seed: int, strength_rel: float = 1e-3) -> E.Lattice:
+    """An error-seeded copy of the large ring: misalignments drawn from
+    ``default_rng(seed)`` as in ``large_ring`` and, from the same generator,
+    0.1 % Gaussian errors on every magnet's main strength (dipole and quadrupole
+    gradients, sextupole and octupole coefficients)."""
+    ring = large_ring(seed=seed)
+    rng = np.random.default_rng(seed + 100_000)
+    for e in ring:
+        if e.PassMethod in ("StrMPoleSymplectic4RadPass", "BndMPoleSymplectic4RadPass",
+                            "StrMPoleSymplectic4Pass", "BndMPoleSymplectic4Pass"):
+            b = np.array(e.PolynomB, dtype=np.float64)
+            k = int(np.flatnonzero(b)[-1]) if np.any(b) else 1
+            b[k] *= 1.0 + strength_rel * rng.standard_normal()
+            e.PolynomB = b
+    return ring
+
+
+def da_grid(n: int, seed: int, xmax: float = 4e-3, ymax: float = 2e-3,
+            deltas=(-0.03, 0.0, 0.03), centre=LARGE_ORBIT) -> np.ndarray:
+    """``n`` particles on an x-y dynamic-aperture grid around ``centre``, split
+    over the momentum offsets ``deltas`` (Fortran-ordered (6, n)).  The grid
+    for each delta has ceil(n/len(deltas)) points, row-major over x in
+    [-xmax, xmax] and y in (0, ymax]; ``seed`` jitters it by a tenth of a step
+    so variants do not share identical start points."""
+    rng = np.random.default_rng(seed)
+    per = -(-n // len(deltas))
+    ny = max(1, int(round(np.sqrt(per / 2.0))))
+    nx = -(-per // ny)
+    xs = np.linspace(-xmax, xmax, nx)
+    ys = np.linspace(ymax / ny, ymax, ny)
+    gx, gy = np.meshgrid(xs, ys, indexing="ij")
+    pts = np.stack([gx.ravel(), gy.ravel()])[:, :per]
+    out = np.zeros((6, n))
+    c = np.asarray(centre, dtype=np.float64)
+    k = 0
+    for d in deltas:
+        m = min(per, n - k)
+        jit = 0.1 * rng.standard_normal((2, m)) * np.array([[2 * xmax / max(nx - 1, 1)],
+                                                            [ymax / ny]])
+        out[:, k:k + m] = c[:, None]
+        out[0, k:k + m] += pts[0, :m] + jit[0]
+        out[2, k:k + m] += pts[1, :m] + jit[1]
+        out[4, k:k + m] += d
+        k += m
+    return np.asfortranarray(out)
+
+
+def batch_workload(nvariants: int = 256, first_seed: int = 2, turn_scale: float = 1.0,
+                   seed: int = 0):
+    """The batched-variant workload: for variant i (lattice seed first_seed+i)
+    N_i = round(exp(U[ln 1024, ln 16384])) particles on a DA grid and
+    T_i ~ U{500..5000} turns (times ``turn_scale``, at least 1), all drawn from
+    ``default_rng(seed)``.  Returns a list of (seed, N_i, T_i)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(nvariants):
+        n = int(round(np.exp(rng.uniform(np.log(1024), np.log(16384)))))
+        t = int(rng.integers(500, 5001))
+        out.append((first_seed + i, n, max(1, int(round(t * turn_scale)))))
+    return out
+
+
+def fodo_variant(seed: int, strength_rel: float = 1e-3) -> E.Lattice:
+    """The FODO ring with 0.1 % Gaussian errors (``default_rng(seed)``) on every
+    quadrupole and sextupole strength; each magnet is its own object."""
+    ring = fodo_ring()
+    rng = np.random.default_rng(seed)
+    for e in ring:
+        if e.PassMethod == "StrMPoleSymplectic4Pass":
+            b = np.array(e.PolynomB, dtype=np.float64)
+            k = int(np.flatnonzero(b)[-1])
+            b[k] *= 1.0 + strength_rel * rng.standard_normal()
+            e.PolynomB = b
+    return ring
+
+
+def serving_pool(nfodo: int = 8, nlarge: int = 8):
+    """The 16 lattices of the serving workload: FODO and large-ring copies
+    with different error seeds.  Returns ({name: lattice}, {name: orbit})."""
+    lats, orbits = {}, {}
+    for s in range(nfodo):
+        lats["fodo%d" % s] = fodo_variant(1000 + s)
+        orbits["fodo%d" % s] = np.zeros(6)
+    for s in range(nlarge):
+        lats["large%d" % s] = large_ring_variant(2000 + s)
+        orbits["large%d" % s] = np.asarray(LARGE_ORBIT)
+    return lats, orbits

@@ -1,0 +1,234 @@
+"""Continuous-batching tracking server.
+
+Requests (a lattice, a particle set, a turn count) arrive over time.  The
+server keeps every admitted request's particles in HBM and advances all of
+them together: each round is ONE persistent launch in which every active
+request is a job that tracks its next chunk of turns (the absolute turn
+counter carries over, so the RF phase is the same as in one long call).
+Between rounds, finished requests are retired and waiting requests are
+admitted as HBM budget frees up (arrival order, with smaller requests
+allowed to pass a head that does not fit).  The chunk length is chosen so a
+round costs about ``round_flops`` algorithmic flops, which bounds how long a
+new arrival waits before it joins.
+
+The reference has no serving layer: each request would be one blocking
+``atpass`` call (``pyat/at.c:340-681``); ``serve_sequential`` runs the same
+trace that way through the drop-in entry point, for comparison.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import flops
+from .engine import Engine, mode_code
+from .lattice import compile_lattice
+from .tracking import gpupass
+
+BYTES_PER_PARTICLE = 48 + 1 + 4 + 4 + 48      # state + loss map
+
+
+@dataclass
+class Request:
+    rid: int
+    lattice: str
+    particles: np.ndarray           # (6, N) Fortran order (host)
+    nturns: int
+    arrival: float                  # seconds from the start of the trace
+    kind: str = "bunch"
+    # filled by the server
+    admitted: float | None = None
+    finished: float | None = None
+    result: np.ndarray | None = None
+    losses: dict | None = None
+    done_turns: int = 0
+    dev: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return int(self.particles.shape[1])
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+class TrackingServer:
+    def __init__(self, lattices: dict, hbm_budget_bytes: float = 150e9, device: int = 0,
+                 mode="fast", round_flops: float = 2e12, max_chunk: int = 512):
+        import torch
+
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        self.eng = Engine.get(device)
+        self.mode = mode_code(mode)
+        self.budget = float(hbm_budget_bytes)
+        self.round_flops = float(round_flops)
+        self.max_chunk = int(max_chunk)
+        self.stream = torch.cuda.Stream(self.dev)
+        self.lids = {}
+        self.fpt = {}
+        for name, lat in lattices.items():
+            cl = compile_lattice(lat, getattr(lat, "energy", 0.0),
+                                 getattr(getattr(lat, "particle", None), "rest_energy", 0.0))
+            self.lids[name] = self.eng.upload(cl)
+            self.fpt[name] = flops.flops_per_particle_turn(cl)[0]
+        self.waiting: list[Request] = []
+        self.active: list[Request] = []
+        self.done: list[Request] = []
+        self.used = 0.0
+        self.rounds = 0
+        self.particle_turns = 0
+
+    # -- admission / retirement ------------------------------------------------
+    def _admit(self, now: float):
+        torch = self.torch
+        keep = []
+        for req in self.waiting:
+            need = req.n * BYTES_PER_PARTICLE
+            if self.used + need <= self.budget:
+                n = req.n
+                req.dev = {
+                    "r": torch.from_numpy(np.ascontiguousarray(req.particles.T)).to(self.dev),
+                    "lost": torch.zeros(n, dtype=torch.uint8, device=self.dev),
+                    "lturn": torch.zeros(n, dtype=torch.int32, device=self.dev),
+                    "lelem": torch.zeros(n, dtype=torch.int32, device=self.dev),
+                    "lcoord": torch.zeros((n, 6), dtype=torch.float64, device=self.dev),
+                }
+                self.used += need
+                req.admitted = now
+                self.active.append(req)
+            else:
+                keep.append(req)
+        self.waiting = keep
+
+    def _retire(self, now: float):
+        still = []
+        for req in self.active:
+            if req.done_turns >= req.nturns:
+                d = req.dev
+                req.result = np.asfortranarray(d["r"].cpu().numpy().T)
+                req.losses = {"islost": d["lost"].cpu().numpy().astype(bool),
+                              "turn": d["lturn"].cpu().numpy().view(np.uint32),
+                              "elem": d["lelem"].cpu().numpy().view(np.uint32),
+                              "coord": np.asfortranarray(d["lcoord"].cpu().numpy().T)}
+                req.dev = {}
+                req.finished = now
+                self.used -= req.n * BYTES_PER_PARTICLE
+                self.done.append(req)
+            else:
+                still.append(req)
+        self.active = still
+
+    # -- one round ---------------------------------------------------------------
+    def _round(self):
+        cost = sum(r.n * self.fpt[r.lattice] for r in self.active)
+        chunk = int(max(1, min(self.max_chunk, self.round_flops // max(cost, 1))))
+        jobs = []
+        for req in self.active:
+            t = min(chunk, req.nturns - req.done_turns)
+            d = req.dev
+            jobs.append({"lattice_id": self.lids[req.lattice], "nturns": t,
+                         "turn0": req.done_turns, "r": d["r"].data_ptr(), "np": req.n,
+                         "losses": (d["lost"].data_ptr(), d["lturn"].data_ptr(),
+                                    d["lelem"].data_ptr(), d["lcoord"].data_ptr())})
+            req._step = t
+        with self.torch.cuda.stream(self.stream):
+            self.eng.track_batch(jobs, self.mode, stream=self.stream.cuda_stream)
+        self.stream.synchronize()
+        self.eng.sync(self.stream.cuda_stream)
+        for req in self.active:
+            req.done_turns += req._step
+            self.particle_turns += req.n * req._step
+        self.rounds += 1
+
+    def serve(self, requests: list[Request], time_limit: float | None = None):
+        """Replay a trace: request k becomes visible at ``arrival`` seconds after
+        the start; rounds run back to back while there is work.  Returns the
+        wall time of the whole trace."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(pending) or self.waiting or self.active:
+            now = time.perf_counter() - t0
+            while i < len(pending) and pending[i].arrival <= now:
+                self.waiting.append(pending[i])
+                i += 1
+            self._admit(now)
+            if self.active:
+                self._round()
+                self._retire(time.perf_counter() - t0)
+            elif i < len(pending):
+                time.sleep(max(0.0, min(0.01, pending[i].arrival - now)))
+            if time_limit is not None and time.perf_counter() - t0 > time_limit:
+                break
+        return time.perf_counter() - t0
+
+    def close(self):
+        for lid in self.lids.values():
+            self.eng.free(lid)
+        self.lids = {}
+
+
+def serve_sequential(lattices: dict, requests: list[Request], mode="fast", device: int = 0):
+    """The plain drop-in as a server: one blocking ``gpupass`` call per request,
+    in arrival order (a request waits for all earlier ones)."""
+    pending = sorted(requests, key=lambda r: r.arrival)
+    t0 = time.perf_counter()
+    for req in pending:
+        now = time.perf_counter() - t0
+        if req.arrival > now:
+            time.sleep(req.arrival - now)
+        r = np.asfortranarray(req.particles.copy())
+        req.admitted = time.perf_counter() - t0
+        _, ld = gpupass(lattices[req.lattice], r, req.nturns, losses=True, mode=mode,
+                        gpu_pool=[device])
+        req.result, req.losses = r, ld
+        req.finished = time.perf_counter() - t0
+    return time.perf_counter() - t0
+
+
+def latency_stats(reqs: list[Request]) -> dict:
+    lat = np.array([r.latency for r in reqs if r.finished is not None])
+    if lat.size == 0:
+        return {"completed": 0}
+    return {"completed": int(lat.size), "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
+            "max_s": float(lat.max())}
+
+
+def make_trace(lattice_names: list[str], nreq: int, rate_hz: float = 200.0, seed: int = 0,
+               n_range=(1e3, 2e6), t_range=(100, 10_000), centre_of=None):
+    """A Poisson stream: exponential inter-arrival times at ``rate_hz``; each
+    request picks a lattice uniformly, N and T log-uniform in their ranges and
+    one of three kinds: a dynamic-aperture grid scan (x-y grid x 5 momentum
+    offsets), a momentum-aperture scan (small x-y offset, delta spread over
+    +/-5 %), or a Gaussian bunch.  ``centre_of(name)`` gives each lattice's
+    orbit to centre the particles on."""
+    from . import rings
+
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    reqs = []
+    for k in range(nreq):
+        t += rng.exponential(1.0 / rate_hz)
+        name = lattice_names[int(rng.integers(len(lattice_names)))]
+        n = int(round(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+        nt = int(round(np.exp(rng.uniform(np.log(t_range[0]), np.log(t_range[1])))))
+        kind = ("da", "ma", "bunch")[int(rng.integers(3))]
+        c = np.zeros(6) if centre_of is None else np.asarray(centre_of(name), dtype=np.float64)
+        if kind == "da":
+            p = rings.da_grid(n, seed=k, deltas=(-0.02, -0.01, 0.0, 0.01, 0.02), centre=c)
+        elif kind == "ma":
+            p = np.zeros((6, n))
+            p[:] = c[:, None]
+            p[0] += 1e-5
+            p[2] += 1e-5
+            p[4] += np.linspace(-0.05, 0.05, n)
+            p = np.asfortranarray(p)
+        else:
+            p = rings.gaussian(n, rings.LARGE_SIGMA, seed=k, centre=c)
+        reqs.append(Request(k, name, p, nt, t, kind))
+    return reqs

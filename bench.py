@@ -55,6 +55,8 @@ def _args():
     ap.add_argument("--mode", default="fast", choices=["fast", "exact"])
     ap.add_argument("--threads", type=int, default=0, help="threads per block (0: default)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving trace")
+    ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -362,6 +364,10 @@ def run_b200(a):
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": "failed: %s" % str(exc)[:200]}
 
+    serve = None
+    if world == 1 and not a.no_serve:
+        serve = run_serving(a.serve_requests, mode, local)
+
     traffic = None
     prof = os.path.join(REPO, "profiles", "traffic_%s.json" % a.workload)
     if os.path.exists(prof):
@@ -380,12 +386,46 @@ def run_b200(a):
                          "peak_source": "measured live: atb_fp64_peak DFMA chains on this GPU",
                          "flops_per_particle_turn": fpt, "survivor_particle_turns": survivors},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps, "clocks": clk,
+            "serving": serve,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run_serving(nreq, mode, device):
+    """A finite Poisson trace (200 requests/s) over the 16-lattice pool,
+    served with continuous batching and, for comparison, one blocking drop-in
+    call per request in arrival order.  Sizes are scaled down from the full
+    ranges (N up to 1e5 particles, T up to 1000 turns) so the trace finishes in
+    seconds; the offered load still exceeds the GPU's capacity, so latencies
+    are queue-dominated in both forms."""
+    from at_b200 import rings, serving
+
+    lats, orbits = rings.serving_pool()
+    kw = dict(rate_hz=200.0, seed=7, n_range=(1e3, 1e5), t_range=(100, 1000),
+              centre_of=orbits.get)
+    trace = serving.make_trace(list(lats), nreq, **kw)
+    srv = serving.TrackingServer(lats, hbm_budget_bytes=150e9, device=device, mode=mode)
+    try:
+        wall = srv.serve(trace)
+    finally:
+        srv.close()
+    st = serving.latency_stats(trace)
+    pt = sum(r.n * r.nturns for r in trace)
+    seq_trace = serving.make_trace(list(lats), nreq, **kw)
+    wall_seq = serving.serve_sequential(lats, seq_trace, mode=mode, device=device)
+    sq = serving.latency_stats(seq_trace)
+    same = all(np.array_equal(a.result, b.result, equal_nan=True) for a, b in zip(trace, seq_trace))
+    return {"requests": nreq, "rate_hz": 200.0, "lattices": len(lats),
+            "sizes": "N log-uniform [1e3, 1e5], T log-uniform [100, 1000]",
+            "continuous_batching": dict(st, particle_turns_per_s=pt / wall, rounds=srv.rounds,
+                                        wall_s=wall),
+            "plain_drop_in_sequential": dict(sq, particle_turns_per_s=pt / wall_seq,
+                                             wall_s=wall_seq),
+            "results_identical": bool(same)}
 
 
 def main():

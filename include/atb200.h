@@ -128,6 +128,19 @@ int atb_track_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np, i
 int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,
                     void* stream);
 
+/* Prepared batches: the same jobs as atb_track_batch, with the launch lists
+ * built and uploaded once, so a launch is one memset and one persistent
+ * kernel; atb_batch_capture records that launch as a CUDA graph (on the
+ * handle's stream) and later launches replay the graph.  The job descriptors'
+ * device buffers are used in place at every launch (the particles continue
+ * from where the previous launch left them).  The reference runs each lattice
+ * and particle set as a separate atpass call (pyat/at.c:340-681). */
+int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,
+                      int32_t* batch_id);
+int atb_batch_capture(atb_handle* h, int32_t batch_id);
+int atb_batch_launch(atb_handle* h, int32_t batch_id, void* stream);
+int atb_batch_free(atb_handle* h, int32_t batch_id);
+
 /* Measurement helper with no counterpart in the reference: the FP64 FMA
  * throughput of `device` (TFLOP/s, one FMA = 2 flops) from independent DFMA
  * chains in registers, the denominator of the tracking kernel's roofline. */

@@ -1,0 +1,77 @@
+"""Batched lattice variants (the DA-scan workload) and the autotuner.
+
+CPU: the workload generators are seeded and within their stated ranges.
+GPU: every job of one batched launch (replayed from a CUDA graph) equals the
+same particles tracked alone through the drop-in entry point, bit for bit
+(same kernel and arithmetic; the launch shape does not enter a particle's
+arithmetic).
+"""
+import numpy as np
+import pytest
+
+from at_b200 import rings
+
+
+def test_batch_workload_ranges_and_determinism():
+    w = rings.batch_workload(256)
+    assert w == rings.batch_workload(256)
+    seeds = [s for s, _, _ in w]
+    assert seeds == list(range(2, 258))
+    ns = np.array([n for _, n, _ in w])
+    ts = np.array([t for _, _, t in w])
+    assert ns.min() >= 1024 and ns.max() <= 16384
+    assert ts.min() >= 500 and ts.max() <= 5000
+    assert len(set(ns)) > 100
+
+
+def test_da_grid_layout():
+    r = rings.da_grid(1000, seed=4)
+    assert r.shape == (6, 1000) and r.flags.f_contiguous
+    d = np.round(r[4] - rings.LARGE_ORBIT[4], 12)
+    assert set(np.unique(d)) == {-0.03, 0.0, 0.03}
+    assert np.all(r[2] - rings.LARGE_ORBIT[2] > 0)
+
+
+def test_variant_changes_only_errors():
+    a = rings.large_ring_variant(2)
+    b = rings.large_ring_variant(3)
+    assert len(a) == len(b) == len(rings.large_ring())
+    assert [e.PassMethod for e in a] == [e.PassMethod for e in b]
+    qa = [e for e in a if e.FamName == "QF"][0]
+    qb = [e for e in b if e.FamName == "QF"][0]
+    assert qa.PolynomB[1] != qb.PolynomB[1]
+    assert abs(qa.PolynomB[1] / rings.LARGE_KF - 1) < 1e-2
+    assert not np.array_equal(qa.T1, qb.T1)
+
+
+@pytest.mark.gpu
+def test_batched_variants_equal_individual_runs(tmp_path, monkeypatch):
+    monkeypatch.setenv("AT_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    from at_b200 import tracking
+    from at_b200.batch import BatchTracker
+
+    work = rings.batch_workload(6, turn_scale=0.006, seed=1)
+    lats = [rings.large_ring_variant(s) for s, _, _ in work]
+    parts = [rings.da_grid(max(200, n // 10), seed=s) for s, n, _ in work]
+    turns = [t for _, _, t in work]
+    bt = BatchTracker(lats, parts, turns, mode="fast", tune=True, graph=True)
+    try:
+        assert bt.tuning is not None
+        bt.run()
+        res1 = bt.results()
+        bt.reset()
+        bt.run()                                   # graph replay
+        res2 = bt.results()
+    finally:
+        bt.close()
+    for (ra, la), (rb, lb) in zip(res1, res2):
+        np.testing.assert_array_equal(ra, rb)
+        np.testing.assert_array_equal(la["islost"], lb["islost"])
+    for (r, ld), lat, p, t in zip(res1, lats, parts, turns):
+        ref = p.copy(order="F")
+        _, lr = tracking.gpupass(lat, ref, t, losses=True, mode="fast")
+        np.testing.assert_array_equal(r, ref)
+        for k in ("islost", "turn", "elem", "coord"):
+            np.testing.assert_array_equal(ld[k], lr[k])
+    assert any(ld["islost"].any() for _, ld in res1)       # +/-3 % particles get lost
+    assert (tmp_path / "tune.json").exists()
