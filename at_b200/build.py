@@ -1,8 +1,9 @@
 """Build the CUDA engine ``at_b200/libatb200.so`` in-tree for sm_100a.
 
-The two kernel translation units are compiled with different contraction
-flags (``-fmad=false`` for the exact-order kernel), then linked with the host
-runtime into one shared library exporting the C ABI of ``include/atb200.h``.
+The kernel translation units are compiled with different contraction flags
+(``-fmad=false`` for the exact-order tracking kernel and the tangent kernel),
+then linked with the host runtime into one shared library exporting the C ABI
+of ``include/atb200.h``.
 """
 from __future__ import annotations
 
@@ -23,10 +24,12 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + CSRC, 
 UNITS = [
     ("track_exact.cu", ["-fmad=false"]),
     ("track_fast.cu", ["-fmad=true"]),
+    ("tangent.cu", ["-fmad=false"]),
     ("atb200.cu", []),
     ("atb_noalloc.cu", []),
 ]
-DEPS = ["atb_physics.cuh", "track_kernel.cuh", "atb_kernel_api.h", "atb_table.h"]
+DEPS = ["atb_physics.cuh", "atb_dual.cuh", "track_kernel.cuh", "tangent_kernel.cuh",
+        "atb_kernel_api.h", "atb_table.h"]
 
 
 def nvcc() -> str:

@@ -36,6 +36,7 @@ extern "C" __global__ void atb_track_kernel_exact(const AtbJob*, const AtbTile*,
                                                   int);
 extern "C" __global__ void atb_track_kernel_fast(const AtbJob*, const AtbTile*, int, int*, int*,
                                                  int);
+extern "C" __global__ void atb_tangent_kernel(const AtbTangent);
 
 namespace {
 
@@ -96,6 +97,7 @@ struct Lattice {
     int nelem = 0;
     int64_t nwords = 0;
     std::vector<uint32_t> off;
+    std::vector<uint64_t> hdr;  /* every element's header word              */
     std::vector<AtbSeg> segs;   /* pipelined segments (empty when resident) */
     bool resident = false;
     int plan_cap = 0;           /* seg capacity used to build the plan      */
@@ -115,7 +117,8 @@ struct atb_handle {
     int64_t rout_budget = 4LL << 30;
     std::vector<Lattice> lats;
     DevBuf r, rout, lost, lturn, lelem, lcoord, refpts, jobs, tiles, counter, status, alive,
-        moments;
+        moments, tan_pelem, tan_porder;
+    std::vector<int32_t> h_pelem;
     std::vector<AtbTile> h_tiles;
     std::vector<struct Batch> batches;
 };
@@ -476,6 +479,8 @@ int atb_lattice_upload(atb_handle* h, const double* words, int64_t nwords,
     L.nwords = nwords;
     L.off.assign(elem_off, elem_off + nelem + 1);
     if (nelem == 0) L.off.assign(1, 0u);
+    L.hdr.resize(nelem);
+    for (int i = 0; i < nelem; ++i) std::memcpy(&L.hdr[i], words + elem_off[i], 8);
     size_t wbytes = (size_t)(nwords + 2) * 8;
     if (L.words.ensure(wbytes) != cudaSuccess || L.doff.ensure(L.off.size() * 4) != cudaSuccess) {
         L.used = false;
@@ -501,6 +506,7 @@ int atb_lattice_update(atb_handle* h, int32_t id, const double* words, int64_t n
     DeviceGuard g(h->device);
     ATB_CUDA(cudaStreamSynchronize(h->stream));
     if (nwords) ATB_CUDA(cudaMemcpy(L->words.p, words, nwords * 8, cudaMemcpyHostToDevice));
+    for (int i = 0; i < L->nelem; ++i) std::memcpy(&L->hdr[i], words + L->off[i], 8);
     return ATB_OK;
 }
 
@@ -683,6 +689,77 @@ int atb_track_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t n
     /* pageable-source copies of the launch lists are staged before
        cudaMemcpyAsync returns, so the host vectors may be reused at once */
     return launch(h, jobs, h->h_tiles, smem, grid_max, mode, st);
+}
+
+int atb_tangent_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t nturns,
+                       int32_t turn0, const int32_t* param_elem, const int32_t* param_order,
+                       const double* param_value, int32_t nparam, double* jac, double* grad,
+                       uint8_t* islost, void* stream) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Lattice* L = get_lat(h, id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    if (np < 0 || nturns < 0 || nparam < 0) return fail(ATB_ERR_ARG, "negative size");
+    if (np > 0 && (!r || !jac)) return fail(ATB_ERR_ARG, "r or jac is NULL");
+    if (nparam > 0 && (!param_elem || !param_order || !param_value || (np > 0 && !grad)))
+        return fail(ATB_ERR_ARG, "parameter arrays missing");
+    /* validate the differentiated strengths against the element headers */
+    h->h_pelem.assign((size_t)std::max(L->nelem, 1), -1);
+    for (int q = 0; q < nparam; ++q) {
+        const int e = param_elem[q];
+        const int k = param_order[q];
+        if (e < 0 || e >= L->nelem) return fail(ATB_ERR_ARG, "parameter element out of range");
+        if (h->h_pelem[e] >= 0)
+            return fail(ATB_ERR_ARG, "element " + std::to_string(e) + " has two parameters");
+        const uint64_t hd = L->hdr[e];
+        const int op = (int)((hd >> ATB_H_OP_SHIFT) & ATB_H_OP_MASK);
+        const int mo = (int)((hd >> ATB_H_MO_SHIFT) & ATB_H_MO_MASK);
+        const uint32_t fl = (uint32_t)((hd >> ATB_H_FL_SHIFT) & ATB_H_FL_MASK);
+        if (op != ATB_OP_STRMPOLE && op != ATB_OP_STRMPOLE_RAD && op != ATB_OP_BNDMPOLE &&
+            op != ATB_OP_BNDMPOLE_RAD && op != ATB_OP_THINMPOLE)
+            return fail(ATB_ERR_ARG, "element " + std::to_string(e) + " has no PolynomB");
+        if (k < 1 || k > mo)
+            return fail(ATB_ERR_ARG, "PolynomB order " + std::to_string(k) +
+                                         " outside [1, MaxOrder] of element " +
+                                         std::to_string(e));
+        if (k == 1 && (fl & (ATB_F_FQ_IN_LIN | ATB_F_FQ_OUT_LIN)))
+            return fail(ATB_ERR_ARG, "element " + std::to_string(e) +
+                                         ": linear quadrupole-fringe maps are not differentiated");
+        h->h_pelem[e] = q;
+    }
+    if (np == 0) return ATB_OK;
+    DeviceGuard g(h->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    AtbTangent A;
+    std::memset(&A, 0, sizeof(A));
+    A.table = L->words.as<double>();
+    A.elem_off = L->doff.as<uint32_t>();
+    A.nelem = L->nelem;
+    A.nturns = nturns;
+    A.turn0 = turn0;
+    A.nparam = nparam;
+    A.r = r;
+    A.np = np;
+    if (nparam > 0) {
+        if (h->tan_pelem.ensure(h->h_pelem.size() * 4) != cudaSuccess ||
+            h->tan_porder.ensure((size_t)nparam * 4) != cudaSuccess)
+            return fail(ATB_ERR_NOMEM, "cudaMalloc(parameter map) failed");
+        /* pageable sources are staged before cudaMemcpyAsync returns */
+        ATB_CUDA(cudaMemcpyAsync(h->tan_pelem.p, h->h_pelem.data(), h->h_pelem.size() * 4,
+                                 cudaMemcpyHostToDevice, st));
+        ATB_CUDA(cudaMemcpyAsync(h->tan_porder.p, param_order, (size_t)nparam * 4,
+                                 cudaMemcpyHostToDevice, st));
+        A.pelem = h->tan_pelem.as<int32_t>();
+        A.porder = h->tan_porder.as<int32_t>();
+        A.pvalue = param_value;
+    }
+    A.jac = jac;
+    A.grad = grad;
+    A.lost = islost;
+    const long long blocks = (np + ATB_TANGENT_THREADS - 1) / ATB_TANGENT_THREADS;
+    if (blocks > 0x7fffffffLL) return fail(ATB_ERR_ARG, "too many particles");
+    atb_tangent_kernel<<<(unsigned)blocks, ATB_TANGENT_THREADS, 0, st>>>(A);
+    ATB_CUDA(cudaGetLastError());
+    return ATB_OK;
 }
 
 int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,

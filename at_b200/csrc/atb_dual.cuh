@@ -10,6 +10,12 @@
 
 namespace atb {
 
+/* the double overloads stay visible next to the dual ones below */
+using ::sin;
+using ::cos;
+using ::tan;
+using ::exp;
+
 template <int K>
 struct Dual {
     double v;
@@ -23,6 +29,10 @@ struct Dual {
     __device__ __forceinline__ Dual& operator-=(const Dual& o) { return *this = *this - o; }
     __device__ __forceinline__ Dual& operator*=(const Dual& o) { return *this = *this * o; }
     __device__ __forceinline__ Dual& operator/=(const Dual& o) { return *this = *this / o; }
+    __device__ __forceinline__ Dual& operator+=(double o) { v += o; return *this; }
+    __device__ __forceinline__ Dual& operator-=(double o) { v -= o; return *this; }
+    __device__ __forceinline__ Dual& operator*=(double o) { return *this = *this * o; }
+    __device__ __forceinline__ Dual& operator/=(double o) { return *this = *this / o; }
 
     friend __device__ __forceinline__ Dual operator+(const Dual& a, const Dual& b) {
         Dual r;
@@ -105,11 +115,12 @@ struct Dual {
     }
 };
 
+/* sin and cos are called separately (not sincos) so the value is exactly
+ * the one the double kernels compute */
 template <int K>
 __device__ __forceinline__ Dual<K> sin(const Dual<K>& a) {
     Dual<K> r;
-    double s, c;
-    ::sincos(a.v, &s, &c);
+    const double s = ::sin(a.v), c = ::cos(a.v);
     r.v = s;
 #pragma unroll
     for (int i = 0; i < K; ++i) r.d[i] = c * a.d[i];
@@ -119,8 +130,7 @@ __device__ __forceinline__ Dual<K> sin(const Dual<K>& a) {
 template <int K>
 __device__ __forceinline__ Dual<K> cos(const Dual<K>& a) {
     Dual<K> r;
-    double s, c;
-    ::sincos(a.v, &s, &c);
+    const double s = ::sin(a.v), c = ::cos(a.v);
     r.v = c;
 #pragma unroll
     for (int i = 0; i < K; ++i) r.d[i] = -s * a.d[i];

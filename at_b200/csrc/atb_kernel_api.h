@@ -61,4 +61,26 @@ typedef struct AtbTile {
     int64_t first;
 } AtbTile;
 
+/* Tangent (forward-mode) tracking: one launch over np particles of one
+ * lattice, with the Jacobian of the final coordinates with respect to the
+ * initial ones and to nparam multipole strengths. */
+#define ATB_TANGENT_THREADS 128
+
+typedef struct AtbTangent {
+    const double* table;        /* element table words                      */
+    const uint32_t* elem_off;   /* word offset of every element (+ end)     */
+    int32_t nelem;
+    int32_t nturns;
+    int32_t turn0;
+    int32_t nparam;
+    double* r;                  /* (6, np) state, updated in place          */
+    int64_t np;
+    const int32_t* pelem;       /* per element: parameter index or -1       */
+    const int32_t* porder;      /* per parameter: PolynomB order            */
+    const double* pvalue;       /* per parameter: strength used             */
+    double* jac;                /* (np, 6, 6): d r_i / d r0_j               */
+    double* grad;               /* (nparam, 6, np): d r_i / d K_q           */
+    uint8_t* lost;              /* optional (np): 1 if the particle was lost */
+} AtbTangent;
+
 #endif /* ATB_KERNEL_API_H */

@@ -20,21 +20,28 @@
 #define ATB_PHYSICS_CUH
 
 #include "atb_table.h"
+#include "atb_dual.cuh"
 
 namespace atb {
 
-struct P6 {
-    double x, px, y, py, dp, ct;
+/* The particle state.  T is double in the tracking kernels and a dual number
+ * (value + partial derivatives) in the tangent kernel; every function below
+ * is a template on T so both run the same expressions. */
+template <class T>
+struct P6T {
+    T x, px, y, py, dp, ct;
 };
+using P6 = P6T<double>;
 
 #define ATB_C0 2.99792458e8
 
 __device__ __forceinline__ double inf_d() { return __longlong_as_double(0x7ff0000000000000LL); }
 __device__ __forceinline__ double nan_d() { return __longlong_as_double(0x7ff8000000000000LL); }
 
-__device__ __forceinline__ bool all_finite(const P6& r) {
-    return isfinite(r.x) && isfinite(r.px) && isfinite(r.y) && isfinite(r.py) &&
-           isfinite(r.dp) && isfinite(r.ct);
+template <class T>
+__device__ __forceinline__ bool all_finite(const P6T<T>& r) {
+    return isfinite(val(r.x)) && isfinite(val(r.px)) && isfinite(val(r.y)) &&
+           isfinite(val(r.py)) && isfinite(val(r.dp)) && isfinite(val(r.ct));
 }
 
 /* Fast-mode reciprocal of a positive operand near 1: the hardware estimate
@@ -51,17 +58,19 @@ __device__ __forceinline__ double rcp_nr(double d) {
 }
 
 /* atlalib.c:50-57 ATaddvv */
-__device__ __forceinline__ void add_t(P6& r, const double* t) {
+template <class T>
+__device__ __forceinline__ void add_t(P6T<T>& r, const double* t) {
     r.x += t[0]; r.px += t[1]; r.y += t[2]; r.py += t[3]; r.dp += t[4]; r.ct += t[5];
 }
 
 /* atlalib.c:17-32 ATmultmv: temp[i] = 0 + sum_j A[i+6j]*r[j], j ascending */
-__device__ __forceinline__ void mult_dense(P6& r, const double* A) {
-    const double r0 = r.x, r1 = r.px, r2 = r.y, r3 = r.py, r4 = r.dp, r5 = r.ct;
-    double t[6];
+template <class T>
+__device__ __forceinline__ void mult_dense(P6T<T>& r, const double* A) {
+    const T r0 = r.x, r1 = r.px, r2 = r.y, r3 = r.py, r4 = r.dp, r5 = r.ct;
+    T t[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        double s = 0.0;
+        T s = 0.0;
         s += A[i] * r0;
         s += A[i + 6] * r1;
         s += A[i + 12] * r2;
@@ -77,8 +86,9 @@ __device__ __forceinline__ void mult_dense(P6& r, const double* A) {
  * its zero terms dropped, which is value-identical for finite coordinates.
  * A non-finite coordinate takes the full sum with the zero entries written
  * out, so 0*inf -> NaN propagates exactly as in the reference. */
-__device__ __forceinline__ void mult_tilt(P6& r, const double* m) {
-    const double x = r.x, px = r.px, y = r.y, py = r.py, d = r.dp, c = r.ct;
+template <class T>
+__device__ __forceinline__ void mult_tilt(P6T<T>& r, const double* m) {
+    const T x = r.x, px = r.px, y = r.y, py = r.py, d = r.dp, c = r.ct;
     if (!all_finite(r)) {
         const double z = 0.0;
         r.x = 0.0 + m[0] * x + z * px + m[1] * y + z * py + z * d + z * c;
@@ -95,26 +105,30 @@ __device__ __forceinline__ void mult_tilt(P6& r, const double* m) {
     r.py = m[6] * px + m[7] * py;
 }
 
-__device__ __forceinline__ void mult_r(P6& r, const double* blk, bool dense) {
+template <class T>
+__device__ __forceinline__ void mult_r(P6T<T>& r, const double* blk, bool dense) {
     if (dense) mult_dense(r, blk); else mult_tilt(r, blk);
 }
 
 /* atlalib.c:169-175 checkiflostRectangularAp */
-__device__ __forceinline__ void check_rect(P6& r, const double* lim) {
-    if (r.x < lim[0] || r.x > lim[1]) r.ct = inf_d();
-    else if (r.y < lim[2] || r.y > lim[3]) r.ct = inf_d();
+template <class T>
+__device__ __forceinline__ void check_rect(P6T<T>& r, const double* lim) {
+    const double x = val(r.x), y = val(r.y);
+    if (x < lim[0] || x > lim[1]) r.ct = T(inf_d());
+    else if (y < lim[2] || y > lim[3]) r.ct = T(inf_d());
 }
 
 /* atlalib.c:185-190 checkiflostEllipticalAp */
-__device__ __forceinline__ void check_ellip(P6& r, const double* ax) {
-    double xn = r.x / ax[0];
-    double zn = r.y / ax[1];
-    if ((xn * xn + zn * zn) >= 1) r.ct = inf_d();
+template <class T>
+__device__ __forceinline__ void check_ellip(P6T<T>& r, const double* ax) {
+    double xn = val(r.x) / ax[0];
+    double zn = val(r.y) / ax[1];
+    if ((xn * xn + zn * zn) >= 1) r.ct = T(inf_d());
 }
 
 /* atlalib.c:70-75 ATChangePRef */
-template <bool FAST>
-__device__ __forceinline__ void change_pref(P6& r, double s) {
+template <bool FAST, class T>
+__device__ __forceinline__ void change_pref(P6T<T>& r, double s) {
     r.px /= s;
     r.py /= s;
     r.dp = (r.dp + 1.0 - s) / s;
@@ -122,17 +136,17 @@ __device__ __forceinline__ void change_pref(P6& r, double s) {
 
 /* atlalib.c:59-68 ATdrift6 == driftkickrad.c:36-45 drift6 == diff_drift.c:30-43
  * (without the diffusion-matrix branch) */
-template <bool FAST>
-__device__ __forceinline__ void drift6(P6& r, double L) {
-    if (FAST) {
+template <bool FAST, class T>
+__device__ __forceinline__ void drift6(P6T<T>& r, double L) {
+    if constexpr (FAST) {
         double pn = 1.0 / (1.0 + r.dp);
         double nl = L * pn;
         r.x += nl * r.px;
         r.y += nl * r.py;
         r.ct += (0.5 * nl * pn) * (r.px * r.px + r.py * r.py);
     } else {
-        double pn = 1 / (1 + r.dp);
-        double nl = L * pn;
+        T pn = 1 / (1 + r.dp);
+        T nl = L * pn;
         r.x += nl * r.px;
         r.y += nl * r.py;
         r.ct += nl * pn * (r.px * r.px + r.py * r.py) / 2;
@@ -140,53 +154,84 @@ __device__ __forceinline__ void drift6(P6& r, double L) {
 }
 
 /* driftkick.c:37-48 fastdrift.  FAST: c2 = NormL/(2(1+delta)) precomputed. */
-template <bool FAST>
-__device__ __forceinline__ void fastdrift(P6& r, double nl, double c2) {
+template <bool FAST, class T>
+__device__ __forceinline__ void fastdrift(P6T<T>& r, const T& nl, const T& c2) {
     r.x += nl * r.px;
     r.y += nl * r.py;
-    if (FAST) r.ct += c2 * (r.px * r.px + r.py * r.py);
+    if constexpr (FAST) r.ct += c2 * (r.px * r.px + r.py * r.py);
     else r.ct += nl * (r.px * r.px + r.py * r.py) / (2 * (1 + r.dp));
 }
 
 /* The Horner recursion shared by every multipole kick
  * (driftkick.c:51-115, diff_str_kick.c:33-40, diff_bnd_kick.c:40-47):
  * Re + i Im = sum_n (B_n + i A_n)(x + i y)^n, highest order first. */
-template <int MO>
-__device__ __forceinline__ void horner_fixed(const double* A, const double* B, double x, double y,
-                                             double& re, double& im) {
+template <int MO, class T>
+__device__ __forceinline__ void horner_fixed(const double* A, const double* B, const T& x,
+                                             const T& y, T& re, T& im) {
     re = B[MO];
     im = A[MO];
 #pragma unroll
     for (int i = MO - 1; i >= 0; --i) {
-        double ret = re * x - im * y + B[i];
+        T ret = re * x - im * y + B[i];
         im = im * x + re * y + A[i];
         re = ret;
     }
 }
 
-__device__ __forceinline__ void horner_dyn(const double* A, const double* B, int mo, double x,
-                                           double y, double& re, double& im) {
+template <class T>
+__device__ __forceinline__ void horner_dyn(const double* A, const double* B, int mo, const T& x,
+                                           const T& y, T& re, T& im) {
     re = B[mo];
     im = A[mo];
     for (int i = mo - 1; i >= 0; --i) {
-        double ret = re * x - im * y + B[i];
+        T ret = re * x - im * y + B[i];
         im = im * x + re * y + A[i];
         re = ret;
+    }
+}
+
+/* Tangent kernel only: the explicit partial of the field with respect to the
+ * differentiated coefficient B_k, d(Re + i Im)/dB_k = (x + i y)^k, added to
+ * the last derivative slot (the parameter direction). */
+template <class T>
+__device__ __forceinline__ void seed_coef(double x, double y, int k, T& re, T& im) {
+    if constexpr (is_dual<T>::value) {
+        if (k < 0) return;
+        double zr = 1.0, zi = 0.0;
+        for (int i = 0; i < k; ++i) {
+            const double t = zr * x - zi * y;
+            zi = zr * y + zi * x;
+            zr = t;
+        }
+        constexpr int K = sizeof(re.d) / sizeof(double);
+        re.d[K - 1] += zr;
+        im.d[K - 1] += zi;
     }
 }
 
 /* Coefficient holder: for MO >= 0 the coefficients are copied into
  * registers once per element; MO < 0 reads them (broadcast) from the staged
- * table on every kick. */
+ * table on every kick.  set_param() (tangent kernel only) replaces B_k by a
+ * runtime strength and marks it as the differentiated parameter. */
 template <int MO>
 struct Poly {
     double a[MO + 1], b[MO + 1];
+    int sk;
     __device__ __forceinline__ void load(const double* A, const double* B, int) {
 #pragma unroll
         for (int i = 0; i <= MO; ++i) { a[i] = A[i]; b[i] = B[i]; }
+        sk = -1;
     }
-    __device__ __forceinline__ void field(double x, double y, double& re, double& im) const {
+    __device__ __forceinline__ void set_param(int k, double v) {
+#pragma unroll
+        for (int i = 0; i <= MO; ++i)
+            if (i == k) b[i] = v;
+        sk = k;
+    }
+    template <class T>
+    __device__ __forceinline__ void field(const T& x, const T& y, T& re, T& im) const {
         horner_fixed<MO>(a, b, x, y, re, im);
+        seed_coef(val(x), val(y), sk, re, im);
     }
 };
 
@@ -195,28 +240,43 @@ struct Poly<-1> {
     const double* a;
     const double* b;
     int mo;
+    int sk;
+    double kv;
     __device__ __forceinline__ void load(const double* A, const double* B, int m) {
-        a = A; b = B; mo = m;
+        a = A; b = B; mo = m; sk = -1; kv = 0.0;
     }
-    __device__ __forceinline__ void field(double x, double y, double& re, double& im) const {
-        horner_dyn(a, b, mo, x, y, re, im);
+    __device__ __forceinline__ void set_param(int k, double v) { sk = k; kv = v; }
+    template <class T>
+    __device__ __forceinline__ void field(const T& x, const T& y, T& re, T& im) const {
+        if constexpr (is_dual<T>::value) {
+            re = (sk == mo) ? kv : b[mo];
+            im = a[mo];
+            for (int i = mo - 1; i >= 0; --i) {
+                T ret = re * x - im * y + ((i == sk) ? kv : b[i]);
+                im = im * x + re * y + a[i];
+                re = ret;
+            }
+            seed_coef(val(x), val(y), sk, re, im);
+        } else {
+            horner_dyn(a, b, mo, x, y, re, im);
+        }
     }
 };
 
 /* driftkick.c:92-115 strthinkick */
-template <class PL>
-__device__ __forceinline__ void strthinkick(P6& r, const PL& pl, double L) {
-    double re, im;
+template <class PL, class T>
+__device__ __forceinline__ void strthinkick(P6T<T>& r, const PL& pl, double L) {
+    T re, im;
     pl.field(r.x, r.y, re, im);
     r.px -= L * re;
     r.py += L * im;
 }
 
 /* driftkick.c:51-89 bndthinkick; lirho = L*irho folded on the host */
-template <class PL>
-__device__ __forceinline__ void bndthinkick(P6& r, const PL& pl, double L, double irho,
+template <class PL, class T>
+__device__ __forceinline__ void bndthinkick(P6T<T>& r, const PL& pl, double L, double irho,
                                             double lirho) {
-    double re, im;
+    T re, im;
     pl.field(r.x, r.y, re, im);
     r.px -= L * (re - (r.dp - r.x * irho) * irho);
     r.py += L * im;
@@ -226,12 +286,12 @@ __device__ __forceinline__ void bndthinkick(P6& r, const PL& pl, double L, doubl
 /* Radiating kicks.  ``pn`` carries 1/(1+delta) between steps in FAST mode. */
 
 /* diff_str_kick.c:19-83 with B2perp of diff_str_kick.c:1-17 (bdiff == NULL) */
-template <bool FAST, class PL>
-__device__ __forceinline__ void str_kick_rad(P6& r, const PL& pl, double L, double radc,
-                                             double& pn) {
-    double re, im;
+template <bool FAST, class PL, class T>
+__device__ __forceinline__ void str_kick_rad(P6T<T>& r, const PL& pl, double L, double radc,
+                                             T& pn) {
+    T re, im;
     pl.field(r.x, r.y, re, im);
-    if (FAST) {
+    if constexpr (FAST) {
         double xpr = r.px * pn;
         double ypr = r.py * pn;
         double s = xpr * xpr + ypr * ypr;
@@ -246,13 +306,13 @@ __device__ __forceinline__ void str_kick_rad(P6& r, const PL& pl, double L, doub
         r.px = xpr * opd - L * re;
         r.py = ypr * opd + L * im;
     } else {
-        double p_norm = 1.0 / (1.0 + r.dp);
-        double xpr = r.px * p_norm;
-        double ypr = r.py * p_norm;
-        double v_norm2 = 1.0 / (1.0 + xpr * xpr + ypr * ypr);
-        double bx = im, by = re;
-        double b2p = (by * by + bx * bx + (bx * ypr - by * xpr) * (bx * ypr - by * xpr)) * v_norm2;
-        double factor = (1.0 + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
+        T p_norm = 1.0 / (1.0 + r.dp);
+        T xpr = r.px * p_norm;
+        T ypr = r.py * p_norm;
+        T v_norm2 = 1.0 / (1.0 + xpr * xpr + ypr * ypr);
+        T bx = im, by = re;
+        T b2p = (by * by + bx * bx + (bx * ypr - by * xpr) * (bx * ypr - by * xpr)) * v_norm2;
+        T factor = (1.0 + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
         r.dp -= radc * b2p * factor;
         p_norm = 1.0 / (1.0 + r.dp);
         r.px = xpr / p_norm;
@@ -263,12 +323,12 @@ __device__ __forceinline__ void str_kick_rad(P6& r, const PL& pl, double L, doub
 }
 
 /* diff_bnd_kick.c:101-174 with its B2perp (:85-99), bdiff == NULL */
-template <bool FAST, class PL>
-__device__ __forceinline__ void bnd_kick_rad(P6& r, const PL& pl, double L, double irho,
-                                             double lirho, double radc, double& pn) {
-    double re, im;
+template <bool FAST, class PL, class T>
+__device__ __forceinline__ void bnd_kick_rad(P6T<T>& r, const PL& pl, double L, double irho,
+                                             double lirho, double radc, T& pn) {
+    T re, im;
     pl.field(r.x, r.y, re, im);
-    if (FAST) {
+    if constexpr (FAST) {
         double xpr = r.px * pn;
         double ypr = r.py * pn;
         double hx = 1.0 + r.x * irho;
@@ -287,17 +347,17 @@ __device__ __forceinline__ void bnd_kick_rad(P6& r, const PL& pl, double L, doub
         r.py = ypr * opd + L * im;
         r.ct += lirho * r.x;
     } else {
-        double p_norm = 1.0 / (1.0 + r.dp);
-        double x = r.x;
-        double xpr = r.px * p_norm;
-        double ypr = r.py * p_norm;
-        double bx = im, by = re + irho;
-        double v_norm2 = 1.0 / ((1.0 + x * irho) * (1.0 + x * irho) + xpr * xpr + ypr * ypr);
-        double b2p = ((by * (1 + x * irho)) * (by * (1 + x * irho)) +
-                      (bx * (1 + x * irho)) * (bx * (1 + x * irho)) +
-                      (bx * ypr - by * xpr) * (bx * ypr - by * xpr)) * v_norm2;
-        double factor = (1.0 + x * irho + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
-        double dp_0 = r.dp;
+        T p_norm = 1.0 / (1.0 + r.dp);
+        T x = r.x;
+        T xpr = r.px * p_norm;
+        T ypr = r.py * p_norm;
+        T bx = im, by = re + irho;
+        T v_norm2 = 1.0 / ((1.0 + x * irho) * (1.0 + x * irho) + xpr * xpr + ypr * ypr);
+        T b2p = ((by * (1 + x * irho)) * (by * (1 + x * irho)) +
+                 (bx * (1 + x * irho)) * (bx * (1 + x * irho)) +
+                 (bx * ypr - by * xpr) * (bx * ypr - by * xpr)) * v_norm2;
+        T factor = (1.0 + x * irho + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
+        T dp_0 = r.dp;
         r.dp -= radc * b2p * factor;
         p_norm = 1.0 / (1.0 + r.dp);
         r.px = xpr / p_norm;
@@ -309,16 +369,16 @@ __device__ __forceinline__ void bnd_kick_rad(P6& r, const PL& pl, double L, doub
 }
 
 /* diff_drift.c:30-43 inside a radiating magnet; FAST reuses pn = 1/(1+delta) */
-template <bool FAST>
-__device__ __forceinline__ void diff_drift(P6& r, double L, double pn) {
-    if (FAST) {
+template <bool FAST, class T>
+__device__ __forceinline__ void diff_drift(P6T<T>& r, double L, const T& pn) {
+    if constexpr (FAST) {
         double nl = L * pn;
         r.x += nl * r.px;
         r.y += nl * r.py;
         r.ct += (0.5 * nl * pn) * (r.px * r.px + r.py * r.py);
     } else {
-        double p_norm = 1.0 / (1.0 + r.dp);
-        double NormL = L * p_norm;
+        T p_norm = 1.0 / (1.0 + r.dp);
+        T NormL = L * p_norm;
         r.x += NormL * r.px;
         r.y += NormL * r.py;
         r.ct += NormL * p_norm * (r.px * r.px + r.py * r.py) / 2.0;
@@ -326,17 +386,17 @@ __device__ __forceinline__ void diff_drift(P6& r, double L, double pn) {
 }
 
 /* quadfringe.c:3-51 QuadFringePassP (sign=+1) / QuadFringePassN (sign=-1) */
-template <bool FAST>
-__device__ __forceinline__ void quad_fringe(P6& r, double b2, bool entrance) {
-    double u = b2 / (12.0 * (1.0 + r.dp));
-    double x2 = r.x * r.x;
-    double z2 = r.y * r.y;
-    double xz = r.x * r.y;
-    double gx = u * (x2 + 3 * z2) * r.x;
-    double gz = u * (z2 + 3 * x2) * r.y;
-    double r1tmp = 3 * u * (2 * xz * r.py - (x2 + z2) * r.px);
-    double r3tmp = 3 * u * (2 * xz * r.px - (x2 + z2) * r.py);
-    double dct = (gz * r.py - gx * r.px) / (1 + r.dp);
+template <bool FAST, class T, class B2>
+__device__ __forceinline__ void quad_fringe(P6T<T>& r, const B2& b2, bool entrance) {
+    T u = b2 / (12.0 * (1.0 + r.dp));
+    T x2 = r.x * r.x;
+    T z2 = r.y * r.y;
+    T xz = r.x * r.y;
+    T gx = u * (x2 + 3 * z2) * r.x;
+    T gz = u * (z2 + 3 * x2) * r.y;
+    T r1tmp = 3 * u * (2 * xz * r.py - (x2 + z2) * r.px);
+    T r3tmp = 3 * u * (2 * xz * r.px - (x2 + z2) * r.py);
+    T dct = (gz * r.py - gx * r.px) / (1 + r.dp);
     if (entrance) {
         r.x += gx;
         r.y -= gz;
@@ -353,8 +413,9 @@ __device__ __forceinline__ void quad_fringe(P6& r, double b2, bool entrance) {
 }
 
 /* one linear map of quadfringe.c:45-112 (x and y 2x2 blocks) */
-__device__ __forceinline__ void lin_fringe_map(P6& r, const double* m) {
-    const double x = r.x, px = r.px, y = r.y, py = r.py;
+template <class T>
+__device__ __forceinline__ void lin_fringe_map(P6T<T>& r, const double* m) {
+    const T x = r.x, px = r.px, y = r.y, py = r.py;
     r.x = m[0] * x + m[1] * px;
     r.px = m[2] * x + m[3] * px;
     r.y = m[4] * y + m[5] * py;
@@ -366,22 +427,25 @@ __device__ __forceinline__ void lin_fringe_map(P6& r, const double* m) {
  * fy_c = irho*tan(edge) is used whenever the tangent's argument is exactly
  * the edge angle (fringecorr == 0), as the reference then evaluates the same
  * tan(edge_angle). */
-template <bool FAST>
-__device__ __forceinline__ void edge_fringe(P6& r, double irho, double edge, double fc,
+template <bool FAST, class T>
+__device__ __forceinline__ void edge_fringe(P6T<T>& r, double irho, double edge, double fc,
                                             double fx, double fy_c, int method, bool fc0,
                                             double sgn) {
-    double fy;
+    T fy;
     if (method == ATB_BM_3) {
-        double q = r.px / (1 + r.dp);
+        T q = r.px / (1 + r.dp);
         fy = irho * tan(sgn > 0 ? (edge - fc + q) : (edge - fc - q));
     } else {
-        double t;
         if (FAST && fc0) {
-            fy = (method == ATB_BM_2) ? fy_c / (1 + r.dp) : fy_c;
+            if (method == ATB_BM_2) fy = fy_c / (1 + r.dp); else fy = T(fy_c);
         } else {
-            t = edge - fc / (1 + r.dp);
-            double tn = (t == edge) ? fy_c : irho * tan(t);
-            fy = (method == ATB_BM_2) ? tn / (1 + r.dp) : tn;
+            T t = edge - fc / (1 + r.dp);
+            T tn = (val(t) == edge) ? T(fy_c) : irho * tan(t);
+            if constexpr (is_dual<T>::value) {
+                /* same value, with the derivative of tan(t) kept */
+                if (val(t) == edge) { tn = irho * tan(t); tn.v = fy_c; }
+            }
+            if (method == ATB_BM_2) fy = tn / (1 + r.dp); else fy = tn;
         }
     }
     r.px += r.x * fx;
@@ -389,21 +453,24 @@ __device__ __forceinline__ void edge_fringe(P6& r, double irho, double edge, dou
 }
 
 /* diff_bend_fringe.c:1-52 (bdiff == NULL) for the radiating bend */
-template <bool FAST>
-__device__ __forceinline__ void edge_fringe_rad(P6& r, double irho, double edge, double psi,
+template <bool FAST, class T>
+__device__ __forceinline__ void edge_fringe_rad(P6T<T>& r, double irho, double edge, double psi,
                                                 double fx, double fy_c, int method, bool fc0,
                                                 double sgn) {
-    double p_norm = 1.0 / (1.0 + r.dp);
-    double fy;
+    T p_norm = 1.0 / (1.0 + r.dp);
+    T fy;
     if (method == ATB_BM_3) {
         fy = irho * tan(edge - psi + sgn * r.px * p_norm);
     } else {
         if (FAST && fc0) {
-            fy = (method == ATB_BM_2) ? fy_c * p_norm : fy_c;
+            if (method == ATB_BM_2) fy = fy_c * p_norm; else fy = T(fy_c);
         } else {
-            double t = edge - psi * p_norm;
-            double tn = (t == edge) ? fy_c : irho * tan(t);
-            fy = (method == ATB_BM_2) ? tn * p_norm : tn;
+            T t = edge - psi * p_norm;
+            T tn = (val(t) == edge) ? T(fy_c) : irho * tan(t);
+            if constexpr (is_dual<T>::value) {
+                if (val(t) == edge) { tn = irho * tan(t); tn.v = fy_c; }
+            }
+            if (method == ATB_BM_2) fy = tn * p_norm; else fy = tn;
         }
     }
     r.px += r.x * fx;

@@ -118,18 +118,21 @@ struct Rec {
 
 /* ---------------- misalignment / aperture wrappers ----------------------- */
 
-__device__ __forceinline__ void entrance_misalign(P6& r, const Rec& e) {
+template <class T>
+__device__ __forceinline__ void entrance_misalign(P6T<T>& r, const Rec& e) {
     const uint32_t fl = e.flags();
     if (const double* t1 = e.blk(ATB_OPT_T1)) add_t(r, t1);
     if (const double* r1 = e.blk(ATB_OPT_R1)) mult_r(r, r1, fl & ATB_F_R1_DENSE);
 }
 
-__device__ __forceinline__ void apertures(P6& r, const Rec& e) {
+template <class T>
+__device__ __forceinline__ void apertures(P6T<T>& r, const Rec& e) {
     if (const double* ra = e.blk(ATB_OPT_RAP)) check_rect(r, ra);
     if (const double* ea = e.blk(ATB_OPT_EAP)) check_ellip(r, ea);
 }
 
-__device__ __forceinline__ void exit_misalign(P6& r, const Rec& e) {
+template <class T>
+__device__ __forceinline__ void exit_misalign(P6T<T>& r, const Rec& e) {
     const uint32_t fl = e.flags();
     if (const double* r2 = e.blk(ATB_OPT_R2)) mult_r(r, r2, fl & ATB_F_R2_DENSE);
     if (const double* t2 = e.blk(ATB_OPT_T2)) add_t(r, t2);
@@ -137,10 +140,31 @@ __device__ __forceinline__ void exit_misalign(P6& r, const Rec& e) {
 
 /* ---------------- pass methods ------------------------------------------- */
 
+/* A differentiated strength (tangent kernel only): PolynomB[k] of the
+ * element is replaced by v and carried as the last derivative direction. */
+struct Param {
+    int k;        /* coefficient order, -1: none */
+    double v;
+};
+
+/* the quadrupole-fringe gradient b1 = PolynomB[1], seeded when it is the
+ * differentiated strength */
+template <class T>
+__device__ __forceinline__ T fringe_b1(const Rec& e, const Param& pm) {
+    T b1 = e.f(ATB_SM_B1);
+    if constexpr (is_dual<T>::value) {
+        if (pm.k == 1) {
+            b1.v = pm.v;
+            b1.d[sizeof(b1.d) / sizeof(double) - 1] = 1.0;
+        }
+    }
+    return b1;
+}
+
 /* StrMPoleSymplectic4Pass.c:29-109, BndMPoleSymplectic4Pass.c:38-129,
  * StrMPoleSymplectic4RadPass.c:30-115, BndMPoleSymplectic4RadPass.c:39-128 */
-template <int MO, bool BEND, bool RAD>
-__device__ __forceinline__ void pass_multipole(P6& r, const Rec& e) {
+template <int MO, bool BEND, bool RAD, class T>
+__device__ __forceinline__ void pass_multipole(P6T<T>& r, const Rec& e, const Param& pm) {
     const uint32_t fl = e.flags();
     const double L1 = e.f(ATB_SM_L1), L2 = e.f(ATB_SM_L2);
     const double K1 = e.f(ATB_SM_K1), K2 = e.f(ATB_SM_K2);
@@ -149,11 +173,14 @@ __device__ __forceinline__ void pass_multipole(P6& r, const Rec& e) {
     const double* B = A + mo + 1;
     Poly<MO> pl;
     pl.load(A, B, mo);
+    if constexpr (is_dual<T>::value) {
+        if (pm.k >= 0) pl.set_param(pm.k, pm.v);
+    }
 
     if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_SM_SCALE));
-    double nl1 = 0.0, nl2 = 0.0;
+    T nl1 = 0.0, nl2 = 0.0;
     if (!RAD) {
-        double p_norm = 1.0 / (1.0 + r.dp);
+        T p_norm = 1.0 / (1.0 + r.dp);
         nl1 = L1 * p_norm;
         nl2 = L2 * p_norm;
     }
@@ -173,7 +200,7 @@ __device__ __forceinline__ void pass_multipole(P6& r, const Rec& e) {
                                e.f(ATB_BM_FYIN), m_in, fl & ATB_F_FC0_IN, 1.0);
     }
     if (fl & ATB_F_FQ_IN) {
-        const double b1 = e.f(ATB_SM_B1);
+        const T b1 = fringe_b1<T>(e, pm);
         if (fl & ATB_F_FQ_IN_LIN) {
             const double* fm = e.blk(ATB_OPT_FRINGE);
             lin_fringe_map(r, fm);
@@ -186,7 +213,8 @@ __device__ __forceinline__ void pass_multipole(P6& r, const Rec& e) {
     const int ns = e.nsteps();
     if (RAD) {
         const double radc = e.f(ATB_SM_RADC);
-        double pn = kFast ? 1.0 / (1.0 + r.dp) : 0.0;
+        T pn = 0.0;
+        if (kFast) pn = 1.0 / (1.0 + r.dp);
         for (int m = 0; m < ns; ++m) {
             diff_drift<kFast>(r, L1, pn);
             if (BEND) bnd_kick_rad<kFast>(r, pl, K1, irho, k1i, radc, pn);
@@ -200,9 +228,9 @@ __device__ __forceinline__ void pass_multipole(P6& r, const Rec& e) {
             diff_drift<kFast>(r, L1, pn);
         }
     } else {
-        double c1 = 0.0, c2 = 0.0;
+        T c1 = 0.0, c2 = 0.0;
         if (kFast) {
-            double h = 0.5 / (1.0 + r.dp);
+            T h = 0.5 / (1.0 + r.dp);
             c1 = nl1 * h;
             c2 = nl2 * h;
         }
@@ -217,7 +245,7 @@ __device__ __forceinline__ void pass_multipole(P6& r, const Rec& e) {
         }
     }
     if (fl & ATB_F_FQ_OUT) {
-        const double b1 = e.f(ATB_SM_B1);
+        const T b1 = fringe_b1<T>(e, pm);
         if (fl & ATB_F_FQ_OUT_LIN) {
             const double* fm = e.blk(ATB_OPT_FRINGE);
             lin_fringe_map(r, fm + 16);
@@ -241,19 +269,25 @@ __device__ __forceinline__ void pass_multipole(P6& r, const Rec& e) {
     if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_SM_ISCALE));
 }
 
-template <bool BEND, bool RAD>
-__device__ __forceinline__ void pass_multipole_dispatch(P6& r, const Rec& e) {
-    switch (e.mo()) {
-        case 0: pass_multipole<0, BEND, RAD>(r, e); break;
-        case 1: pass_multipole<1, BEND, RAD>(r, e); break;
-        case 2: pass_multipole<2, BEND, RAD>(r, e); break;
-        case 3: pass_multipole<3, BEND, RAD>(r, e); break;
-        default: pass_multipole<-1, BEND, RAD>(r, e); break;
+template <bool BEND, bool RAD, class T>
+__device__ __forceinline__ void pass_multipole_dispatch(P6T<T>& r, const Rec& e, const Param& pm) {
+    if constexpr (is_dual<T>::value) {
+        /* one generic instance for the tangent kernel keeps its size sane */
+        pass_multipole<-1, BEND, RAD>(r, e, pm);
+    } else {
+        switch (e.mo()) {
+            case 0: pass_multipole<0, BEND, RAD>(r, e, pm); break;
+            case 1: pass_multipole<1, BEND, RAD>(r, e, pm); break;
+            case 2: pass_multipole<2, BEND, RAD>(r, e, pm); break;
+            case 3: pass_multipole<3, BEND, RAD>(r, e, pm); break;
+            default: pass_multipole<-1, BEND, RAD>(r, e, pm); break;
+        }
     }
 }
 
 /* DriftPass.c:16-48 */
-__device__ __forceinline__ void pass_drift(P6& r, const Rec& e) {
+template <class T>
+__device__ __forceinline__ void pass_drift(P6T<T>& r, const Rec& e) {
     entrance_misalign(r, e);
     apertures(r, e);
     drift6<kFast>(r, e.f(ATB_DR_LE));
@@ -262,20 +296,25 @@ __device__ __forceinline__ void pass_drift(P6& r, const Rec& e) {
 }
 
 /* IdentityPass.c:20-43 */
-__device__ __forceinline__ void pass_identity(P6& r, const Rec& e) {
+template <class T>
+__device__ __forceinline__ void pass_identity(P6T<T>& r, const Rec& e) {
     entrance_misalign(r, e);
     apertures(r, e);
     exit_misalign(r, e);
 }
 
 /* ThinMPolePass.c:28-70 */
-__device__ __forceinline__ void pass_thinmpole(P6& r, const Rec& e) {
+template <class T>
+__device__ __forceinline__ void pass_thinmpole(P6T<T>& r, const Rec& e, const Param& pm) {
     const uint32_t fl = e.flags();
     const int mo = e.mo();
     const double* A = e.p + ATB_TM_POLY;
     const double* B = A + mo + 1;
     Poly<-1> pl;
     pl.load(A, B, mo);
+    if constexpr (is_dual<T>::value) {
+        if (pm.k >= 0) pl.set_param(pm.k, pm.v);
+    }
     const double bax = e.f(ATB_TM_BAX), bay = e.f(ATB_TM_BAY);
     if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_TM_SCALE));
     entrance_misalign(r, e);
@@ -289,13 +328,15 @@ __device__ __forceinline__ void pass_thinmpole(P6& r, const Rec& e) {
 }
 
 /* RFCavityPass.c:23-68 -> attrackfunc.c:5-42 (trackRFCavity) */
-__device__ __forceinline__ void rf_kick(P6& r, const Rec& e, int nturn) {
+template <class T>
+__device__ __forceinline__ void rf_kick(P6T<T>& r, const Rec& e, int nturn) {
     const double nv = e.f(ATB_RF_NV), tf = e.f(ATB_RF_TF), lag = e.f(ATB_RF_LAG);
     const double ht = e.f(ATB_RF_HT), phi = e.f(ATB_RF_PHI);
     r.dp += -nv * sin(tf * ((r.ct - lag) / ATB_C0 - ht * (double)nturn) - phi);
 }
 
-__device__ __forceinline__ void pass_rfcavity(P6& r, const Rec& e, int nturn) {
+template <class T>
+__device__ __forceinline__ void pass_rfcavity(P6T<T>& r, const Rec& e, int nturn) {
     const uint32_t fl = e.flags();
     if (!(fl & ATB_F_THICK)) {
         if (fl & ATB_F_NV) rf_kick(r, e, nturn);
@@ -308,7 +349,8 @@ __device__ __forceinline__ void pass_rfcavity(P6& r, const Rec& e, int nturn) {
 }
 
 /* CorrectorPass.c:25-90 */
-__device__ __forceinline__ void pass_corrector(P6& r, const Rec& e) {
+template <class T>
+__device__ __forceinline__ void pass_corrector(P6T<T>& r, const Rec& e) {
     const uint32_t fl = e.flags();
     const double xk = e.f(ATB_CO_XK), yk = e.f(ATB_CO_YK);
     if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_CO_SCALE));
@@ -319,8 +361,8 @@ __device__ __forceinline__ void pass_corrector(P6& r, const Rec& e) {
         r.py += yk;
     } else {
         const double le = e.f(ATB_CO_LE);
-        double p_norm = 1.0 / (1.0 + r.dp);
-        double nl = le * p_norm;
+        T p_norm = 1.0 / (1.0 + r.dp);
+        T nl = le * p_norm;
         entrance_misalign(r, e);
         apertures(r, e);
         r.ct += nl * p_norm * (e.f(ATB_CO_K2) + r.px * r.px + r.py * r.py + r.px * xk + r.py * yk) / 2;
@@ -336,16 +378,18 @@ __device__ __forceinline__ void pass_corrector(P6& r, const Rec& e) {
 
 /* One element on one particle; lost particles (x is NaN) are skipped as every
  * reference pass method does (e.g. StrMPoleSymplectic4Pass.c:59). */
-__device__ __forceinline__ void track_element(P6& r, const Rec& e, int nturn) {
-    if (isnan(r.x)) return;
+template <class T>
+__device__ __forceinline__ void track_element(P6T<T>& r, const Rec& e, int nturn,
+                                              const Param& pm = Param{-1, 0.0}) {
+    if (isnan(val(r.x))) return;
     switch (e.op()) {
         case ATB_OP_IDENTITY: pass_identity(r, e); break;
         case ATB_OP_DRIFT: pass_drift(r, e); break;
-        case ATB_OP_STRMPOLE: pass_multipole_dispatch<false, false>(r, e); break;
-        case ATB_OP_STRMPOLE_RAD: pass_multipole_dispatch<false, true>(r, e); break;
-        case ATB_OP_BNDMPOLE: pass_multipole_dispatch<true, false>(r, e); break;
-        case ATB_OP_BNDMPOLE_RAD: pass_multipole_dispatch<true, true>(r, e); break;
-        case ATB_OP_THINMPOLE: pass_thinmpole(r, e); break;
+        case ATB_OP_STRMPOLE: pass_multipole_dispatch<false, false>(r, e, pm); break;
+        case ATB_OP_STRMPOLE_RAD: pass_multipole_dispatch<false, true>(r, e, pm); break;
+        case ATB_OP_BNDMPOLE: pass_multipole_dispatch<true, false>(r, e, pm); break;
+        case ATB_OP_BNDMPOLE_RAD: pass_multipole_dispatch<true, true>(r, e, pm); break;
+        case ATB_OP_THINMPOLE: pass_thinmpole(r, e, pm); break;
         case ATB_OP_RFCAVITY: pass_rfcavity(r, e, nturn); break;
         case ATB_OP_CORRECTOR: pass_corrector(r, e); break;
         case ATB_OP_APERTURE: check_rect(r, e.p + ATB_AP_LIM); break;
@@ -354,9 +398,10 @@ __device__ __forceinline__ void track_element(P6& r, const Rec& e, int nturn) {
 }
 
 /* pyat/at.c:123: lost if any coordinate is non-finite or |r_n| > 1, n < 5 */
-__device__ __forceinline__ bool is_bad(const P6& r) {
-    return !all_finite(r) || fabs(r.x) > 1.0 || fabs(r.px) > 1.0 || fabs(r.y) > 1.0 ||
-           fabs(r.py) > 1.0 || fabs(r.dp) > 1.0;
+template <class T>
+__device__ __forceinline__ bool is_bad(const P6T<T>& r) {
+    return !all_finite(r) || fabs(val(r.x)) > 1.0 || fabs(val(r.px)) > 1.0 ||
+           fabs(val(r.y)) > 1.0 || fabs(val(r.py)) > 1.0 || fabs(val(r.dp)) > 1.0;
 }
 
 __device__ __forceinline__ void load6(const double* src, P6& r) {
@@ -379,6 +424,8 @@ __device__ __forceinline__ int seg_at(const AtbJob& J, long long q) {
 }
 
 /* ---------------- the kernel --------------------------------------------- */
+
+#ifndef ATB_NO_TRACK_KERNEL
 
 extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
 ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
@@ -574,6 +621,8 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
         __syncthreads();
     }
 }
+
+#endif  // ATB_NO_TRACK_KERNEL
 
 }  // namespace atb
 

@@ -138,6 +138,21 @@ class Engine:
                                      1 if losses is not None else 0, lp[0], lp[1], lp[2], lp[3],
                                      alive_ptr, moments_ptr, mode_code(mode), stream))
 
+    def tangent_device(self, lid: int, r_ptr: int, npart: int, nturns: int, turn0: int,
+                       param_elem: np.ndarray, param_order: np.ndarray, value_ptr: int | None,
+                       jac_ptr: int, grad_ptr: int | None, lost_ptr: int | None = None,
+                       stream: int | None = None):
+        """Enqueue tangent tracking of a device-resident (6, N) array: exact
+        derivatives d r / d r0 into ``jac_ptr`` (N, 6, 6) and d r / d K into
+        ``grad_ptr`` (P, 6, N) for the strengths PolynomB[param_order[q]] of
+        elements param_elem[q], whose values are read from ``value_ptr``."""
+        pe = np.ascontiguousarray(param_elem, dtype=np.int32)
+        po = np.ascontiguousarray(param_order, dtype=np.int32)
+        check(lib().atb_tangent_device(self.h, int(lid), r_ptr, int(npart), int(nturns),
+                                       int(turn0), ptr(pe) if pe.size else None,
+                                       ptr(po) if po.size else None, value_ptr, int(pe.size),
+                                       jac_ptr, grad_ptr, lost_ptr, stream))
+
     def track_batch(self, jobs: list[dict], mode=None, stream: int | None = None):
         """One persistent launch over many jobs (dicts with lattice_id, r, np,
         nturns, optional turn0 and losses=(islost, lturn, lelem, lcoord)

@@ -182,10 +182,11 @@ def large_ring(seed: int = 1, ncells: int = 32, misalign: bool = True,
 
 LARGE_SIGMA = (1e-4, 1e-5, 1e-5, 1e-6, 1e-3, 1e-3)
 
-#: 6-D closed orbit of ``large_ring()`` (seed 1) at its entrance, found by
-#: Newton iteration on the one-turn map; tests check it is a fixed point.
-LARGE_ORBIT = (-0.0005127165227938493, -3.0086497035789093e-05, -0.000910018854244866,
-               0.0003269288773499088, 3.754422313425573e-05, -0.022855500398494124)
+#: 6-D closed orbit of ``large_ring()`` (seed 1) at its entrance as the
+#: reference's find_orbit6 defines it (M(x) = x + theta, theta the RF
+#: path-length slip), found by Newton iteration on the one-turn map.
+LARGE_ORBIT = (-0.0005151025164660066, -3.068590557039712e-05, -0.0009101295900902443,
+               0.00032698077877960427, 2.839234239542605e-05, -0.022852877509548702)
 
 
 def large_ring_bunch(n: int, seed: int = 0) -> np.ndarray:

@@ -57,6 +57,7 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving trace")
     ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--no-diff", action="store_true", help="skip the tangent-kernel timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -367,6 +368,9 @@ def run_b200(a):
     serve = None
     if world == 1 and not a.no_serve:
         serve = run_serving(a.serve_requests, mode, local)
+    dif = None
+    if world == 1 and not a.no_diff:
+        dif = run_diff(local)
 
     traffic = None
     prof = os.path.join(REPO, "profiles", "traffic_%s.json" % a.workload)
@@ -386,7 +390,7 @@ def run_b200(a):
                          "peak_source": "measured live: atb_fp64_peak DFMA chains on this GPU",
                          "flops_per_particle_turn": fpt, "survivor_particle_turns": survivors},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps, "clocks": clk,
-            "serving": serve,
+            "serving": serve, "differentiation": dif,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -426,6 +430,72 @@ def run_serving(nreq, mode, device):
             "plain_drop_in_sequential": dict(sq, particle_turns_per_s=pt / wall_seq,
                                              wall_s=wall_seq),
             "results_identical": bool(same)}
+
+
+def run_diff(device, n=65536):
+    """Exact derivatives on the FODO ring (the differentiable-tracking
+    workload): 65,536 particles, sigma 1e-6 around the closed orbit, with
+    respect to the initial coordinates and the 64 quadrupole + 64 sextupole
+    strengths, for 1 and 100 turns.  Device time of the tangent launch (CUDA
+    events), of the autograd backward contraction, and of the 2 x 128 + 12
+    exact-mode tracking runs that central differences would need instead."""
+    import torch
+
+    from at_b200 import diff, physics, rings
+    from at_b200.engine import Engine
+
+    ring = rings.fodo_ring()
+    orbit = physics.find_orbit6(ring, mode="exact")
+    r0 = rings.gaussian(n, [1e-6] * 6, seed=11, centre=orbit)
+    params = diff.multipole_strengths(ring)
+    tr = diff.TangentTracker(ring, params, device=device)
+    dev = torch.device("cuda", device)
+    x = torch.tensor(np.ascontiguousarray(r0.T), dtype=torch.float64, device=dev)
+    out = {"workload": "FODO ring (385 elements), %d particles sigma 1e-6 around the closed "
+                       "orbit, %d strengths (64 quadrupole + 64 sextupole)" % (n, len(params))}
+    eng = Engine.get(device)
+    lid = eng.upload(tr.cl)
+    try:
+        for nt in (1, 100):
+            tr.track(x, None, nt)                     # warm-up
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r, jac, grad, lost = tr.track(x, None, nt)
+            e1.record()
+            e1.synchronize()
+            t_tan = e0.elapsed_time(e1) * 1e-3
+            # the adjoint (vector-Jacobian) products of the autograd backward
+            g = torch.randn_like(r)
+            e0.record()
+            torch.einsum("ni,nij->nj", g, jac)
+            torch.einsum("ni,pin->p", g, grad)
+            e1.record()
+            e1.synchronize()
+            t_bwd = e0.elapsed_time(e1) * 1e-3
+            # one exact-mode tracking of the same particles (device resident)
+            xr = x.clone()
+            eng.track_device(lid, xr.data_ptr(), n, nt, mode="exact",
+                             stream=torch.cuda.current_stream(dev).cuda_stream)
+            xr = x.clone()
+            e0.record()
+            eng.track_device(lid, xr.data_ptr(), n, nt, mode="exact",
+                             stream=torch.cuda.current_stream(dev).cuda_stream)
+            e1.record()
+            e1.synchronize()
+            eng.sync(torch.cuda.current_stream(dev).cuda_stream)
+            t_trk = e0.elapsed_time(e1) * 1e-3
+            runs = 2 * len(params) + 12
+            out["turns_%d" % nt] = {
+                "tangent_ms": 1e3 * t_tan, "backward_ms": 1e3 * t_bwd,
+                "particle_turns_per_s": n * nt / t_tan,
+                "lost": int(lost.sum().item()),
+                "exact_tracking_ms": 1e3 * t_trk,
+                "central_differences_ms": 1e3 * t_trk * runs,
+                "speedup_vs_central_differences": t_trk * runs / t_tan}
+    finally:
+        eng.free(lid)
+        tr.close()
+    return out
 
 
 def main():

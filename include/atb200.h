@@ -123,6 +123,25 @@ int atb_track_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np, i
                      uint32_t* lelem, double* lcoord, uint32_t* alive, double* moments,
                      int32_t mode, void* stream);
 
+/* Tangent tracking (device pointers, enqueued on `stream`, NULL: the
+ * handle's stream): tracks the (6, np) particles `r` in place for `nturns`
+ * whole turns in the exact arithmetic and writes the exact derivatives of
+ * the final coordinates, jac (np, 6, 6) = d r_i / d r0_j and grad
+ * (nparam, 6, np) = d r_i / d K_q, for nparam multipole strengths
+ * K_q = PolynomB[param_order[q]] of element param_elem[q] (host arrays; one
+ * strength per element, order in [1, MaxOrder]).  The strengths used are
+ * read from param_value (device, nparam), which replaces the table's values
+ * for those coefficients, so a caller can move them without re-uploading the
+ * lattice.  Lost particles come back NaN in r, jac and grad (islost, optional,
+ * marks them).  Replaces the finite-difference Jacobian of
+ * pyat/at/physics/matrix.py:105-165 (find_m66) and the finite differences a
+ * caller of lattice_pass would take for strength sensitivities; the
+ * reference has no exact-derivative tracking. */
+int atb_tangent_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np, int32_t nturns,
+                       int32_t turn0, const int32_t* param_elem, const int32_t* param_order,
+                       const double* param_value, int32_t nparam, double* jac, double* grad,
+                       uint8_t* islost, void* stream);
+
 /* Many lattice variants and particle sets in one persistent launch (device
  * pointers); the tiles of the longest jobs are scheduled first. */
 int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,

@@ -19,6 +19,23 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* The arithmetic type.  The oracle proper is double; oracle_q.c includes
+ * this file with ORACLE_REAL set to a wider type (and the R_* functions to
+ * its math library) for finite differences whose rounding floor lies far
+ * below double's.  Element data and the interface stay double. */
+#ifndef ORACLE_REAL
+typedef double real;
+#define R_SIN sin
+#define R_COS cos
+#define R_TAN tan
+#define R_EXP exp
+#define R_POW pow
+#define R_ROUND round
+#define R_FABS fabs
+#else
+typedef ORACLE_REAL real;
+#endif
+
 /* pass methods (must match oracle.py) */
 enum {
     O_IDENTITY = 0, O_DRIFT, O_STRMPOLE, O_STRMPOLE_RAD, O_BNDMPOLE, O_BNDMPOLE_RAD,
@@ -58,15 +75,15 @@ static const double O_RAD_CONST = 2.0 / 3.0 * O_RE;
 /* ---- small vector helpers ---------------------------------------------- */
 
 /* atlalib.c:50-57 */
-static void o_addv(double *r, const double *d) {
+static void o_addv(real *r, const double *d) {
     for (int i = 0; i < 6; i++) r[i] += d[i];
 }
 
 /* atlalib.c:17-32: column-major 6x6 times vector, accumulated from 0 */
-static void o_mulmv(double *r, const double *m) {
-    double out[6];
+static void o_mulmv(real *r, const double *m) {
+    real out[6];
     for (int i = 0; i < 6; i++) {
-        double acc = 0;
+        real acc = 0;
         for (int j = 0; j < 6; j++) acc += m[i + j * 6] * r[j];
         out[i] = acc;
     }
@@ -74,56 +91,56 @@ static void o_mulmv(double *r, const double *m) {
 }
 
 /* atlalib.c:169-175 */
-static void o_rect_ap(double *r, const double *lim) {
+static void o_rect_ap(real *r, const double *lim) {
     if (r[0] < lim[0] || r[0] > lim[1]) r[5] = INFINITY;
     else if (r[2] < lim[2] || r[2] > lim[3]) r[5] = INFINITY;
 }
 
 /* atlalib.c:185-190 */
-static void o_ellip_ap(double *r, const double *ax) {
-    double u = r[0] / ax[0];
-    double v = r[2] / ax[1];
+static void o_ellip_ap(real *r, const double *ax) {
+    real u = r[0] / ax[0];
+    real v = r[2] / ax[1];
     if ((u * u + v * v) >= 1) r[5] = INFINITY;
 }
 
 /* atlalib.c:70-75 */
-static void o_pref(double *r, double s) {
+static void o_pref(real *r, real s) {
     r[1] /= s;
     r[3] /= s;
     r[4] = (r[4] + 1.0 - s) / s;
 }
 
 /* atlalib.c:59-68 (== driftkickrad.c drift6 and diff_drift without bdiff) */
-static void o_drift6(double *r, double L) {
-    double pn = 1 / (1 + r[4]);
-    double nl = L * pn;
+static void o_drift6(real *r, real L) {
+    real pn = 1 / (1 + r[4]);
+    real nl = L * pn;
     r[0] += nl * r[1];
     r[2] += nl * r[3];
     r[5] += nl * pn * (r[1] * r[1] + r[3] * r[3]) / 2;
 }
 
 /* diff_drift.c:30-43 (its literal constants are 1.0 and 2.0) */
-static void o_ddrift(double *r, double L) {
-    double pn = 1.0 / (1.0 + r[4]);
-    double nl = L * pn;
+static void o_ddrift(real *r, real L) {
+    real pn = 1.0 / (1.0 + r[4]);
+    real nl = L * pn;
     r[0] += nl * r[1];
     r[2] += nl * r[3];
     r[5] += nl * pn * (r[1] * r[1] + r[3] * r[3]) / 2.0;
 }
 
 /* driftkick.c:37-48 */
-static void o_fastdrift(double *r, double nl) {
+static void o_fastdrift(real *r, real nl) {
     r[0] += nl * r[1];
     r[2] += nl * r[3];
     r[5] += nl * (r[1] * r[1] + r[3] * r[3]) / (2 * (1 + r[4]));
 }
 
 /* the multipole field, highest order first (driftkick.c:92-115 et al.) */
-static void o_field(const double *r, const double *A, const double *B, int n,
-                    double *re, double *im) {
-    double a = B[n], b = A[n];
+static void o_field(const real *r, const real *A, const real *B, int n,
+                    real *re, real *im) {
+    real a = B[n], b = A[n];
     for (int k = n - 1; k >= 0; k--) {
-        double t = a * r[0] - b * r[2] + B[k];
+        real t = a * r[0] - b * r[2] + B[k];
         b = b * r[0] + a * r[2] + A[k];
         a = t;
     }
@@ -132,16 +149,16 @@ static void o_field(const double *r, const double *A, const double *B, int n,
 }
 
 /* driftkick.c:92-115 strthinkick */
-static void o_strkick(double *r, const double *A, const double *B, double L, int n) {
-    double re, im;
+static void o_strkick(real *r, const real *A, const real *B, real L, int n) {
+    real re, im;
     o_field(r, A, B, n, &re, &im);
     r[1] -= L * re;
     r[3] += L * im;
 }
 
 /* driftkick.c:51-89 bndthinkick */
-static void o_bndkick(double *r, const double *A, const double *B, double L, double h, int n) {
-    double re, im;
+static void o_bndkick(real *r, const real *A, const real *B, real L, real h, int n) {
+    real re, im;
     o_field(r, A, B, n, &re, &im);
     r[1] -= L * (re - (r[4] - r[0] * h) * h);
     r[3] += L * im;
@@ -149,16 +166,16 @@ static void o_bndkick(double *r, const double *A, const double *B, double L, dou
 }
 
 /* diff_str_kick.c:19-83 (bdiff == NULL) */
-static void o_strkick_rad(double *r, const double *A, const double *B, int n, double L,
-                          double radc) {
-    double re, im;
+static void o_strkick_rad(real *r, const real *A, const real *B, int n, real L,
+                          real radc) {
+    real re, im;
     o_field(r, A, B, n, &re, &im);
-    double pn = 1.0 / (1.0 + r[4]);
-    double xp = r[1] * pn, yp = r[3] * pn;
-    double bx = im, by = re;
-    double vn = 1.0 / (1.0 + xp * xp + yp * yp);
-    double b2 = (by * by + bx * bx + (bx * yp - by * xp) * (bx * yp - by * xp)) * vn;
-    double f = (1.0 + (xp * xp + yp * yp) / 2.0) / (pn * pn) * L;
+    real pn = 1.0 / (1.0 + r[4]);
+    real xp = r[1] * pn, yp = r[3] * pn;
+    real bx = im, by = re;
+    real vn = 1.0 / (1.0 + xp * xp + yp * yp);
+    real b2 = (by * by + bx * bx + (bx * yp - by * xp) * (bx * yp - by * xp)) * vn;
+    real f = (1.0 + (xp * xp + yp * yp) / 2.0) / (pn * pn) * L;
     r[4] -= radc * b2 * f;
     pn = 1.0 / (1.0 + r[4]);
     r[1] = xp / pn;
@@ -168,19 +185,19 @@ static void o_strkick_rad(double *r, const double *A, const double *B, int n, do
 }
 
 /* diff_bnd_kick.c:101-174 with its B2perp (:85-99), bdiff == NULL */
-static void o_bndkick_rad(double *r, const double *A, const double *B, int n, double L,
-                          double h, double radc) {
-    double re, im;
+static void o_bndkick_rad(real *r, const real *A, const real *B, int n, real L,
+                          real h, real radc) {
+    real re, im;
     o_field(r, A, B, n, &re, &im);
-    double pn = 1.0 / (1.0 + r[4]);
-    double x = r[0];
-    double xp = r[1] * pn, yp = r[3] * pn;
-    double bx = im, by = re + h;
-    double vn = 1.0 / ((1.0 + x * h) * (1.0 + x * h) + xp * xp + yp * yp);
-    double b2 = ((by * (1 + x * h)) * (by * (1 + x * h)) + (bx * (1 + x * h)) * (bx * (1 + x * h)) +
+    real pn = 1.0 / (1.0 + r[4]);
+    real x = r[0];
+    real xp = r[1] * pn, yp = r[3] * pn;
+    real bx = im, by = re + h;
+    real vn = 1.0 / ((1.0 + x * h) * (1.0 + x * h) + xp * xp + yp * yp);
+    real b2 = ((by * (1 + x * h)) * (by * (1 + x * h)) + (bx * (1 + x * h)) * (bx * (1 + x * h)) +
                  (bx * yp - by * xp) * (bx * yp - by * xp)) * vn;
-    double f = (1.0 + x * h + (xp * xp + yp * yp) / 2.0) / (pn * pn) * L;
-    double d0 = r[4];
+    real f = (1.0 + x * h + (xp * xp + yp * yp) / 2.0) / (pn * pn) * L;
+    real d0 = r[4];
     r[4] -= radc * b2 * f;
     pn = 1.0 / (1.0 + r[4]);
     r[1] = xp / pn;
@@ -191,14 +208,14 @@ static void o_bndkick_rad(double *r, const double *A, const double *B, int n, do
 }
 
 /* quadfringe.c:3-51: sgn = +1 (QuadFringePassP) or -1 (QuadFringePassN) */
-static void o_quad_fringe(double *r, double b2, int sgn) {
-    double u = b2 / (12.0 * (1.0 + r[4]));
-    double x2 = r[0] * r[0], z2 = r[2] * r[2], xz = r[0] * r[2];
-    double gx = u * (x2 + 3 * z2) * r[0];
-    double gz = u * (z2 + 3 * x2) * r[2];
-    double t1 = 3 * u * (2 * xz * r[3] - (x2 + z2) * r[1]);
-    double t3 = 3 * u * (2 * xz * r[1] - (x2 + z2) * r[3]);
-    double dc = (gz * r[3] - gx * r[1]) / (1 + r[4]);
+static void o_quad_fringe(real *r, real b2, int sgn) {
+    real u = b2 / (12.0 * (1.0 + r[4]));
+    real x2 = r[0] * r[0], z2 = r[2] * r[2], xz = r[0] * r[2];
+    real gx = u * (x2 + 3 * z2) * r[0];
+    real gz = u * (z2 + 3 * x2) * r[2];
+    real t1 = 3 * u * (2 * xz * r[3] - (x2 + z2) * r[1]);
+    real t3 = 3 * u * (2 * xz * r[1] - (x2 + z2) * r[3]);
+    real dc = (gz * r[3] - gx * r[1]) / (1 + r[4]);
     if (sgn > 0) {
         r[0] += gx; r[2] -= gz; r[5] -= dc; r[1] += t1; r[3] -= t3;
     } else {
@@ -207,8 +224,8 @@ static void o_quad_fringe(double *r, double b2, int sgn) {
 }
 
 /* quadfringe.c: quadPartialFringeMatrix, 2x2 blocks (m[0..3] x, m[4..7] y) */
-static void o_fringe_matrix(double K1, const double *fi, int part, double *m) {
-    double in = 1.0, k2 = K1 * K1, j1x, j2x, j3x, j1y, j2y, j3y;
+static void o_fringe_matrix(real K1, const double *fi, int part, real *m) {
+    real in = 1.0, k2 = K1 * K1, j1x, j2x, j3x, j1y, j2y, j3y;
     if (part == 1) {
         j1x = in * (K1 * fi[1] - 2 * k2 * fi[3] / 3. - k2 * fi[0] * fi[2] / 2);
         j2x = in * K1 * fi[2];
@@ -222,13 +239,13 @@ static void o_fringe_matrix(double K1, const double *fi, int part, double *m) {
     }
     j2y = -j2x;
     j3y = j3x;
-    double ex = exp(j1x), ey = exp(j1y);
+    real ex = R_EXP(j1x), ey = R_EXP(j1y);
     m[0] = ex; m[1] = j2x / ex; m[2] = ex * j3x; m[3] = (1 + j2x * j3x) / ex;
     m[4] = ey; m[5] = j2y / ey; m[6] = ey * j3y; m[7] = (1 + j2y * j3y) / ey;
 }
 
-static void o_apply22(double *r, const double *m) {
-    double x = r[0], px = r[1], y = r[2], py = r[3];
+static void o_apply22(real *r, const real *m) {
+    real x = r[0], px = r[1], y = r[2], py = r[3];
     r[0] = m[0] * x + m[1] * px;
     r[1] = m[2] * x + m[3] * px;
     r[2] = m[4] * y + m[5] * py;
@@ -236,8 +253,8 @@ static void o_apply22(double *r, const double *m) {
 }
 
 /* quadfringe.c:45-112 linearQuadFringeElegantEntrance/Exit */
-static void o_lin_fringe(double *r, double b2, const double *fm, const double *fp, int entrance) {
-    double m[8], s;
+static void o_lin_fringe(real *r, real b2, const double *fm, const double *fp, int entrance) {
+    real m[8], s;
     if (entrance) {
         o_fringe_matrix(b2, fp, 2, m);
         s = m[0]; m[0] = m[3]; m[3] = s;
@@ -258,41 +275,41 @@ static void o_lin_fringe(double *r, double b2, const double *fm, const double *f
 }
 
 /* atphyslib.c:15-79 edge_fringe_entrance/exit; sgn +1 entrance, -1 exit */
-static void o_edge(double *r, double h, double edge, double fint, double gap, int method,
+static void o_edge(real *r, real h, real edge, real fint, real gap, int method,
                    int sgn) {
-    double fc = 0.0, fy;
+    real fc = 0.0, fy;
     if (!((fint == 0.0) || (gap == 0.0) || (method == 0))) {
-        double se = sin(edge), ce = cos(edge);
+        real se = R_SIN(edge), ce = R_COS(edge);
         fc = h * gap * fint * (1 + se * se) / ce;
     }
-    double fx = h * tan(edge);
+    real fx = h * R_TAN(edge);
     if (method == 2)
-        fy = h * tan(edge - fc / (1 + r[4])) / (1 + r[4]);
+        fy = h * R_TAN(edge - fc / (1 + r[4])) / (1 + r[4]);
     else if (method == 3)
-        fy = (sgn > 0) ? h * tan(edge - fc + r[1] / (1 + r[4]))
-                       : h * tan(edge - fc - r[1] / (1 + r[4]));
+        fy = (sgn > 0) ? h * R_TAN(edge - fc + r[1] / (1 + r[4]))
+                       : h * R_TAN(edge - fc - r[1] / (1 + r[4]));
     else
-        fy = h * tan(edge - fc / (1 + r[4]));
+        fy = h * R_TAN(edge - fc / (1 + r[4]));
     r[1] += r[0] * fx;
     r[3] -= r[2] * fy;
 }
 
 /* diff_bend_fringe.c:1-52 (bdiff == NULL) */
-static void o_edge_rad(double *r, double h, double edge, double fint, double gap, int method,
-                       double sgn) {
-    double pn = 1.0 / (1.0 + r[4]);
-    double psi = 0.0, fy;
+static void o_edge_rad(real *r, real h, real edge, real fint, real gap, int method,
+                       real sgn) {
+    real pn = 1.0 / (1.0 + r[4]);
+    real psi = 0.0, fy;
     if (!((fint == 0.0) || (gap == 0.0) || (method == 0))) {
-        double se = sin(edge), ce = cos(edge);
+        real se = R_SIN(edge), ce = R_COS(edge);
         psi = h * gap * fint * (1.0 + se * se) / ce;
     }
-    double fx = h * tan(edge);
+    real fx = h * R_TAN(edge);
     if (method == 2)
-        fy = h * tan(edge - psi * pn) * pn;
+        fy = h * R_TAN(edge - psi * pn) * pn;
     else if (method == 3)
-        fy = h * tan(edge - psi + sgn * r[1] * pn);
+        fy = h * R_TAN(edge - psi + sgn * r[1] * pn);
     else
-        fy = h * tan(edge - psi * pn);
+        fy = h * R_TAN(edge - psi * pn);
     r[1] += r[0] * fx;
     r[3] -= r[2] * fy;
 }
@@ -307,20 +324,20 @@ static double o_gamma(double energy, double rest) {
 /* StrMPole/BndMPole (Rad) Symplectic4: StrMPoleSymplectic4Pass.c:29-109,
  * BndMPoleSymplectic4Pass.c:38-129, StrMPoleSymplectic4RadPass.c:30-115,
  * BndMPoleSymplectic4RadPass.c:39-128 */
-static void o_multipole(double *r, const OElem *e, const double *A, const double *B, int bend,
-                        int rad, double radc) {
-    double le = e->Length;
-    double SL = le / e->NumIntSteps;
-    double L1 = SL * O_DRIFT1, L2 = SL * O_DRIFT2, K1 = SL * O_KICK1, K2 = SL * O_KICK2;
+static void o_multipole(real *r, const OElem *e, const real *A, const real *B, int bend,
+                        int rad, real radc) {
+    real le = e->Length;
+    real SL = le / e->NumIntSteps;
+    real L1 = SL * O_DRIFT1, L2 = SL * O_DRIFT2, K1 = SL * O_KICK1, K2 = SL * O_KICK2;
     int n = e->MaxOrder;
-    double h = bend ? e->BendingAngle / e->Length : 0.0;
+    real h = bend ? e->BendingAngle / e->Length : 0.0;
     int lin_in = (e->fringeIntM0 && e->fringeIntP0 && e->FringeQuadEntrance == 2);
     int lin_out = (e->fringeIntM0 && e->fringeIntP0 && e->FringeQuadExit == 2);
-    double s = e->Scaling;
-    double nl1 = 0, nl2 = 0;
+    real s = e->Scaling;
+    real nl1 = 0, nl2 = 0;
     if (s != 1.0) o_pref(r, s);
     if (!rad) {
-        double pn = 1.0 / (1.0 + r[4]);
+        real pn = 1.0 / (1.0 + r[4]);
         nl1 = L1 * pn;
         nl2 = L2 * pn;
     }
@@ -371,8 +388,8 @@ static void o_multipole(double *r, const OElem *e, const double *A, const double
 }
 
 /* ThinMPolePass.c:28-70 */
-static void o_thin(double *r, const OElem *e, const double *A, const double *B) {
-    double s = e->Scaling;
+static void o_thin(real *r, const OElem *e, const real *A, const real *B) {
+    real s = e->Scaling;
     if (s != 1.0) o_pref(r, s);
     if (e->T1) o_addv(r, e->T1);
     if (e->R1) o_mulmv(r, e->R1);
@@ -388,23 +405,23 @@ static void o_thin(double *r, const OElem *e, const double *A, const double *B) 
 }
 
 /* attrackfunc.c:5-42 trackRFCavity, via RFCavityPass.c:359-392 */
-static void o_rf(double *r, const OElem *e, double nv, double hn, int nturn, double T0) {
-    double le = e->Length, f = e->Frequency, lag = e->TimeLag, phi = e->PhaseLag;
+static void o_rf(real *r, const OElem *e, real nv, real hn, int nturn, real T0) {
+    real le = e->Length, f = e->Frequency, lag = e->TimeLag, phi = e->PhaseLag;
     if (le == 0) {
         if (nv != 0)
-            r[4] += -nv * sin(O_TWOPI * f * ((r[5] - lag) / O_C0 - (hn / f - T0) * nturn) - phi);
+            r[4] += -nv * R_SIN(O_TWOPI * f * ((r[5] - lag) / O_C0 - (hn / f - T0) * nturn) - phi);
     } else {
-        double half = le / 2;
+        real half = le / 2;
         o_drift6(r, half);
         if (nv != 0.0)
-            r[4] += -nv * sin(O_TWOPI * f * ((r[5] - lag) / O_C0 - (hn / f - T0) * nturn) - phi);
+            r[4] += -nv * R_SIN(O_TWOPI * f * ((r[5] - lag) / O_C0 - (hn / f - T0) * nturn) - phi);
         o_drift6(r, half);
     }
 }
 
 /* CorrectorPass.c:25-90 */
-static void o_corr(double *r, const OElem *e) {
-    double xk = e->KickAngle[0], yk = e->KickAngle[1], le = e->Length, s = e->Scaling;
+static void o_corr(real *r, const OElem *e) {
+    real xk = e->KickAngle[0], yk = e->KickAngle[1], le = e->Length, s = e->Scaling;
     if (s != 1.0) o_pref(r, s);
     if (le == 0.0) {
         if (e->T1) o_addv(r, e->T1);
@@ -414,8 +431,8 @@ static void o_corr(double *r, const OElem *e) {
         r[1] += xk;
         r[3] += yk;
     } else {
-        double pn = 1.0 / (1.0 + r[4]);
-        double nl = le * pn;
+        real pn = 1.0 / (1.0 + r[4]);
+        real nl = le * pn;
         if (e->T1) o_addv(r, e->T1);
         if (e->R1) o_mulmv(r, e->R1);
         if (e->RApertures) o_rect_ap(r, e->RApertures);
@@ -434,7 +451,7 @@ static void o_corr(double *r, const OElem *e) {
 }
 
 /* DriftPass.c:16-48 */
-static void o_driftpass(double *r, const OElem *e) {
+static void o_driftpass(real *r, const OElem *e) {
     if (e->T1) o_addv(r, e->T1);
     if (e->R1) o_mulmv(r, e->R1);
     if (e->RApertures) o_rect_ap(r, e->RApertures);
@@ -447,7 +464,7 @@ static void o_driftpass(double *r, const OElem *e) {
 }
 
 /* IdentityPass.c:20-43 */
-static void o_identity(double *r, const OElem *e) {
+static void o_identity(real *r, const OElem *e) {
     if (e->T1) o_addv(r, e->T1);
     if (e->R1) o_mulmv(r, e->R1);
     if (e->RApertures) o_rect_ap(r, e->RApertures);
@@ -461,8 +478,8 @@ static void o_identity(double *r, const OElem *e) {
  * into the coefficient arrays and restores them afterwards), the RF harmonic
  * number round(F*T0) and the normalised voltage. */
 typedef struct {
-    double A[64], B[64];
-    double nv, hn, radc;
+    real A[64], B[64];
+    real nv, hn, radc;
 } OPrep;
 
 static void o_prepare(const OElem *e, OPrep *p, double energy, double rest, double T0) {
@@ -478,20 +495,20 @@ static void o_prepare(const OElem *e, OPrep *p, double energy, double rest, doub
                 p->B[0] -= e->KickAngle[0];
                 p->A[0] += e->KickAngle[1];
             } else {
-                p->B[0] -= sin(e->KickAngle[0]) / e->Length;
-                p->A[0] += sin(e->KickAngle[1]) / e->Length;
+                p->B[0] -= R_SIN(e->KickAngle[0]) / e->Length;
+                p->A[0] += R_SIN(e->KickAngle[1]) / e->Length;
             }
         }
     }
     if (e->pass == O_STRMPOLE_RAD || e->pass == O_BNDMPOLE_RAD)
-        p->radc = O_RAD_CONST * pow(o_gamma(energy, rest), 3);
+        p->radc = O_RAD_CONST * R_POW(o_gamma(energy, rest), 3);
     if (e->pass == O_RFCAVITY) {
-        p->hn = round(e->Frequency * T0);
+        p->hn = R_ROUND(e->Frequency * T0);
         p->nv = e->Voltage / energy;
     }
 }
 
-static void o_element(double *r, const OElem *e, const OPrep *p, int nturn, double T0) {
+static void o_element(real *r, const OElem *e, const OPrep *p, int nturn, double T0) {
     if (isnan(r[0])) return;
     switch (e->pass) {
         case O_IDENTITY: o_identity(r, e); break;
@@ -509,14 +526,18 @@ static void o_element(double *r, const OElem *e, const OPrep *p, int nturn, doub
 }
 
 /* pyat/at.c:123 */
-static int o_bad(const double *r) {
+static int o_bad(const real *r) {
     for (int k = 0; k < 6; k++)
-        if (!isfinite(r[k]) || (fabs(r[k]) > 1 && k < 5)) return 1;
+        if (!isfinite(r[k]) || (R_FABS(r[k]) > 1 && k < 5)) return 1;
     return 0;
 }
 
+static void o_put6(double *dst, const real *src) {
+    for (int k = 0; k < 6; k++) dst[k] = (double)src[k];
+}
+
 /* The engine of pyat/at.c:596-654 for one particle; returns 0. */
-static void o_particle(double *r, const OElem *el, const OPrep *pp, int nelem, int nturns,
+static void o_particle(real *r, const OElem *el, const OPrep *pp, int nelem, int nturns,
                        int turn0, int start, int end, const uint32_t *refs, int nref,
                        int losses, int check, double T0, double *rout, int64_t np, int64_t p,
                        uint8_t *lost, uint32_t *lturn, uint32_t *lelem, double *lcoord) {
@@ -529,7 +550,7 @@ static void o_particle(double *r, const OElem *el, const OPrep *pp, int nelem, i
         uint32_t next = (ri < nref) ? refs[ri++] : 0x7fffffffu;
         for (int i = s0; i < end; i++) {
             if ((uint32_t)i == next) {
-                if (rout) memcpy(rout + 6 * (p + np * slot), r, 6 * sizeof(double));
+                if (rout) o_put6(rout + 6 * (p + np * slot), r);
                 slot++;
                 next = (ri < nref) ? refs[ri++] : 0x7fffffffu;
             }
@@ -540,7 +561,7 @@ static void o_particle(double *r, const OElem *el, const OPrep *pp, int nelem, i
                     is_lost = 1;
                     lturn[p] = (uint32_t)nturn;
                     lelem[p] = (uint32_t)i;
-                    memcpy(lcoord + 6 * p, r, 6 * sizeof(double));
+                    o_put6(lcoord + 6 * p, r);
                     r[0] = NAN; r[1] = 0; r[2] = 0; r[3] = 0; r[4] = 0; r[5] = 0;
                 }
             } else if (isfinite(r[0]) && o_bad(r)) {
@@ -548,11 +569,18 @@ static void o_particle(double *r, const OElem *el, const OPrep *pp, int nelem, i
             }
         }
         if ((uint32_t)nelem == next) {
-            if (rout) memcpy(rout + 6 * (p + np * slot), r, 6 * sizeof(double));
+            if (rout) o_put6(rout + 6 * (p + np * slot), r);
             slot++;
         }
     }
     if (losses) lost[p] = (uint8_t)is_lost;
+}
+
+static OPrep *o_prepare_all(const OElem *el, int nelem, double energy, double rest, double T0) {
+    OPrep *pp = (OPrep *)calloc((size_t)(nelem > 0 ? nelem : 1), sizeof(OPrep));
+    if (!pp) return NULL;
+    for (int i = 0; i < nelem; i++) o_prepare(&el[i], &pp[i], energy, rest, T0);
+    return pp;
 }
 
 /* Track np particles (6, np Fortran order) in place.  Mirrors at_atpass. */
@@ -560,9 +588,8 @@ int oracle_track(const OElem *el, int nelem, double *r, int64_t np, int nturns, 
                  int start, int end, const uint32_t *refs, int nref, int losses, int check,
                  double energy, double rest, double T0, double *rout, uint8_t *lost,
                  uint32_t *lturn, uint32_t *lelem, double *lcoord, int nthreads) {
-    OPrep *pp = (OPrep *)calloc((size_t)(nelem > 0 ? nelem : 1), sizeof(OPrep));
+    OPrep *pp = o_prepare_all(el, nelem, energy, rest, T0);
     if (!pp) return -1;
-    for (int i = 0; i < nelem; i++) o_prepare(&el[i], &pp[i], energy, rest, T0);
     if (losses) {
         memset(lost, 0, (size_t)np);
         memset(lturn, 0, (size_t)np * 4);
@@ -571,8 +598,11 @@ int oracle_track(const OElem *el, int nelem, double *r, int64_t np, int nturns, 
     }
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads > 0 ? nthreads : 1)
     for (int64_t p = 0; p < np; p++) {
-        o_particle(r + 6 * p, el, pp, nelem, nturns, turn0, start, end, refs, nref, losses, check,
+        real buf[6];
+        for (int k = 0; k < 6; k++) buf[k] = r[6 * p + k];
+        o_particle(buf, el, pp, nelem, nturns, turn0, start, end, refs, nref, losses, check,
                    T0, rout, np, p, lost, lturn, lelem, lcoord);
+        o_put6(r + 6 * p, buf);
     }
     free(pp);
     return 0;

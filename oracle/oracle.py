@@ -21,6 +21,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "oracle.c")
 LIB = os.path.join(HERE, "liboracle.so")
+SRC_Q = os.path.join(HERE, "oracle_q.c")
+LIB_Q = os.path.join(HERE, "liboracle_q.so")
 
 PASSES = {
     "IdentityPass": 0, "DriftPass": 1, "StrMPoleSymplectic4Pass": 2,
@@ -49,17 +51,29 @@ class OElem(C.Structure):
     ]
 
 
+def _stale(lib, srcs):
+    return not os.path.exists(lib) or any(os.path.getmtime(lib) < os.path.getmtime(s)
+                                          for s in srcs)
+
+
 def build(force: bool = False) -> str:
-    """Compile the C restatement (ISO C99, no FMA contraction, OpenMP)."""
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+    """Compile the C restatement (ISO C99, no FMA contraction, OpenMP), and
+    its binary128 variant for high-precision finite differences."""
+    if force or _stale(LIB, [SRC]):
         cmd = ["gcc", "-O2", "-std=c99", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
                "-fPIC", "-shared", SRC, "-o", LIB + ".tmp", "-lm"]
         subprocess.run(cmd, check=True)
         os.replace(LIB + ".tmp", LIB)
+    if force or _stale(LIB_Q, [SRC, SRC_Q]):
+        cmd = ["gcc", "-O2", "-std=gnu99", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
+               "-fPIC", "-shared", SRC_Q, "-o", LIB_Q + ".tmp", "-lquadmath", "-lm"]
+        subprocess.run(cmd, check=True)
+        os.replace(LIB_Q + ".tmp", LIB_Q)
     return LIB
 
 
 _lib = None
+_lib_q = None
 
 
 def _load():
@@ -75,6 +89,19 @@ def _load():
         f.restype = C.c_int
         _lib = L
     return _lib
+
+
+def _load_q():
+    global _lib_q
+    if _lib_q is None:
+        build()
+        L = C.CDLL(LIB_Q)
+        f = L.oracle_track_hilo
+        f.argtypes = [C.POINTER(OElem), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                      C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int]
+        f.restype = C.c_int
+        _lib_q = L
+    return _lib_q
 
 
 def _arr(el, name, keep):
@@ -167,6 +194,31 @@ def track(line, r, nturns, refpts=None, turn=0, energy=0.0, rest_energy=0.0, los
     if losses:
         ld = {"islost": lost.astype(bool), "turn": lturn, "elem": lelem, "coord": lcoord}
     return rout, ld
+
+
+def track_quad(line, r, nturns, turn=0, energy=0.0, rest_energy=0.0, nthreads=None):
+    """Track the (6, N) array ``r`` (not modified) for whole turns with the
+    oracle's integrators in binary128; returns ``(hi, lo)``, two (6, N)
+    double arrays whose sum is the binary128 result.  For finite differences
+    of the map far below double's rounding floor."""
+    lib = _load_q()
+    keep: list = []
+    els = _elements(line, keep)
+    ring_length = 0.0
+    for e in line:
+        ring_length += float(getattr(e, "Length", 0.0))
+    T0 = ring_length / C0
+    rin = np.asfortranarray(r, dtype=np.float64)
+    npart = rin.size // 6
+    hi = np.empty((6, npart), dtype=np.float64, order="F")
+    lo = np.empty((6, npart), dtype=np.float64, order="F")
+    if nthreads is None:
+        nthreads = os.cpu_count() or 1
+    rc = lib.oracle_track_hilo(els, len(line), rin.ctypes.data, hi.ctypes.data, lo.ctypes.data,
+                               npart, nturns, turn, energy, rest_energy, T0, nthreads)
+    if rc != 0:
+        raise MemoryError("oracle allocation failed")
+    return hi, lo
 
 
 def ext_suffix() -> str:

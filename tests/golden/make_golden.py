@@ -119,6 +119,27 @@ def fodo_fixture():
     np.savez_compressed(os.path.join(HERE, "fodo_rad_20turns.npz"), rin=r0, rout_final=r)
 
 
+def m66_fixture():
+    """The reference's closed orbit (find_orbit6) and one-turn matrix
+    (find_m66, pyat/at/physics/matrix.py:105-165: central differences with
+    XYStep/DPStep) of the FODO ring, for the exact-derivative Jacobian."""
+    sys.path.insert(0, REPO)
+    from at_b200 import rings
+    line = []
+    for e in rings.fodo_ring():
+        d = vars_of(e)
+        if d["PassMethod"] == "RFCavityPass":
+            # the reference finds its cavities by class
+            line.append(at.RFCavity(d["FamName"], d["Length"], d["Voltage"], d["Frequency"],
+                                    d["HarmNumber"], d["Energy"], TimeLag=d["TimeLag"]))
+        else:
+            line.append(ref_element(d))
+    lat = at.Lattice(line, energy=3e9, particle=at.Particle("electron"), periodicity=1)
+    orbit, _ = at.find_orbit6(lat)
+    m66, _ = at.find_m66(lat, orbit=orbit)
+    np.savez_compressed(os.path.join(HERE, "fodo_m66.npz"), orbit=orbit, m66=m66)
+
+
 def vars_of(e):
     d = {}
     for k, v in vars(e).items():
@@ -184,4 +205,5 @@ if __name__ == "__main__":
     fodo_fixture()
     sink_fixture()
     hmba_fixture()
+    m66_fixture()
     print("golden fixtures written to", HERE)

@@ -193,14 +193,17 @@ def test_pipelined_segments_match_resident(mode):
 def test_large_ring_one_turn():
     """The radiating large ring (misaligned, 1954 elements) against the oracle.
 
-    exact: 1e-14.  fast: 2e-13 -- FMA contraction alone sets the floor here:
-    the oracle's own C source compiled with -ffp-contract=fast -mfma differs
-    from the reference order by 1.08e-13 (y) after one turn of this ring."""
+    exact: 1e-13, the one-turn bound; the exact kernel differs from the
+    oracle only through CUDA's sin/tan against the C library's (a few 1e-14
+    after one turn of this ring).  fast: 2e-13 -- FMA contraction alone sets
+    the floor here: the oracle's own C source compiled with
+    -ffp-contract=fast -mfma differs from the reference order by 1.08e-13 (y)
+    after one turn of this ring."""
     ring = rings.large_ring()
     r0 = rings.large_ring_bunch(2048)
     ro = r0.copy(order="F")
     oracle.track(ring, ro, 1, energy=ring.energy, rest_energy=ring.particle.rest_energy)
-    for mode, tol in (("exact", 1e-14), ("fast", 2e-13)):
+    for mode, tol in (("exact", 1e-13), ("fast", 2e-13)):
         rg = r0.copy(order="F")
         _gpu_track(ring, rg, 1, ring.energy, ring.particle.rest_energy, mode)
         assert scale_rel_diff(rg, ro) <= tol, mode
