@@ -58,6 +58,9 @@ def _args():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving trace")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--no-diff", action="store_true", help="skip the tangent-kernel timing")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-variant run")
+    ap.add_argument("--batch-turn-scale", type=float, default=0.01,
+                    help="scale of the batched variants' turn counts (1.0: 500-5000 turns)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -371,6 +374,9 @@ def run_b200(a):
     dif = None
     if world == 1 and not a.no_diff:
         dif = run_diff(local)
+    bat = None
+    if world == 1 and not a.no_batch:
+        bat = run_batching(local, mode, a.batch_turn_scale)
 
     traffic = None
     prof = os.path.join(REPO, "profiles", "traffic_%s.json" % a.workload)
@@ -390,7 +396,7 @@ def run_b200(a):
                          "peak_source": "measured live: atb_fp64_peak DFMA chains on this GPU",
                          "flops_per_particle_turn": fpt, "survivor_particle_turns": survivors},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps, "clocks": clk,
-            "serving": serve, "differentiation": dif,
+            "serving": serve, "differentiation": dif, "batching": bat,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -430,6 +436,61 @@ def run_serving(nreq, mode, device):
             "plain_drop_in_sequential": dict(sq, particle_turns_per_s=pt / wall_seq,
                                              wall_s=wall_seq),
             "results_identical": bool(same)}
+
+
+def _survivor_turns(ld, nturns):
+    lost = ld["islost"]
+    return float(np.where(lost, ld["turn"].astype(np.float64) + 1.0, float(nturns)).sum())
+
+
+def run_batching(device, mode, turn_scale):
+    """The batched-variant workload: 256 error-seeded copies of the large
+    ring (seeds 2-257), each with N_i in [1024, 16384] particles on an x-y
+    dynamic-aperture grid at delta in {-3 %, 0, +3 %} and T_i in [500, 5000]
+    turns scaled by ``turn_scale``, as ONE graph-captured persistent launch
+    (launch shape from the autotuner), against the plain drop-in called once
+    per variant on the same jobs."""
+    from at_b200 import rings, tracking
+    from at_b200.batch import BatchTracker
+
+    work = rings.batch_workload(256, first_seed=2, turn_scale=turn_scale, seed=0)
+    lats = [rings.large_ring_variant(s) for s, _, _ in work]
+    parts = [rings.da_grid(n, seed=s) for s, n, _ in work]
+    turns = [t for _, _, t in work]
+    t0 = time.perf_counter()
+    bt = BatchTracker(lats, parts, turns, mode=mode, tune=True, graph=True, device=device)
+    setup = time.perf_counter() - t0
+    try:
+        bt.run()
+        bt.reset()
+        dt = bt.run()
+        w0 = time.perf_counter()
+        bt.reset()
+        bt.run()
+        wall_batch = time.perf_counter() - w0
+        res = bt.results()
+        tuning = bt.tuning
+    finally:
+        bt.close()
+    pt = sum(n * t for (_, n, t) in work)
+    surv = sum(_survivor_turns(ld, t) for (_, ld), t in zip(res, turns))
+    t0 = time.perf_counter()
+    same = True
+    for k, (lat, p, t) in enumerate(zip(lats, parts, turns)):
+        r = p.copy(order="F")
+        tracking.gpupass(lat, r, t, losses=True, mode=mode, gpu_pool=[device])
+        if k % 32 == 0:
+            same = same and bool(np.array_equal(r, res[k][0], equal_nan=True))
+    seq = time.perf_counter() - t0
+    return {"variants": len(work), "particles": int(sum(n for _, n, _ in work)),
+            "turns": "U{500..5000} x %g" % turn_scale, "particle_turns": pt,
+            "survivor_particle_turns": surv,
+            "one_launch": {"device_s": dt, "wall_s_incl_reset": wall_batch,
+                           "particle_turns_per_s": pt / dt,
+                           "survivor_particle_turns_per_s": surv / dt},
+            "plain_drop_in_per_variant": {"wall_s": seq, "particle_turns_per_s": pt / seq},
+            "setup_s_compile_upload_tune_capture": setup,
+            "autotune": tuning, "results_identical_sampled": same}
 
 
 def run_diff(device, n=65536):
