@@ -599,6 +599,29 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
                     }
                 }
             }
+            /* a tile whose particles are all lost stops early (nothing it
+               would still compute is observable without refpts snapshots) */
+            if (J.nref == 0 && tt + 1 < J.nturns) {
+                const bool live = active && !isnan(r.x) && !(J.losses && lost);
+                if (!__syncthreads_or(live)) {
+                    if (!resident) {
+                        /* wait for the copies this tile has in flight: after q
+                           consumed segments, segments [0, min(nq, q + 2)) were
+                           issued, buffer b holding the ones with index % 2 == b */
+                        const long long issued = (q + 2 < nq) ? q + 2 : nq;
+                        for (int b = 0; b < 2; ++b) {
+                            long long pending = (issued - b + 1) / 2 - (q - b + 1) / 2;
+                            for (; pending > 0; --pending) {
+                                if (!mbar_wait_bounded(&bars[b], use_count[b] & 1u))
+                                    timed_out = true;
+                                use_count[b]++;
+                            }
+                        }
+                        __syncthreads();
+                    }
+                    break;
+                }
+            }
         }
         if (timed_out) {
             /* drain our own copies still in flight before leaving */

@@ -117,14 +117,19 @@ def _rot(theta: float) -> np.ndarray:
 
 
 def large_ring(seed: int = 1, ncells: int = 32, misalign: bool = True,
-               radiation: bool = True) -> E.Lattice:
+               radiation: bool = True, design_seed: int | None = None) -> E.Lattice:
     """The radiating large ring: 32 cells x 61 elements + 2 RF = 1954 elements.
 
-    Each magnet gets T1 = -(dx, 0, dy, 0, 0, 0), T2 = -T1 and R1/R2 = x-y
-    rotations by +/-theta with dx, dy ~ N(0, 30 um) and theta ~ N(0, 100 urad),
-    drawn from ``default_rng(seed)`` after the 7 dipole gradients."""
+    The 7 dipole gradients are the first draws of ``default_rng(seed)``
+    (of ``default_rng(design_seed)`` when given: error-seeded copies keep the
+    design of seed 1 and redraw only the errors).  Each magnet gets
+    T1 = -(dx, 0, dy, 0, 0, 0), T2 = -T1 and R1/R2 = x-y rotations by +/-theta
+    with dx, dy ~ N(0, 30 um) and theta ~ N(0, 100 urad), drawn from
+    ``default_rng(seed)`` after those 7 draws."""
     rng = np.random.default_rng(seed)
     kdip = rng.uniform(-0.5, 0.5, 7)
+    if design_seed is not None:
+        kdip = np.random.default_rng(design_seed).uniform(-0.5, 0.5, 7)
     angle = 2 * math.pi / (ncells * 7)
     spm = "StrMPoleSymplectic4RadPass" if radiation else "StrMPoleSymplectic4Pass"
     bpm = "BndMPoleSymplectic4RadPass" if radiation else "BndMPoleSymplectic4Pass"
@@ -199,11 +204,12 @@ def large_ring_bunch(n: int, seed: int = 0) -> np.ndarray:
 # batched variants of the large ring (dynamic-aperture scans)
 # ---------------------------------------------------------------------------
 def large_ring_variant(seed: int, strength_rel: float = 1e-3) -> E.Lattice:
-    """An error-seeded copy of the large ring: misalignments drawn from
-    ``default_rng(seed)`` as in ``large_ring`` and, from the same generator,
-    0.1 % Gaussian errors on every magnet's main strength (dipole and quadrupole
-    gradients, sextupole and octupole coefficients)."""
-    ring = large_ring(seed=seed)
+    """An error-seeded copy of the large ring: the design of seed 1 (its
+    dipole gradients), misalignments drawn from ``default_rng(seed)`` as in
+    ``large_ring``, and 0.1 % Gaussian errors on every magnet's main strength
+    (dipole and quadrupole gradients, sextupole and octupole coefficients)
+    from ``default_rng(seed + 100000)``."""
+    ring = large_ring(seed=seed, design_seed=1)
     rng = np.random.default_rng(seed + 100_000)
     for e in ring:
         if e.PassMethod in ("StrMPoleSymplectic4RadPass", "BndMPoleSymplectic4RadPass",

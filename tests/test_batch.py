@@ -42,6 +42,20 @@ def test_variant_changes_only_errors():
     assert qa.PolynomB[1] != qb.PolynomB[1]
     assert abs(qa.PolynomB[1] / rings.LARGE_KF - 1) < 1e-2
     assert not np.array_equal(qa.T1, qb.T1)
+    # the design (dipole gradients) is seed 1's; only the errors differ
+    d1 = [e.PolynomB[1] for e in rings.large_ring(seed=1) if e.FamName == "B"][:7]
+    da = [e.PolynomB[1] for e in a if e.FamName == "B"][:7]
+    np.testing.assert_allclose(da, d1, rtol=1e-2)
+
+
+def test_variant_is_stable_on_the_oracle():
+    """An error-seeded copy keeps a DA grid's core alive (oracle, 5 turns)."""
+    from oracle import oracle
+    lat = rings.large_ring_variant(7)
+    r = rings.da_grid(60, seed=7, deltas=(0.0,), xmax=1e-3, ymax=5e-4)
+    _, ld = oracle.track(lat, r, 5, energy=lat.energy, rest_energy=lat.particle.rest_energy,
+                         losses=True)
+    assert ld["islost"].mean() < 0.2
 
 
 @pytest.mark.gpu

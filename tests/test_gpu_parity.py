@@ -231,3 +231,33 @@ def test_find_orbit6_matches_constant():
     ring = rings.large_ring()
     orb = physics.find_orbit6(ring)
     np.testing.assert_allclose(orb, rings.LARGE_ORBIT, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("ring_name", ["fodo", "large"])
+def test_all_lost_tiles_stop_early(ring_name):
+    """Tiles whose particles are all lost leave the turn loop early (after
+    draining their in-flight table copies when the table streams in
+    segments); the results equal a run that cannot stop early (with a
+    refpts snapshot) and the oracle's loss map."""
+    if ring_name == "fodo":
+        ring, en, rest = rings.fodo_ring(), 3e9, ELECTRON_REST
+        r0 = rings.gaussian(2048, seed=8)
+        nt = 40
+    else:
+        ring = rings.large_ring()
+        en, rest = ring.energy, ring.particle.rest_energy
+        r0 = rings.large_ring_bunch(2048, seed=8)
+        nt = 6
+    r0[:, 256:768] *= 1e3            # two whole tiles lost in the first turn
+    ra = r0.copy(order="F")
+    _, la, _ = _gpu_track(ring, ra, nt, en, rest, "exact", losses=True)
+    rb = r0.copy(order="F")
+    _gpu_track(ring, rb, nt, en, rest, "exact", losses=True,
+               refpts=np.array([0], dtype=np.uint32))
+    np.testing.assert_array_equal(ra, rb)
+    assert la["islost"][256:768].all() and not la["islost"].all()
+    ro = r0.copy(order="F")
+    _, lo = oracle.track(ring, ro, nt, energy=en, rest_energy=rest, losses=True)
+    np.testing.assert_array_equal(la["islost"], lo["islost"])
+    np.testing.assert_array_equal(la["turn"], lo["turn"])
+    np.testing.assert_array_equal(la["elem"], lo["elem"])
