@@ -3,7 +3,10 @@
  * derivatives, with the arithmetic the integrators use (+, -, *, /, sin, tan,
  * cos, exp).  The pass-method templates in atb_physics.cuh and
  * track_kernel.cuh run unchanged on this type, which propagates the Jacobian
- * of every operation exactly (no finite differences).
+ * of every operation exactly (no finite differences).  Values are computed
+ * with the plain operators (the tangent unit is compiled without FMA
+ * contraction, so they equal the exact tracking kernel's); the derivative
+ * updates use explicit fma(), which that flag does not touch.
  */
 #ifndef ATB_DUAL_CUH
 #define ATB_DUAL_CUH
@@ -59,7 +62,7 @@ struct Dual {
         Dual r;
         r.v = a.v * b.v;
 #pragma unroll
-        for (int i = 0; i < K; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+        for (int i = 0; i < K; ++i) r.d[i] = fma(a.d[i], b.v, a.v * b.d[i]);
         return r;
     }
     friend __device__ __forceinline__ Dual operator/(const Dual& a, const Dual& b) {
@@ -67,7 +70,7 @@ struct Dual {
         r.v = a.v / b.v;
         const double ib = 1.0 / b.v;
 #pragma unroll
-        for (int i = 0; i < K; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
+        for (int i = 0; i < K; ++i) r.d[i] = fma(-r.v, b.d[i], a.d[i]) * ib;
         return r;
     }
     /* mixed forms keep a constant operand from carrying zero derivatives */

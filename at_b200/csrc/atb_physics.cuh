@@ -165,17 +165,31 @@ __device__ __forceinline__ void fastdrift(P6T<T>& r, const T& nl, const T& c2) {
 /* The Horner recursion shared by every multipole kick
  * (driftkick.c:51-115, diff_str_kick.c:33-40, diff_bnd_kick.c:40-47):
  * Re + i Im = sum_n (B_n + i A_n)(x + i y)^n, highest order first. */
+/* one Horner step (re, im) <- (re, im)(x + i y) + (b + i a).  The fast
+ * kernels evaluate it as two FMA chains per component (a different
+ * association from the reference, within an ulp); the others keep the
+ * reference's expression. */
+template <class T>
+__device__ __forceinline__ void horner_step(T& re, T& im, const T& x, const T& y, double b,
+                                            double a) {
+#if ATB_FAST
+    const T ret = fma(re, x, fma(-im, y, b));
+    im = fma(im, x, fma(re, y, a));
+    re = ret;
+#else
+    T ret = re * x - im * y + b;
+    im = im * x + re * y + a;
+    re = ret;
+#endif
+}
+
 template <int MO, class T>
 __device__ __forceinline__ void horner_fixed(const double* A, const double* B, const T& x,
                                              const T& y, T& re, T& im) {
     re = B[MO];
     im = A[MO];
 #pragma unroll
-    for (int i = MO - 1; i >= 0; --i) {
-        T ret = re * x - im * y + B[i];
-        im = im * x + re * y + A[i];
-        re = ret;
-    }
+    for (int i = MO - 1; i >= 0; --i) horner_step(re, im, x, y, B[i], A[i]);
 }
 
 template <class T>
@@ -183,11 +197,7 @@ __device__ __forceinline__ void horner_dyn(const double* A, const double* B, int
                                            const T& y, T& re, T& im) {
     re = B[mo];
     im = A[mo];
-    for (int i = mo - 1; i >= 0; --i) {
-        T ret = re * x - im * y + B[i];
-        im = im * x + re * y + A[i];
-        re = ret;
-    }
+    for (int i = mo - 1; i >= 0; --i) horner_step(re, im, x, y, B[i], A[i]);
 }
 
 /* Tangent kernel only: the explicit partial of the field with respect to the
@@ -283,28 +293,40 @@ __device__ __forceinline__ void bndthinkick(P6T<T>& r, const PL& pl, double L, d
     r.ct += lirho * r.x;
 }
 
-/* Radiating kicks.  ``pn`` carries 1/(1+delta) between steps in FAST mode. */
+/* Radiating kicks.  ``pn`` carries 1/(1+delta) between steps in FAST mode,
+ * and ``rL`` = radc * L is folded once per element.  The FAST forms group the
+ * energy-loss product as (rL q)(h vn) opd^2, q = B2perp before the 1/(1+s)
+ * normalisation, and evaluate 1/(1+s) for s = x'^2 + y'^2 < 1e-5 by its
+ * series 1 - s + s^2 - s^3 (truncation below 1e-20). */
+
+__device__ __forceinline__ double inv_one_plus_small(double s) {
+    if (s < 1e-5) {
+        const double t = fma(-s, 1.0 - s, 1.0);
+        return fma(-s, t, 1.0);
+    }
+    return rcp_nr(1.0 + s);
+}
 
 /* diff_str_kick.c:19-83 with B2perp of diff_str_kick.c:1-17 (bdiff == NULL) */
 template <bool FAST, class PL, class T>
 __device__ __forceinline__ void str_kick_rad(P6T<T>& r, const PL& pl, double L, double radc,
-                                             T& pn) {
+                                             double rL, T& pn) {
     T re, im;
     pl.field(r.x, r.y, re, im);
     if constexpr (FAST) {
-        double xpr = r.px * pn;
-        double ypr = r.py * pn;
-        double s = xpr * xpr + ypr * ypr;
-        double vn = rcp_nr(1.0 + s);
-        double cr = im * ypr - re * xpr;
-        double b2p = (re * re + im * im + cr * cr) * vn;
-        double opd = 1.0 + r.dp;
-        double factor = (1.0 + 0.5 * s) * (opd * opd) * L;
-        r.dp -= radc * b2p * factor;
-        opd = 1.0 + r.dp;
-        pn = rcp_nr(opd);
-        r.px = xpr * opd - L * re;
-        r.py = ypr * opd + L * im;
+        const double xpr = r.px * pn;
+        const double ypr = r.py * pn;
+        const double s = fma(xpr, xpr, ypr * ypr);
+        const double vn = inv_one_plus_small(s);
+        const double cr = fma(im, ypr, -(re * xpr));
+        const double q = fma(re, re, fma(im, im, cr * cr));
+        const double opd = 1.0 + r.dp;
+        const double h = fma(0.5, s, 1.0);
+        r.dp = fma(-(rL * q) * (h * vn), opd * opd, r.dp);
+        const double opd2 = 1.0 + r.dp;
+        pn = rcp_nr(opd2);
+        r.px = fma(xpr, opd2, -L * re);
+        r.py = fma(ypr, opd2, L * im);
     } else {
         T p_norm = 1.0 / (1.0 + r.dp);
         T xpr = r.px * p_norm;
@@ -325,27 +347,29 @@ __device__ __forceinline__ void str_kick_rad(P6T<T>& r, const PL& pl, double L, 
 /* diff_bnd_kick.c:101-174 with its B2perp (:85-99), bdiff == NULL */
 template <bool FAST, class PL, class T>
 __device__ __forceinline__ void bnd_kick_rad(P6T<T>& r, const PL& pl, double L, double irho,
-                                             double lirho, double radc, T& pn) {
+                                             double lirho, double radc, double rL, T& pn) {
     T re, im;
     pl.field(r.x, r.y, re, im);
     if constexpr (FAST) {
-        double xpr = r.px * pn;
-        double ypr = r.py * pn;
-        double hx = 1.0 + r.x * irho;
-        double s = xpr * xpr + ypr * ypr;
-        double vn = rcp_nr(hx * hx + s);
-        double by = re + irho;
-        double cr = im * ypr - by * xpr;
-        double b2p = ((by * by + im * im) * (hx * hx) + cr * cr) * vn;
-        double opd = 1.0 + r.dp;
-        double factor = (hx + 0.5 * s) * (opd * opd) * L;
-        double dp0 = r.dp;
-        r.dp -= radc * b2p * factor;
-        opd = 1.0 + r.dp;
-        pn = rcp_nr(opd);
-        r.px = xpr * opd - L * (re - (dp0 - r.x * irho) * irho);
-        r.py = ypr * opd + L * im;
-        r.ct += lirho * r.x;
+        const double xpr = r.px * pn;
+        const double ypr = r.py * pn;
+        const double hx = fma(r.x, irho, 1.0);
+        const double hx2 = hx * hx;
+        const double s = fma(xpr, xpr, ypr * ypr);
+        const double vn = rcp_nr(hx2 + s);
+        const double by = re + irho;
+        const double cr = fma(im, ypr, -(by * xpr));
+        const double q = fma(fma(by, by, im * im), hx2, cr * cr);
+        const double opd = 1.0 + r.dp;
+        const double h = fma(0.5, s, hx);
+        const double dp0 = r.dp;
+        r.dp = fma(-(rL * q) * (h * vn), opd * opd, r.dp);
+        const double opd2 = 1.0 + r.dp;
+        pn = rcp_nr(opd2);
+        const double u = fma(-fma(-r.x, irho, dp0), irho, re);
+        r.px = fma(xpr, opd2, -L * u);
+        r.py = fma(ypr, opd2, L * im);
+        r.ct = fma(lirho, r.x, r.ct);
     } else {
         T p_norm = 1.0 / (1.0 + r.dp);
         T x = r.x;

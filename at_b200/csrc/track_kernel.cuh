@@ -213,18 +213,19 @@ __device__ __forceinline__ void pass_multipole(P6T<T>& r, const Rec& e, const Pa
     const int ns = e.nsteps();
     if (RAD) {
         const double radc = e.f(ATB_SM_RADC);
+        const double rk1 = kFast ? radc * K1 : 0.0, rk2 = kFast ? radc * K2 : 0.0;
         T pn = 0.0;
         if (kFast) pn = 1.0 / (1.0 + r.dp);
         for (int m = 0; m < ns; ++m) {
             diff_drift<kFast>(r, L1, pn);
-            if (BEND) bnd_kick_rad<kFast>(r, pl, K1, irho, k1i, radc, pn);
-            else str_kick_rad<kFast>(r, pl, K1, radc, pn);
+            if (BEND) bnd_kick_rad<kFast>(r, pl, K1, irho, k1i, radc, rk1, pn);
+            else str_kick_rad<kFast>(r, pl, K1, radc, rk1, pn);
             diff_drift<kFast>(r, L2, pn);
-            if (BEND) bnd_kick_rad<kFast>(r, pl, K2, irho, k2i, radc, pn);
-            else str_kick_rad<kFast>(r, pl, K2, radc, pn);
+            if (BEND) bnd_kick_rad<kFast>(r, pl, K2, irho, k2i, radc, rk2, pn);
+            else str_kick_rad<kFast>(r, pl, K2, radc, rk2, pn);
             diff_drift<kFast>(r, L2, pn);
-            if (BEND) bnd_kick_rad<kFast>(r, pl, K1, irho, k1i, radc, pn);
-            else str_kick_rad<kFast>(r, pl, K1, radc, pn);
+            if (BEND) bnd_kick_rad<kFast>(r, pl, K1, irho, k1i, radc, rk1, pn);
+            else str_kick_rad<kFast>(r, pl, K1, radc, rk1, pn);
             diff_drift<kFast>(r, L1, pn);
         }
     } else {

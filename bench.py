@@ -58,6 +58,9 @@ def _args():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving trace")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--no-diff", action="store_true", help="skip the tangent-kernel timing")
+    ap.add_argument("--diff-only", action="store_true",
+                    help="only the tangent-kernel timing (one JSON object)")
+    ap.add_argument("--diff-particles", type=int, default=65536)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-variant run")
     ap.add_argument("--batch-turn-scale", type=float, default=0.01,
                     help="scale of the batched variants' turn counts (1.0: 500-5000 turns)")
@@ -373,7 +376,7 @@ def run_b200(a):
         serve = run_serving(a.serve_requests, mode, local)
     dif = None
     if world == 1 and not a.no_diff:
-        dif = run_diff(local)
+        dif = run_diff(local, a.diff_particles)
     bat = None
     if world == 1 and not a.no_batch:
         bat = run_batching(local, mode, a.batch_turn_scale)
@@ -563,6 +566,9 @@ def main():
     a = _defaults(_args())
     if a.impl == "reference":
         return run_reference(a)
+    if a.diff_only:
+        print(json.dumps({"differentiation": run_diff(0, a.diff_particles)}), flush=True)
+        return 0
     return run_b200(a)
 
 
