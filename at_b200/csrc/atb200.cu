@@ -37,6 +37,7 @@ extern "C" __global__ void atb_track_kernel_exact(const AtbJob*, const AtbTile*,
 extern "C" __global__ void atb_track_kernel_fast(const AtbJob*, const AtbTile*, int, int*, int*,
                                                  int);
 extern "C" __global__ void atb_tangent_kernel(const AtbTangent);
+extern "C" __global__ void atb_element_maps_kernel(const AtbElemMaps);
 
 namespace {
 
@@ -689,6 +690,30 @@ int atb_track_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t n
     /* pageable-source copies of the launch lists are staged before
        cudaMemcpyAsync returns, so the host vectors may be reused at once */
     return launch(h, jobs, h->h_tiles, smem, grid_max, mode, st);
+}
+
+int atb_element_maps(atb_handle* h, int32_t id, const double* orbits, double* m66,
+                     double* b66, double diff_const, void* stream) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Lattice* L = get_lat(h, id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    if (L->nelem == 0) return ATB_OK;
+    if (!orbits || !m66 || !b66) return fail(ATB_ERR_ARG, "NULL buffer");
+    DeviceGuard g(h->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    AtbElemMaps A;
+    std::memset(&A, 0, sizeof(A));
+    A.table = L->words.as<double>();
+    A.elem_off = L->doff.as<uint32_t>();
+    A.nelem = L->nelem;
+    A.orbits = orbits;
+    A.m66 = m66;
+    A.b66 = b66;
+    A.diff_const = diff_const;
+    const int blocks = (L->nelem + ATB_TANGENT_THREADS - 1) / ATB_TANGENT_THREADS;
+    atb_element_maps_kernel<<<blocks, ATB_TANGENT_THREADS, 0, st>>>(A);
+    ATB_CUDA(cudaGetLastError());
+    return ATB_OK;
 }
 
 int atb_tangent_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t nturns,

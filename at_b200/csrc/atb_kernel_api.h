@@ -83,4 +83,17 @@ typedef struct AtbTangent {
     uint8_t* lost;              /* optional (np): 1 if the particle was lost */
 } AtbTangent;
 
+/* Per-element transfer and diffusion matrices for a particle entering each
+ * element at orbits[6 * i]: one thread per element. */
+typedef struct AtbElemMaps {
+    const double* table;
+    const uint32_t* elem_off;
+    int32_t nelem;
+    int32_t pad;
+    const double* orbits;       /* (nelem, 6)                               */
+    double* m66;                /* (nelem, 6, 6) row-major: d out_i / d in_j */
+    double* b66;                /* (nelem, 6, 6) row-major diffusion matrix */
+    double diff_const;          /* DIF_CONST * gamma^5                      */
+} AtbElemMaps;
+
 #endif /* ATB_KERNEL_API_H */

@@ -64,6 +64,9 @@
 #define ATB_F_BM_IN_SHIFT  11          /* bend entrance method, 2 bits     */
 #define ATB_F_BM_OUT_SHIFT 13          /* bend exit method, 2 bits         */
 #define ATB_F_BM_MASK      3u
+#define ATB_F_FINT_IN      (1u << 15)  /* bend entrance FringeInt1 > 0 and FullGap > 0
+                                          (the diffusion-matrix edge term)  */
+#define ATB_F_FINT_OUT     (1u << 16)  /* bend exit FringeInt2 > 0 and FullGap > 0 */
 /* bend fringe "method" codes after host normalisation (atphyslib.c:15-79) */
 #define ATB_BM_LEGACY      0   /* method 0 or any value other than 1,2,3   */
 #define ATB_BM_1           1

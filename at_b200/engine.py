@@ -153,6 +153,13 @@ class Engine:
                                        ptr(po) if po.size else None, value_ptr, int(pe.size),
                                        jac_ptr, grad_ptr, lost_ptr, stream))
 
+    def element_maps(self, lid: int, orbits_ptr: int, m_ptr: int, b_ptr: int,
+                     diff_const: float, stream: int | None = None):
+        """Enqueue the per-element transfer and diffusion matrices for the
+        entrance orbits at ``orbits_ptr`` ((nelem, 6) device array)."""
+        check(lib().atb_element_maps(self.h, int(lid), orbits_ptr, m_ptr, b_ptr,
+                                     float(diff_const), stream))
+
     def track_batch(self, jobs: list[dict], mode=None, stream: int | None = None):
         """One persistent launch over many jobs (dicts with lattice_id, r, np,
         nturns, optional turn0 and losses=(islost, lturn, lelem, lcoord)

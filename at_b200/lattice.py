@@ -42,6 +42,16 @@ C0 = 2.99792458e8
 RE = 2.8179403205e-15
 E0_GEV = 510.99895069e-6
 RAD_CONST = 2.0 / 3.0 * RE
+ROOT_3 = 1.7320508075688772
+HBAR_C = 197.3269804e-18            # reduced Planck constant x c [GeV.m]
+# atconstants.h:30, evaluated in the same order
+DIF_CONST = 55.0 / 24.0 / ROOT_3 * HBAR_C / E0_GEV * RE
+
+
+def diffusion_constant(energy: float, rest_energy: float) -> float:
+    """DIF_CONST * gamma^5, the quantum-diffusion strength of the radiating
+    multipole passes (StrMPoleSymplectic4RadPass.c: diff_const)."""
+    return DIF_CONST * math.pow(_gamma(energy, rest_energy), 5)
 LIMIT_AMPLITUDE = 1.0
 
 _f64 = np.float64
@@ -366,6 +376,8 @@ def _multipole_common(rec: _Record, el, op: int, bend: bool):
             rec.flags |= (code & T.ATB_F_BM_MASK) << shift
             if fc == 0.0:
                 rec.flags |= fc0
+            if fint > 0 and gap > 0:
+                rec.flags |= T.ATB_F_FINT_IN if shift == T.ATB_F_BM_IN_SHIFT else T.ATB_F_FINT_OUT
         base = T.ATB_BM_POLY
     else:
         base = T.ATB_SM_POLY

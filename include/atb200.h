@@ -142,6 +142,16 @@ int atb_tangent_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np,
                        const double* param_value, int32_t nparam, double* jac, double* grad,
                        uint8_t* islost, void* stream);
 
+/* Element maps for Ohmi's envelope (device pointers, enqueued on `stream`):
+ * for a particle entering element i at orbits[6 i .. 6 i + 5], its transfer
+ * matrix m66[i] (exact derivatives, row-major d out / d in) and its radiation
+ * diffusion matrix b66[i] (row-major; zero for non-radiating pass methods),
+ * with `diff_const` = DIF_CONST gamma^5, all elements in one launch.  Replaces
+ * the per-element loop of pyat/at/physics/radiation.py:76-148 (_dmatr), i.e.
+ * find_elem_m66 and pyat/at.c:755-831 (diffusion_matrix) per element. */
+int atb_element_maps(atb_handle* h, int32_t lattice_id, const double* orbits, double* m66,
+                     double* b66, double diff_const, void* stream);
+
 /* Many lattice variants and particle sets in one persistent launch (device
  * pointers); the tiles of the longest jobs are scheduled first. */
 int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,

@@ -32,6 +32,7 @@ typedef double real;
 #define R_POW pow
 #define R_ROUND round
 #define R_FABS fabs
+#define R_SQRT sqrt
 #else
 typedef ORACLE_REAL real;
 #endif
@@ -71,6 +72,9 @@ static const double O_C0 = 2.99792458e8;
 #define O_RE 2.8179403205e-15
 #define O_E0 510.99895069e-6
 static const double O_RAD_CONST = 2.0 / 3.0 * O_RE;
+#define O_ROOT_3 1.7320508075688772
+#define O_HBAR_C 197.3269804e-18
+static const double O_DIF_CONST = 55.0 / 24.0 / O_ROOT_3 * O_HBAR_C / O_E0 * O_RE;
 
 /* ---- small vector helpers ---------------------------------------------- */
 
@@ -119,10 +123,98 @@ static void o_drift6(real *r, real L) {
     r[5] += nl * pn * (r[1] * r[1] + r[3] * r[3]) / 2;
 }
 
+/* ---- Ohmi diffusion matrix (the bdiff branch of the Rad passes) ---------
+ * B is 6x6 column-major, [i][j] at i + 6 j, as in the reference. */
+
+/* atlalib.c:92-147 ATmultmm then the row pass of ATsandwichmmt: B <- M B M' */
+static void o_sandwich(const real *M, real *B) {
+    real col[6], row[6];
+    for (int i = 0; i < 6; i++) {
+        for (int j = 0; j < 6; j++) {
+            col[j] = 0;
+            for (int k = 0; k < 6; k++) col[j] += M[j + 6 * k] * B[k + 6 * i];
+        }
+        for (int j = 0; j < 6; j++) B[j + 6 * i] = col[j];
+    }
+    for (int i = 0; i < 6; i++) {
+        for (int j = 0; j < 6; j++) {
+            row[j] = 0;
+            for (int k = 0; k < 6; k++) row[j] += B[i + 6 * k] * M[j + 6 * k];
+        }
+        for (int j = 0; j < 6; j++) B[i + 6 * j] = row[j];
+    }
+}
+
+static void o_ident(real *M) {
+    for (int m = 0; m < 36; m++) M[m] = 0.0;
+    for (int m = 0; m < 6; m++) M[m * 7] = 1.0;
+}
+
+/* diff_drift.c:1-28 drift_propagateB */
+static void o_drift_b(real nl, real xp, real yp, real *bd) {
+    real M[36];
+    o_ident(M);
+    M[6] = nl;
+    M[20] = nl;
+    M[24] = -nl * xp;
+    M[26] = -nl * yp;
+    M[11] = nl * xp;
+    M[23] = nl * yp;
+    M[29] = -nl * (xp * xp + yp * yp);
+    o_sandwich(M, bd);
+}
+
+/* diff_thinkick.c:1-33 and diff_bnd_kick.c:1-47 thinkickM (bend = 0: the
+ * straight form, without the curvature terms) */
+static void o_thinkick_m(const real *r, const real *A, const real *B, int n, real L, real h,
+                         int bend, real *bd) {
+    real M[36];
+    real in = n * A[n], rn = n * B[n];
+    for (int k = n - 1; k > 0; k--) {
+        real t = (rn * r[0] - in * r[2]) + k * B[k];
+        in = in * r[0] + rn * r[2] + k * A[k];
+        rn = t;
+    }
+    o_ident(M);
+    M[1] = -L * rn;
+    M[13] = L * in;
+    M[3] = L * in;
+    M[15] = L * rn;
+    if (bend) {
+        M[25] = L * h;
+        M[1] += -L * h * h;
+        M[5] = L * h;
+    }
+    o_sandwich(M, bd);
+}
+
+/* diff_thinkick.c:35-70 thinkickB */
+static void o_thinkick_b(const real *r, real diffc, real b2p, real factor, real *bd) {
+    real pn = 1.0 / (1.0 + r[4]);
+    real pn2 = pn * pn;
+    real b3p = b2p * R_SQRT(b2p);
+    real bb = diffc * b3p * factor / pn2;
+    real b11 = bb * (r[1] * r[1]) * pn2;
+    real b13 = bb * r[1] * r[3] * pn2;
+    real b33 = bb * (r[3] * r[3]) * pn2;
+    real b14 = bb * r[1] * pn;
+    real b34 = bb * r[3] * pn;
+    bd[7] += b11;
+    bd[19] += b13;
+    bd[9] += b13;
+    bd[21] += b33;
+    bd[10] += b14;
+    bd[25] += b14;
+    bd[22] += b34;
+    bd[27] += b34;
+    bd[28] += bb;
+}
+
 /* diff_drift.c:30-43 (its literal constants are 1.0 and 2.0) */
-static void o_ddrift(real *r, real L) {
+static void o_ddrift(real *r, real L, real *bd) {
     real pn = 1.0 / (1.0 + r[4]);
     real nl = L * pn;
+    if (bd) o_drift_b(nl, r[1] * pn, r[3] * pn, bd);
     r[0] += nl * r[1];
     r[2] += nl * r[3];
     r[5] += nl * pn * (r[1] * r[1] + r[3] * r[3]) / 2.0;
@@ -167,7 +259,7 @@ static void o_bndkick(real *r, const real *A, const real *B, real L, real h, int
 
 /* diff_str_kick.c:19-83 (bdiff == NULL) */
 static void o_strkick_rad(real *r, const real *A, const real *B, int n, real L,
-                          real radc) {
+                          real radc, real diffc, real *bd) {
     real re, im;
     o_field(r, A, B, n, &re, &im);
     real pn = 1.0 / (1.0 + r[4]);
@@ -176,6 +268,10 @@ static void o_strkick_rad(real *r, const real *A, const real *B, int n, real L,
     real vn = 1.0 / (1.0 + xp * xp + yp * yp);
     real b2 = (by * by + bx * bx + (bx * yp - by * xp) * (bx * yp - by * xp)) * vn;
     real f = (1.0 + (xp * xp + yp * yp) / 2.0) / (pn * pn) * L;
+    if (bd) {
+        o_thinkick_m(r, A, B, n, L, 0.0, 0, bd);
+        o_thinkick_b(r, diffc, b2, f, bd);
+    }
     r[4] -= radc * b2 * f;
     pn = 1.0 / (1.0 + r[4]);
     r[1] = xp / pn;
@@ -186,7 +282,7 @@ static void o_strkick_rad(real *r, const real *A, const real *B, int n, real L,
 
 /* diff_bnd_kick.c:101-174 with its B2perp (:85-99), bdiff == NULL */
 static void o_bndkick_rad(real *r, const real *A, const real *B, int n, real L,
-                          real h, real radc) {
+                          real h, real radc, real diffc, real *bd) {
     real re, im;
     o_field(r, A, B, n, &re, &im);
     real pn = 1.0 / (1.0 + r[4]);
@@ -197,6 +293,10 @@ static void o_bndkick_rad(real *r, const real *A, const real *B, int n, real L,
     real b2 = ((by * (1 + x * h)) * (by * (1 + x * h)) + (bx * (1 + x * h)) * (bx * (1 + x * h)) +
                  (bx * yp - by * xp) * (bx * yp - by * xp)) * vn;
     real f = (1.0 + x * h + (xp * xp + yp * yp) / 2.0) / (pn * pn) * L;
+    if (bd) {
+        o_thinkick_m(r, A, B, n, L, h, 1, bd);
+        o_thinkick_b(r, diffc, b2, f, bd);
+    }
     real d0 = r[4];
     r[4] -= radc * b2 * f;
     pn = 1.0 / (1.0 + r[4]);
@@ -296,7 +396,7 @@ static void o_edge(real *r, real h, real edge, real fint, real gap, int method,
 
 /* diff_bend_fringe.c:1-52 (bdiff == NULL) */
 static void o_edge_rad(real *r, real h, real edge, real fint, real gap, int method,
-                       real sgn) {
+                       real sgn, real *bd) {
     real pn = 1.0 / (1.0 + r[4]);
     real psi = 0.0, fy;
     if (!((fint == 0.0) || (gap == 0.0) || (method == 0))) {
@@ -310,6 +410,24 @@ static void o_edge_rad(real *r, real h, real edge, real fint, real gap, int meth
         fy = h * R_TAN(edge - psi + sgn * r[1] * pn);
     else
         fy = h * R_TAN(edge - psi * pn);
+    /* diff_bend_fringe.c:31-46: B propagated through the edge map */
+    if (bd) {
+        int ff = (fint > 0 && gap > 0);
+        for (int m = 0; m < 6; m++) {
+            bd[1 + 6 * m] += fx * bd[6 * m];
+            bd[3 + 6 * m] -= fy * bd[2 + 6 * m];
+        }
+        if (ff)
+            for (int m = 0; m < 6; m++)
+                bd[3 + 6 * m] -= bd[4 + 6 * m] * r[2] * (h * h + fy * fy) * psi * pn * pn / h;
+        for (int m = 0; m < 6; m++) {
+            bd[m + 6 * 1] += fx * bd[m + 6 * 0];
+            bd[m + 6 * 3] -= fy * bd[m + 6 * 2];
+        }
+        if (ff)
+            for (int m = 0; m < 6; m++)
+                bd[m + 6 * 3] -= bd[m + 6 * 4] * r[2] * (h * h + fy * fy) * psi * pn * pn / h;
+    }
     r[1] += r[0] * fx;
     r[3] -= r[2] * fy;
 }
@@ -325,7 +443,7 @@ static double o_gamma(double energy, double rest) {
  * BndMPoleSymplectic4Pass.c:38-129, StrMPoleSymplectic4RadPass.c:30-115,
  * BndMPoleSymplectic4RadPass.c:39-128 */
 static void o_multipole(real *r, const OElem *e, const real *A, const real *B, int bend,
-                        int rad, real radc) {
+                        int rad, real radc, real diffc, real *bd) {
     real le = e->Length;
     real SL = le / e->NumIntSteps;
     real L1 = SL * O_DRIFT1, L2 = SL * O_DRIFT2, K1 = SL * O_KICK1, K2 = SL * O_KICK2;
@@ -346,7 +464,7 @@ static void o_multipole(real *r, const OElem *e, const real *A, const real *B, i
     if (e->RApertures) o_rect_ap(r, e->RApertures);
     if (e->EApertures) o_ellip_ap(r, e->EApertures);
     if (bend) {
-        if (rad) o_edge_rad(r, h, e->EntranceAngle, e->FringeInt1, e->FullGap, e->FringeBendEntrance, 1.0);
+        if (rad) o_edge_rad(r, h, e->EntranceAngle, e->FringeInt1, e->FullGap, e->FringeBendEntrance, 1.0, bd);
         else o_edge(r, h, e->EntranceAngle, e->FringeInt1, e->FullGap, e->FringeBendEntrance, 1);
     }
     if (e->FringeQuadEntrance && B[1] != 0) {
@@ -355,13 +473,16 @@ static void o_multipole(real *r, const OElem *e, const real *A, const real *B, i
     }
     for (int m = 0; m < e->NumIntSteps; m++) {
         if (rad) {
-            o_ddrift(r, L1);
-            if (bend) o_bndkick_rad(r, A, B, n, K1, h, radc); else o_strkick_rad(r, A, B, n, K1, radc);
-            o_ddrift(r, L2);
-            if (bend) o_bndkick_rad(r, A, B, n, K2, h, radc); else o_strkick_rad(r, A, B, n, K2, radc);
-            o_ddrift(r, L2);
-            if (bend) o_bndkick_rad(r, A, B, n, K1, h, radc); else o_strkick_rad(r, A, B, n, K1, radc);
-            o_ddrift(r, L1);
+            o_ddrift(r, L1, bd);
+            if (bend) o_bndkick_rad(r, A, B, n, K1, h, radc, diffc, bd);
+            else o_strkick_rad(r, A, B, n, K1, radc, diffc, bd);
+            o_ddrift(r, L2, bd);
+            if (bend) o_bndkick_rad(r, A, B, n, K2, h, radc, diffc, bd);
+            else o_strkick_rad(r, A, B, n, K2, radc, diffc, bd);
+            o_ddrift(r, L2, bd);
+            if (bend) o_bndkick_rad(r, A, B, n, K1, h, radc, diffc, bd);
+            else o_strkick_rad(r, A, B, n, K1, radc, diffc, bd);
+            o_ddrift(r, L1, bd);
         } else {
             o_fastdrift(r, nl1);
             if (bend) o_bndkick(r, A, B, K1, h, n); else o_strkick(r, A, B, K1, n);
@@ -377,7 +498,7 @@ static void o_multipole(real *r, const OElem *e, const real *A, const real *B, i
         else o_quad_fringe(r, B[1], -1);
     }
     if (bend) {
-        if (rad) o_edge_rad(r, h, e->ExitAngle, e->FringeInt2, e->FullGap, e->FringeBendExit, -1.0);
+        if (rad) o_edge_rad(r, h, e->ExitAngle, e->FringeInt2, e->FullGap, e->FringeBendExit, -1.0, bd);
         else o_edge(r, h, e->ExitAngle, e->FringeInt2, e->FullGap, e->FringeBendExit, -1);
     }
     if (e->RApertures) o_rect_ap(r, e->RApertures);
@@ -479,7 +600,7 @@ static void o_identity(real *r, const OElem *e) {
  * number round(F*T0) and the normalised voltage. */
 typedef struct {
     real A[64], B[64];
-    real nv, hn, radc;
+    real nv, hn, radc, diffc;
 } OPrep;
 
 static void o_prepare(const OElem *e, OPrep *p, double energy, double rest, double T0) {
@@ -500,8 +621,10 @@ static void o_prepare(const OElem *e, OPrep *p, double energy, double rest, doub
             }
         }
     }
-    if (e->pass == O_STRMPOLE_RAD || e->pass == O_BNDMPOLE_RAD)
+    if (e->pass == O_STRMPOLE_RAD || e->pass == O_BNDMPOLE_RAD) {
         p->radc = O_RAD_CONST * R_POW(o_gamma(energy, rest), 3);
+        p->diffc = O_DIF_CONST * R_POW(o_gamma(energy, rest), 5);
+    }
     if (e->pass == O_RFCAVITY) {
         p->hn = R_ROUND(e->Frequency * T0);
         p->nv = e->Voltage / energy;
@@ -513,10 +636,10 @@ static void o_element(real *r, const OElem *e, const OPrep *p, int nturn, double
     switch (e->pass) {
         case O_IDENTITY: o_identity(r, e); break;
         case O_DRIFT: o_driftpass(r, e); break;
-        case O_STRMPOLE: o_multipole(r, e, p->A, p->B, 0, 0, 0.0); break;
-        case O_STRMPOLE_RAD: o_multipole(r, e, p->A, p->B, 0, 1, p->radc); break;
-        case O_BNDMPOLE: o_multipole(r, e, p->A, p->B, 1, 0, 0.0); break;
-        case O_BNDMPOLE_RAD: o_multipole(r, e, p->A, p->B, 1, 1, p->radc); break;
+        case O_STRMPOLE: o_multipole(r, e, p->A, p->B, 0, 0, 0.0, 0.0, NULL); break;
+        case O_STRMPOLE_RAD: o_multipole(r, e, p->A, p->B, 0, 1, p->radc, 0.0, NULL); break;
+        case O_BNDMPOLE: o_multipole(r, e, p->A, p->B, 1, 0, 0.0, 0.0, NULL); break;
+        case O_BNDMPOLE_RAD: o_multipole(r, e, p->A, p->B, 1, 1, p->radc, 0.0, NULL); break;
         case O_THINMPOLE: o_thin(r, e, p->A, p->B); break;
         case O_RFCAVITY: o_rf(r, e, p->nv, p->hn, nturn, T0); break;
         case O_CORRECTOR: o_corr(r, e); break;
@@ -605,5 +728,25 @@ int oracle_track(const OElem *el, int nelem, double *r, int64_t np, int nturns, 
         o_put6(r + 6 * p, buf);
     }
     free(pp);
+    return 0;
+}
+
+/* pyat/at.c:755-831 diffusion_matrix: the Ohmi diffusion matrix of one
+ * element for one particle at ``orbit`` (T0 = 0, turn 0), accumulated from
+ * zero by the bdiff branch of the radiating multipole passes; other pass
+ * methods leave it zero.  ``out`` is 6x6 column-major ([i][j] at i + 6 j). */
+int oracle_diffmatrix(const OElem *e, const double *orbit, double energy, double rest,
+                      double *out) {
+    OPrep pp;
+    memset(&pp, 0, sizeof(pp));
+    o_prepare(e, &pp, energy, rest, 0.0);
+    real r[6], bd[36];
+    for (int k = 0; k < 6; k++) r[k] = orbit[k];
+    for (int k = 0; k < 36; k++) bd[k] = 0.0;
+    if (e->pass == O_STRMPOLE_RAD)
+        o_multipole(r, e, pp.A, pp.B, 0, 1, pp.radc, pp.diffc, bd);
+    else if (e->pass == O_BNDMPOLE_RAD)
+        o_multipole(r, e, pp.A, pp.B, 1, 1, pp.radc, pp.diffc, bd);
+    for (int k = 0; k < 36; k++) out[k] = (double)bd[k];
     return 0;
 }

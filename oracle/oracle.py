@@ -87,6 +87,9 @@ def _load():
                       C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                       C.c_void_p, C.c_int]
         f.restype = C.c_int
+        g = L.oracle_diffmatrix
+        g.argtypes = [C.POINTER(OElem), C.c_void_p, C.c_double, C.c_double, C.c_void_p]
+        g.restype = C.c_int
         _lib = L
     return _lib
 
@@ -194,6 +197,18 @@ def track(line, r, nturns, refpts=None, turn=0, energy=0.0, rest_energy=0.0, los
     if losses:
         ld = {"islost": lost.astype(bool), "turn": lturn, "elem": lelem, "coord": lcoord}
     return rout, ld
+
+
+def diffmatrix(element, orbit, energy=0.0, rest_energy=0.0):
+    """The Ohmi diffusion matrix of one element for a particle at ``orbit``
+    (the reference's ``diffusion_matrix``), as a (6, 6) array."""
+    lib = _load()
+    keep: list = []
+    els = _elements([element], keep)
+    orb = np.ascontiguousarray(np.asarray(orbit, dtype=np.float64).ravel())
+    out = np.zeros(36, dtype=np.float64)
+    lib.oracle_diffmatrix(els, orb.ctypes.data, energy, rest_energy, out.ctypes.data)
+    return out.reshape(6, 6, order="F")
 
 
 def track_quad(line, r, nturns, turn=0, energy=0.0, rest_energy=0.0, nthreads=None):

@@ -24,6 +24,7 @@
 #define R_POW powq
 #define R_ROUND roundq
 #define R_FABS fabsq
+#define R_SQRT sqrtq
 
 #include "oracle.c"
 

@@ -119,6 +119,61 @@ def fodo_fixture():
     np.savez_compressed(os.path.join(HERE, "fodo_rad_20turns.npz"), rin=r0, rout_final=r)
 
 
+def ref_lattice(ring):
+    """A reference Lattice of one of our rings (cavities as at.RFCavity, which
+    the reference finds by class)."""
+    line = []
+    for e in ring:
+        d = vars_of(e)
+        if d["PassMethod"] == "RFCavityPass":
+            line.append(at.RFCavity(d["FamName"], d["Length"], d["Voltage"], d["Frequency"],
+                                    d["HarmNumber"], d["Energy"], TimeLag=d["TimeLag"]))
+        else:
+            line.append(ref_element(d))
+    return at.Lattice(line, energy=ring.energy, particle=at.Particle("electron"), periodicity=1)
+
+
+def ohmi_fixture():
+    """The reference's Ohmi-envelope path on the radiating large ring:
+    per-element diffusion matrices (pyat/at.c:755-831 ``diffusion_matrix``)
+    at the closed orbit for the first cell's magnets and for bends with fringe
+    integrals, the cumulative diffusion matrix (``_dmatr``), and
+    ``ohmi_envelope`` (pyat/at/physics/radiation.py:151-276)."""
+    sys.path.insert(0, REPO)
+    from at_b200 import rings
+    from at.physics import radiation as rad
+    from at.tracking import diffusion_matrix
+    lat = ref_lattice(rings.large_ring(seed=1))
+    orbit, _ = at.find_orbit6(lat)
+    bbcum, orbs = rad._dmatr(lat, orbit=orbit)
+    emit0, beamdata, emit = at.ohmi_envelope(lat, refpts=[0, 100, 1000], orbit=orbit)
+    idx = np.array([i for i, e in enumerate(lat[:70]) if e.PassMethod.endswith("RadPass")])
+    bel = np.stack([diffusion_matrix(lat[i], np.asfortranarray(orbs[i].copy()), energy=lat.energy)
+                    for i in idx])
+    # bends with fringe integrals and the four edge methods
+    specs, borb, bfr = [], [], []
+    rng = np.random.default_rng(17)
+    for method in (0, 1, 2, 3):
+        d = {"FamName": "BF", "PassMethod": "BndMPoleSymplectic4RadPass", "Length": 0.8,
+             "BendingAngle": 0.05, "EntranceAngle": 0.02, "ExitAngle": 0.03,
+             "PolynomA": [0.0, 0.0, 0.0], "PolynomB": [0.0, -0.3, 2.0], "MaxOrder": 2,
+             "NumIntSteps": 10, "FullGap": 0.04, "FringeInt1": 0.5, "FringeInt2": 0.4,
+             "FringeBendEntrance": method, "FringeBendExit": method}
+        o = rng.standard_normal(6) * np.array([1e-3, 1e-4, 1e-3, 1e-4, 1e-3, 1e-3])
+        specs.append(d)
+        borb.append(o)
+        bfr.append(diffusion_matrix(ref_element(d), np.asfortranarray(o.copy()), energy=3e9))
+    np.savez_compressed(os.path.join(HERE, "ohmi_large.npz"), orbit=orbit, idx=idx,
+                        orbits=orbs[idx], belem=bel, bcum=bbcum[-1], orbs_all=orbs,
+                        r66=emit0.r66, emitXY=emit0.emitXY, emitXYZ=emit0.emitXYZ,
+                        m66=emit0.m66, tunes=beamdata.tunes, damping_rates=beamdata.damping_rates,
+                        mode_emittances=beamdata.mode_emittances, bend_orbits=np.array(borb),
+                        bend_b=np.array(bfr), refpts=np.array([0, 100, 1000]),
+                        emit_r66=emit.r66, emit_emitXYZ=emit.emitXYZ)
+    with open(os.path.join(HERE, "ohmi_bends.json"), "w") as f:
+        json.dump(specs, f)
+
+
 def m66_fixture():
     """The reference's closed orbit (find_orbit6) and one-turn matrix
     (find_m66, pyat/at/physics/matrix.py:105-165: central differences with
@@ -206,4 +261,5 @@ if __name__ == "__main__":
     sink_fixture()
     hmba_fixture()
     m66_fixture()
+    ohmi_fixture()
     print("golden fixtures written to", HERE)
