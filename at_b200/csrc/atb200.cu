@@ -109,6 +109,7 @@ struct Lattice {
 
 struct atb_handle {
     int device = 0;
+    uint64_t rng_key = 0;              /* quantum-diffusion kicks (atb_set_rng) */
     cudaStream_t stream = nullptr;
     int sm_count = 0;
     int smem_optin = 0;
@@ -209,6 +210,12 @@ int64_t count_records(const uint32_t* refpts, int nref, int start, int end, int 
     }
     if ((uint32_t)nelem == nextref) ++cnt;
     return cnt;
+}
+
+/* the random-kick key of job j: distinct per job, so batched particle sets
+   that share a lattice draw independent kicks */
+uint64_t job_key(const atb_handle* h, int j) {
+    return h->rng_key ^ (0x9e3779b97f4a7c15ULL * (uint64_t)(j + 1));
 }
 
 void fill_job_lattice(AtbJob& J, const Lattice& L, int start_elem, int end_elem) {
@@ -605,6 +612,7 @@ int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns
         AtbJob J;
         std::memset(&J, 0, sizeof(J));
         fill_job_lattice(J, *L, t0 == 0 ? start_elem : 0, end_elem);
+        J.rng_key = job_key(h, 0);
         J.check_loss = (flags & ATB_FLAG_ELEMENT) ? 0 : 1;
         J.r = h->r.as<double>();
         J.np = np;
@@ -672,6 +680,7 @@ int atb_track_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t n
     AtbJob J;
     std::memset(&J, 0, sizeof(J));
     fill_job_lattice(J, *L, 0, L->nelem);
+    J.rng_key = job_key(h, 0);
     J.check_loss = 1;
     J.r = r;
     J.np = np;
@@ -807,6 +816,7 @@ int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int3
         lats.push_back(L);
         std::memset(&J[j], 0, sizeof(AtbJob));
         fill_job_lattice(J[j], *L, 0, L->nelem);
+        J[j].rng_key = job_key(h, j);
         J[j].check_loss = 1;
         J[j].r = d.r;
         J[j].np = d.np;
@@ -853,6 +863,7 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
         lats.push_back(L);
         std::memset(&J[j], 0, sizeof(AtbJob));
         fill_job_lattice(J[j], *L, 0, L->nelem);
+        J[j].rng_key = job_key(h, j);
         J[j].check_loss = 1;
         J[j].r = d.r;
         J[j].np = d.np;
@@ -1008,6 +1019,12 @@ int atb_fp64_peak(int device, double* tflops, double* seconds) {
     const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
     *tflops = flops / (ms * 1e-3) / 1e12;
     if (seconds) *seconds = ms * 1e-3;
+    return ATB_OK;
+}
+
+int atb_set_rng(atb_handle* h, uint64_t key) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    h->rng_key = key;
     return ATB_OK;
 }
 

@@ -53,6 +53,7 @@ typedef struct AtbJob {
     double* lcoord;
     uint32_t* alive;            /* optional: survivors after each turn     */
     double* moments;            /* optional: 12 sums per turn              */
+    uint64_t rng_key;           /* key of the quantum-diffusion kicks      */
 } AtbJob;
 
 typedef struct AtbTile {

@@ -501,6 +501,54 @@ __device__ __forceinline__ void edge_fringe_rad(P6T<T>& r, double irho, double e
     r.py -= r.y * fy;
 }
 
+/* ---- quantum diffusion ------------------------------------------------
+ * The random kicks are counter-based: the normals of particle p at element
+ * ei in turn nturn are a pure function of (key, p, nturn, ei), so every
+ * thread draws its own without shared state and results do not depend on
+ * the launch shape.  The 64-bit mixer is the splitmix64 finaliser
+ * (Steele, Lea and Flood 2014; constants as published by Vigna); normals
+ * come in pairs from the Box-Muller transform of two uniforms in (0, 1]. */
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ void quantdiff_normals(uint64_t key, long long p, int nturn, int ei,
+                                                  double z[6]) {
+    const uint64_t golden = 0x9e3779b97f4a7c15ULL;
+    uint64_t s = mix64(key + golden * (uint64_t)(p + 1));
+    s = mix64(s ^ ((uint64_t)(uint32_t)nturn << 32 | (uint32_t)ei));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        s += golden;
+        const uint64_t a = mix64(s);
+        s += golden;
+        const uint64_t b = mix64(s);
+        const double u1 = (double)((a >> 11) + 1) * 0x1.0p-53;   /* (0, 1] */
+        const double u2 = (double)(b >> 11) * 0x1.0p-53;         /* [0, 1) */
+        const double rad = sqrt(-2.0 * log(u1));
+        double sn, cs;
+        sincospi(2.0 * u2, &sn, &cs);
+        z[2 * k] = rad * cs;
+        z[2 * k + 1] = rad * sn;
+    }
+}
+
+/* QuantDiffPass.c:9-45: r += L z, L lower triangular (column-major), z six
+ * standard normals */
+__device__ __forceinline__ void quantdiff_kick(P6& r, const double* L, const double z[6]) {
+    double d[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j <= i; ++j) s += z[j] * L[i + 6 * j];
+        d[i] = s;
+    }
+    r.x += d[0]; r.px += d[1]; r.y += d[2]; r.py += d[3]; r.dp += d[4]; r.ct += d[5];
+}
+
 }  // namespace atb
 
 #endif  // ATB_PHYSICS_CUH

@@ -35,7 +35,8 @@
 #define ATB_OP_RFCAVITY      7   /* RFCavityPass.c / attrackfunc.c        */
 #define ATB_OP_CORRECTOR     8   /* CorrectorPass.c                       */
 #define ATB_OP_APERTURE      9   /* AperturePass.c                        */
-#define ATB_NUM_OPS         10
+#define ATB_OP_QUANTDIFF    10   /* QuantDiffPass.c                       */
+#define ATB_NUM_OPS         11
 
 /* ---- header word 0 packing --------------------------------------------- */
 #define ATB_H_OP_SHIFT     0
@@ -152,6 +153,9 @@
 
 /* APERTURE */
 #define ATB_AP_LIM     2   /* 4 limits                                       */
+
+/* QuantDiffPass: the 6x6 Lmatp, column-major ([i][j] at i + 6 j) */
+#define ATB_QD_L       2
 
 #define ATB_MAX_RECORD_WORDS 511
 #define ATB_MAX_ORDER 40

@@ -379,9 +379,26 @@ __device__ __forceinline__ void pass_corrector(P6T<T>& r, const Rec& e) {
 
 /* One element on one particle; lost particles (x is NaN) are skipped as every
  * reference pass method does (e.g. StrMPoleSymplectic4Pass.c:59). */
+/* QuantDiffPass.c: random kicks keyed by (key, p, nturn, ei); without a
+ * key (the derivative kernels) the element is the identity, as the
+ * reference's envelope code disables it */
+template <class T>
+__device__ __forceinline__ void pass_quantdiff(P6T<T>& r, const Rec& e, const uint64_t* rng_key,
+                                               long long p, int nturn, int ei) {
+    if constexpr (!is_dual<T>::value) {
+        if (rng_key) {
+            double z[6];
+            quantdiff_normals(*rng_key, p, nturn, ei, z);
+            quantdiff_kick(r, e.p + ATB_QD_L, z);
+        }
+    }
+}
+
 template <class T>
 __device__ __forceinline__ void track_element(P6T<T>& r, const Rec& e, int nturn,
-                                              const Param& pm = Param{-1, 0.0}) {
+                                              const Param& pm = Param{-1, 0.0},
+                                              const uint64_t* rng_key = nullptr, long long p = 0,
+                                              int ei = 0) {
     if (isnan(val(r.x))) return;
     switch (e.op()) {
         case ATB_OP_IDENTITY: pass_identity(r, e); break;
@@ -394,6 +411,7 @@ __device__ __forceinline__ void track_element(P6T<T>& r, const Rec& e, int nturn
         case ATB_OP_RFCAVITY: pass_rfcavity(r, e, nturn); break;
         case ATB_OP_CORRECTOR: pass_corrector(r, e); break;
         case ATB_OP_APERTURE: check_rect(r, e.p + ATB_AP_LIM); break;
+        case ATB_OP_QUANTDIFF: pass_quantdiff(r, e, rng_key, p, nturn, ei); break;
         default: break;
     }
 }
@@ -544,7 +562,7 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
                         ++slot;
                         nextref = (nri < J.nref) ? J.refpts[nri++] : 0xffffffffu;
                     }
-                    track_element(r, e, nturn);
+                    track_element(r, e, nturn, Param{-1, 0.0}, &J.rng_key, p, ei);
                     if (J.check_loss) {
                         if (J.losses) {
                             if (!lost && is_bad(r)) {

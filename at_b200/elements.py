@@ -44,7 +44,7 @@ class Element:
             setattr(self, k, v)
 
     def __setattr__(self, key, value):
-        if key in ("R1", "R2"):
+        if key in ("R1", "R2", "Lmatp"):
             value = _farray(value, (6, 6))
         elif key in _ARRAYS:
             value = _farray(value)
@@ -156,6 +156,16 @@ class RFCavity(Element):
         super().__init__(family_name, length, Voltage=float(voltage),
                          Frequency=float(frequency), HarmNumber=int(harmonic_number),
                          Energy=float(energy), **kwargs)
+
+
+class QuantumDiffusion(Element):
+    """Lumped quantum excitation: random kicks r += L z, L the lower
+    triangular ``Lmatp`` (6x6), z six standard normals (QuantDiffPass)."""
+
+    def __init__(self, family_name: str, lmatp, **kwargs):
+        kwargs.setdefault("PassMethod", "QuantDiffPass")
+        lm = np.asfortranarray(np.asarray(lmatp, dtype=np.float64).reshape(6, 6))
+        super().__init__(family_name, 0.0, Lmatp=lm, **kwargs)
 
 
 class Corrector(Element):

@@ -197,5 +197,10 @@ class Engine:
     def batch_free(self, bid: int):
         check(lib().atb_batch_free(self.h, int(bid)))
 
+    def set_rng(self, key: int):
+        """Key of the quantum-diffusion random kicks of the launches that
+        follow."""
+        check(lib().atb_set_rng(self.h, int(key) & 0xFFFFFFFFFFFFFFFF))
+
     def sync(self, stream: int | None = None):
         check(lib().atb_sync(self.h, stream))

@@ -87,6 +87,8 @@ def element_flops(info, words, off) -> tuple[int, int]:
         f = mis + scal + (30 + 2 * ell if fl & T.ATB_F_THICK else 2 + ell)
     elif op == T.ATB_OP_APERTURE:
         f = 0
+    elif op == T.ATB_OP_QUANTDIFF:
+        f, trans = 21 * 2 + 6 + 3 * 6, 9          # L z, six adds, Box-Muller; log/sqrt/sincos
     else:
         f = 0
     return f, trans

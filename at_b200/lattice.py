@@ -559,6 +559,12 @@ def _compile_element(el, idx: int, energy: float, rest_energy: float, t0: float,
         lim = _need(_get_array(el, "Limits"), 4, "Limits")
         for i in range(4):
             rec.set(T.ATB_AP_LIM + i, lim[i])
+    elif op == T.ATB_OP_QUANTDIFF:
+        # QuantDiffPass.c:47-57: Lmatp, 6x6 (column-major as pyat stores it)
+        rec = _Record(op, T.ATB_QD_L + 36)
+        lm = _need(_get_array(el, "Lmatp"), 36, "Lmatp")
+        for i in range(36):
+            rec.set(T.ATB_QD_L + i, lm[i])
     else:  # pragma: no cover
         raise RuntimeError("unhandled opcode %d" % op)
     if op in (T.ATB_OP_STRMPOLE_RAD, T.ATB_OP_BNDMPOLE_RAD):

@@ -210,6 +210,44 @@ def cumulative_diffusion(ring, orbit, device: int = 0):
     return orbs, bcum, mcum
 
 
+def quantdiffmat(ring, orbit=None, device: int = 0) -> np.ndarray:
+    """Diffusion matrix of the whole ring, the symmetrised B_cum at its end
+    (radiation.py:469-482)."""
+    from . import physics
+
+    if orbit is None:
+        orbit = physics.find_orbit6(ring, mode="exact")
+    _, bcum, _ = cumulative_diffusion(ring, orbit, device)
+    return 0.5 * (bcum[-1] + bcum[-1].T)
+
+
+def lmat(dmat: np.ndarray) -> np.ndarray:
+    """Lower-triangular L with L L^T = dmat (radiation.py:125-146): the
+    eigenvalues are lifted to eps * max|eigenvalue| before the Cholesky
+    factorisation; if it still fails, the non-zero 4x4 block (no vertical
+    diffusion) is factorised alone."""
+    out = np.zeros((6, 6))
+    try:
+        v, w = np.linalg.eigh(dmat)
+        tol = np.finfo(float).eps * np.abs(v).max()
+        v[v < tol] = tol
+        out = np.linalg.cholesky(w @ np.diag(v) @ w.T)
+    except np.linalg.LinAlgError:
+        nz = np.where(dmat != 0)
+        c = np.linalg.cholesky(np.reshape(dmat[nz], (4, 4)))
+        out[nz] = np.reshape(c, (16,))
+    return out
+
+
+def gen_quantdiff_elem(ring, orbit=None, device: int = 0):
+    """A QuantumDiffusion element reproducing the ring's quantum excitation
+    at one point (radiation.py:485-500)."""
+    from .elements import QuantumDiffusion
+
+    return QuantumDiffusion("Diffusion", np.asfortranarray(lmat(quantdiffmat(ring, orbit,
+                                                                            device))))
+
+
 def ohmi_envelope(ring, refpts=None, orbit=None, device: int = 0):
     """Equilibrium beam envelope of a radiating ring (the reference's
     ``ohmi_envelope``, same three returned record arrays: ``emit0`` at the

@@ -43,5 +43,6 @@ PASS_OPCODES = {
     "RFCavityPass": C["ATB_OP_RFCAVITY"],
     "CorrectorPass": C["ATB_OP_CORRECTOR"],
     "AperturePass": C["ATB_OP_APERTURE"],
+    "QuantDiffPass": C["ATB_OP_QUANTDIFF"],
 }
 OPCODE_NAMES = {v: k for k, v in PASS_OPCODES.items()}

@@ -84,6 +84,37 @@ def _as_int(v, name):
     raise TypeError("%s must be an integer, not %s" % (name, type(v).__name__))
 
 
+# -- quantum-diffusion random kicks ---------------------------------------------
+# The reference keeps one PCG32 stream per process, reset by reset_rng
+# (pyat/at.c:833-852); here each call gets a fresh 64-bit key derived from
+# (seed, rank, call number), and the kernels derive every kick from the key.
+_AT_RNG_STATE = 0x853c49e6748fea9b
+_rng = {"seed": _AT_RNG_STATE, "rank": 0, "calls": 0}
+_M64 = 0xFFFFFFFFFFFFFFFF
+
+
+def _mix64(z: int) -> int:
+    """The splitmix64 finaliser (Steele, Lea and Flood 2014)."""
+    z &= _M64
+    z = ((z ^ (z >> 30)) * 0xbf58476d1ce4e5b9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94d049bb133111eb) & _M64
+    return z ^ (z >> 31)
+
+
+def reset_rng(*, rank: int = 0, seed: int | None = None):
+    """Restart the random kicks of QuantDiffPass elements from ``seed``
+    (the reference's ``reset_rng(*, rank=0, seed=None)``): the calls that
+    follow draw the same kicks after every reset with the same arguments."""
+    _rng["seed"] = _AT_RNG_STATE if seed is None else int(seed) & _M64
+    _rng["rank"] = int(rank) & _M64
+    _rng["calls"] = 0
+
+
+def _next_rng_key(device: int) -> int:
+    k = _mix64(_mix64(_rng["seed"] ^ _mix64(_rng["rank"] + 1)) + _rng["calls"])
+    return _mix64(k + 0x9e3779b97f4a7c15 * (device + 1))
+
+
 def _energy_particle(line, energy, particle):
     """pyat/at.c:275-306 set_energy_particle."""
     e = 0.0
@@ -210,6 +241,8 @@ def gpupass(line, r_in, nturns, refpts=_defref, *, turn=0, energy=None, particle
                 _state.lids[d] = eng.upload(cl)
             elif (cl.energy, cl.rest_energy) != old_version:
                 eng.update(_state.lids[d], cl)
+            eng.set_rng(_next_rng_key(d))
+        _rng["calls"] += 1
         # -- track --------------------------------------------------------------
         if len(devs) == 1 or npart < 2 * len(devs):
             eng = _eng.Engine.get(devs[0])

@@ -206,6 +206,15 @@ int atb_track_noalloc(int32_t device, const double* table, int64_t nwords,
                       uint8_t* islost, uint32_t* lturn, uint32_t* lelem, double* lcoord,
                       int32_t mode, void* stream);
 
+/* Key of the random kicks of QuantDiffPass elements in the launches that
+ * follow on this handle.  The reference draws them from one sequential
+ * PCG32 stream (atintegrators/atrandom.c, reset by pyat/at.c:833-852
+ * reset_rng); here the kicks of particle p at element e in turn n are a
+ * function of (key, job, p, n, e), so they are reproducible for a given key
+ * whatever the launch shape, and statistically equivalent to the
+ * reference's.  atb_track_noalloc uses key 0. */
+int atb_set_rng(atb_handle* h, uint64_t key);
+
 /* Wait for all work enqueued by this handle and return the kernels' status
  * (ATB_ERR_TIMEOUT if a bounded wait gave up). */
 int atb_sync(atb_handle* h, void* stream);

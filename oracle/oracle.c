@@ -40,7 +40,7 @@ typedef ORACLE_REAL real;
 /* pass methods (must match oracle.py) */
 enum {
     O_IDENTITY = 0, O_DRIFT, O_STRMPOLE, O_STRMPOLE_RAD, O_BNDMPOLE, O_BNDMPOLE_RAD,
-    O_THINMPOLE, O_RFCAVITY, O_CORRECTOR, O_APERTURE
+    O_THINMPOLE, O_RFCAVITY, O_CORRECTOR, O_APERTURE, O_QUANTDIFF
 };
 
 typedef struct {
@@ -58,6 +58,7 @@ typedef struct {
     double bax, bay;
     const double *PolynomA, *PolynomB, *fringeIntM0, *fringeIntP0;
     const double *R1, *R2, *T1, *T2, *RApertures, *EApertures, *KickAngle, *Limits;
+    const double *Lmatp;
 } OElem;
 
 /* ---- constants: atintegrators/atconstants.h:16-31, pyat/at.c:52-53 ----- */
@@ -644,6 +645,7 @@ static void o_element(real *r, const OElem *e, const OPrep *p, int nturn, double
         case O_RFCAVITY: o_rf(r, e, p->nv, p->hn, nturn, T0); break;
         case O_CORRECTOR: o_corr(r, e); break;
         case O_APERTURE: o_rect_ap(r, e->Limits); break;
+        case O_QUANTDIFF: break;   /* needs the random stream: element-major engine */
         default: break;
     }
 }
@@ -699,6 +701,66 @@ static void o_particle(real *r, const OElem *el, const OPrep *pp, int nelem, int
     if (losses) lost[p] = (uint8_t)is_lost;
 }
 
+/* ---- the random stream of QuantDiffPass ---------------------------------
+ * atintegrators/atrandom.c: O'Neill's PCG32 (XSH-RR output of a 64-bit LCG
+ * with stream increment) and normals by Marsaglia's polar method, one spare
+ * value kept for the next call; the stream is the engine's thread_state,
+ * seeded like pyat/at.c:833-852 reset_rng. */
+typedef struct {
+    uint64_t state, inc;
+    double spare;
+    int has_spare;
+} ORng;
+
+static uint32_t o_pcg32(ORng *g) {
+    uint64_t old = g->state;
+    g->state = old * 6364136223846793005ULL + g->inc;
+    uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xs >> rot) | (xs << ((-rot) & 31));
+}
+
+void oracle_rng_seed(ORng *g, uint64_t initstate, uint64_t initseq) {
+    g->state = 0U;
+    g->inc = (initseq << 1u) | 1u;
+    o_pcg32(g);
+    g->state += initstate;
+    o_pcg32(g);
+    g->has_spare = 0;
+}
+
+static double o_randn(ORng *g) {
+    if (g->has_spare) {
+        g->has_spare = 0;
+        return 0.0 + 1.0 * g->spare;
+    }
+    g->has_spare = 1;
+    double u, v, s;
+    do {
+        u = 2.0 * ldexp(o_pcg32(g), -32) - 1.0;
+        v = 2.0 * ldexp(o_pcg32(g), -32) - 1.0;
+        s = u * u + v * v;
+    } while ((s >= 1.0) || (s == 0.0));
+    s = sqrt(-2.0 * log(s) / s);
+    g->spare = v * s;
+    return 0.0 + 1.0 * u * s;
+}
+
+/* QuantDiffPass.c:9-45: six normals per particle (drawn for lost ones too),
+ * r += L z with L lower triangular, column-major */
+static void o_quantdiff(real *r, const double *L, ORng *g) {
+    double z[6];
+    real d[6];
+    for (int i = 0; i < 6; i++) {
+        d[i] = 0.0;
+        z[i] = o_randn(g);
+    }
+    for (int i = 0; i < 6; i++)
+        for (int j = 0; j <= i; j++) d[i] += z[j] * L[i + 6 * j];
+    if (!isnan(r[0]))
+        for (int i = 0; i < 6; i++) r[i] += d[i];
+}
+
 static OPrep *o_prepare_all(const OElem *el, int nelem, double energy, double rest, double T0) {
     OPrep *pp = (OPrep *)calloc((size_t)(nelem > 0 ? nelem : 1), sizeof(OPrep));
     if (!pp) return NULL;
@@ -706,11 +768,60 @@ static OPrep *o_prepare_all(const OElem *el, int nelem, double energy, double re
     return pp;
 }
 
-/* Track np particles (6, np Fortran order) in place.  Mirrors at_atpass. */
+/* The engine in the reference's own order (element-major: every particle
+ * through element i before element i + 1), single-threaded, for lattices
+ * whose QuantDiffPass elements draw from the sequential random stream. */
+static void o_track_em(real *R, const OElem *el, const OPrep *pp, int nelem, int nturns,
+                       int turn0, int start, int end, const uint32_t *refs, int nref,
+                       int losses, int check, double T0, double *rout, int64_t np,
+                       uint8_t *lost, uint32_t *lturn, uint32_t *lelem, double *lcoord,
+                       ORng *g) {
+    int64_t slot = 0;
+    for (int t = 0; t < nturns; t++) {
+        int nturn = turn0 + t;
+        int s0 = (t == 0) ? start : 0;
+        int ri = 0;
+        uint32_t next = (ri < nref) ? refs[ri++] : 0x7fffffffu;
+        for (int i = s0; i < end; i++) {
+            if ((uint32_t)i == next) {
+                if (rout)
+                    for (int64_t p = 0; p < np; p++) o_put6(rout + 6 * (p + np * slot), R + 6 * p);
+                slot++;
+                next = (ri < nref) ? refs[ri++] : 0x7fffffffu;
+            }
+            for (int64_t p = 0; p < np; p++) {
+                real *r = R + 6 * p;
+                if (el[i].pass == O_QUANTDIFF) o_quantdiff(r, el[i].Lmatp, g);
+                else o_element(r, &el[i], &pp[i], nturn, T0);
+                if (!check) continue;
+                if (losses) {
+                    if (!lost[p] && o_bad(r)) {
+                        lost[p] = 1;
+                        lturn[p] = (uint32_t)nturn;
+                        lelem[p] = (uint32_t)i;
+                        o_put6(lcoord + 6 * p, r);
+                        r[0] = NAN; r[1] = 0; r[2] = 0; r[3] = 0; r[4] = 0; r[5] = 0;
+                    }
+                } else if (isfinite(r[0]) && o_bad(r)) {
+                    r[0] = NAN; r[1] = 0; r[2] = 0; r[3] = 0; r[4] = 0; r[5] = 0;
+                }
+            }
+        }
+        if ((uint32_t)nelem == next) {
+            if (rout)
+                for (int64_t p = 0; p < np; p++) o_put6(rout + 6 * (p + np * slot), R + 6 * p);
+            slot++;
+        }
+    }
+}
+
+/* Track np particles (6, np Fortran order) in place.  Mirrors at_atpass.
+ * ``rng`` is the random stream of QuantDiffPass elements (NULL: they are
+ * skipped). */
 int oracle_track(const OElem *el, int nelem, double *r, int64_t np, int nturns, int turn0,
                  int start, int end, const uint32_t *refs, int nref, int losses, int check,
                  double energy, double rest, double T0, double *rout, uint8_t *lost,
-                 uint32_t *lturn, uint32_t *lelem, double *lcoord, int nthreads) {
+                 uint32_t *lturn, uint32_t *lelem, double *lcoord, int nthreads, ORng *rng) {
     OPrep *pp = o_prepare_all(el, nelem, energy, rest, T0);
     if (!pp) return -1;
     if (losses) {
@@ -718,6 +829,19 @@ int oracle_track(const OElem *el, int nelem, double *r, int64_t np, int nturns, 
         memset(lturn, 0, (size_t)np * 4);
         memset(lelem, 0, (size_t)np * 4);
         memset(lcoord, 0, (size_t)np * 48);
+    }
+    int has_rng = 0;
+    for (int i = 0; i < nelem; i++) has_rng |= (el[i].pass == O_QUANTDIFF);
+    if (has_rng && rng) {
+        real *R = (real *)malloc((size_t)(np > 0 ? np : 1) * 6 * sizeof(real));
+        if (!R) { free(pp); return -1; }
+        for (int64_t k = 0; k < 6 * np; k++) R[k] = r[k];
+        o_track_em(R, el, pp, nelem, nturns, turn0, start, end, refs, nref, losses, check, T0,
+                   rout, np, lost, lturn, lelem, lcoord, rng);
+        for (int64_t p = 0; p < np; p++) o_put6(r + 6 * p, R + 6 * p);
+        free(R);
+        free(pp);
+        return 0;
     }
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads > 0 ? nthreads : 1)
     for (int64_t p = 0; p < np; p++) {

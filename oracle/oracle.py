@@ -28,11 +28,22 @@ PASSES = {
     "IdentityPass": 0, "DriftPass": 1, "StrMPoleSymplectic4Pass": 2,
     "StrMPoleSymplectic4RadPass": 3, "BndMPoleSymplectic4Pass": 4,
     "BndMPoleSymplectic4RadPass": 5, "ThinMPolePass": 6, "RFCavityPass": 7,
-    "CorrectorPass": 8, "AperturePass": 9,
+    "CorrectorPass": 8, "AperturePass": 9, "QuantDiffPass": 10,
 }
 C0 = 2.99792458e8
 
 _dp = C.POINTER(C.c_double)
+
+
+class ORng(C.Structure):
+    """The engine's random stream (atintegrators/atrandom.c pcg32 state)."""
+    _fields_ = [("state", C.c_uint64), ("inc", C.c_uint64), ("spare", C.c_double),
+                ("has_spare", C.c_int)]
+
+
+AT_RNG_STATE = 0x853c49e6748fea9b
+# pyat/at.c:74 THREAD_PCG32_INITIALIZER: the stream before any reset_rng
+_rng = ORng(AT_RNG_STATE, 1, 0.0, 0)
 
 
 class OElem(C.Structure):
@@ -47,7 +58,7 @@ class OElem(C.Structure):
         ("bax", C.c_double), ("bay", C.c_double),
         ("PolynomA", _dp), ("PolynomB", _dp), ("fringeIntM0", _dp), ("fringeIntP0", _dp),
         ("R1", _dp), ("R2", _dp), ("T1", _dp), ("T2", _dp), ("RApertures", _dp),
-        ("EApertures", _dp), ("KickAngle", _dp), ("Limits", _dp),
+        ("EApertures", _dp), ("KickAngle", _dp), ("Limits", _dp), ("Lmatp", _dp),
     ]
 
 
@@ -85,8 +96,10 @@ def _load():
         f.argtypes = [C.POINTER(OElem), C.c_int, C.c_void_p, C.c_int64, C.c_int, C.c_int,
                       C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
                       C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                      C.c_void_p, C.c_int]
+                      C.c_void_p, C.c_int, C.POINTER(ORng)]
         f.restype = C.c_int
+        L.oracle_rng_seed.argtypes = [C.POINTER(ORng), C.c_uint64, C.c_uint64]
+        L.oracle_rng_seed.restype = None
         g = L.oracle_diffmatrix
         g.argtypes = [C.POINTER(OElem), C.c_void_p, C.c_double, C.c_double, C.c_void_p]
         g.restype = C.c_int
@@ -150,7 +163,7 @@ def _elements(line, keep):
             o.bax = float(flat[0]) if sz >= 1 else 0.0
             o.bay = float(flat[1]) if sz >= 2 else 0.0
         for name in ("PolynomA", "PolynomB", "fringeIntM0", "fringeIntP0", "R1", "R2", "T1",
-                     "T2", "RApertures", "EApertures", "KickAngle", "Limits"):
+                     "T2", "RApertures", "EApertures", "KickAngle", "Limits", "Lmatp"):
             setattr(o, name, _arr(el, name, keep))
     return arr
 
@@ -191,12 +204,19 @@ def track(line, r, nturns, refpts=None, turn=0, energy=0.0, rest_energy=0.0, los
                           None if lost is None else lost.ctypes.data,
                           None if lturn is None else lturn.ctypes.data,
                           None if lelem is None else lelem.ctypes.data,
-                          None if lcoord is None else lcoord.ctypes.data, nthreads)
+                          None if lcoord is None else lcoord.ctypes.data, nthreads,
+                          C.byref(_rng))
     if rc != 0:
         raise MemoryError("oracle allocation failed")
     if losses:
         ld = {"islost": lost.astype(bool), "turn": lturn, "elem": lelem, "coord": lcoord}
     return rout, ld
+
+
+def reset_rng(*, rank=0, seed=None):
+    """pyat/at.c:833-852 reset_rng: reseed the engine's random stream."""
+    lib = _load()
+    lib.oracle_rng_seed(C.byref(_rng), AT_RNG_STATE if seed is None else int(seed), int(rank))
 
 
 def diffmatrix(element, orbit, energy=0.0, rest_energy=0.0):

@@ -29,7 +29,7 @@ from at.tracking.atpass import atpass, elempass  # noqa: E402
 import cases  # noqa: E402
 
 ARRAY_ATTRS = {"PolynomA", "PolynomB", "KickAngle", "T1", "T2", "R1", "R2", "RApertures",
-               "EApertures", "Limits", "fringeIntM0", "fringeIntP0", "BendingAngle"}
+               "EApertures", "Limits", "fringeIntM0", "fringeIntP0", "BendingAngle", "Lmatp"}
 
 
 def ref_element(d):
@@ -174,6 +174,43 @@ def ohmi_fixture():
         json.dump(specs, f)
 
 
+def quantdiff_fixture():
+    """QuantDiffPass with the reference's random stream: after
+    reset_rng(seed=...), two consecutive calls (the stream continues), with
+    a refpts snapshot, through a line mixing diffusion kicks and magnets; and
+    the reference's gen_quantdiff_elem matrix for the large ring."""
+    from at.tracking.atpass import reset_rng
+    rng = np.random.default_rng(31)
+    mats = []
+    for scale in (3e-5, 1e-4):
+        m = np.tril(rng.standard_normal((6, 6))) * scale
+        mats.append(np.asfortranarray(m))
+    specs = [
+        {"FamName": "D1", "PassMethod": "DriftPass", "Length": 0.5},
+        {"FamName": "QD1", "PassMethod": "QuantDiffPass", "Lmatp": mats[0]},
+        {"FamName": "Q", "PassMethod": "StrMPoleSymplectic4Pass", "Length": 0.4,
+         "PolynomA": [0.0, 0.0], "PolynomB": [0.0, 1.2], "MaxOrder": 1, "NumIntSteps": 10},
+        {"FamName": "QD2", "PassMethod": "QuantDiffPass", "Lmatp": mats[1]},
+        {"FamName": "D2", "PassMethod": "DriftPass", "Length": 0.3},
+    ]
+    line = [ref_element(d) for d in specs]
+    r0 = np.asfortranarray(rng.standard_normal((6, 40)) * 1e-4)
+    r0[0, 7] = np.nan                       # a lost particle still draws its normals
+    r0[1:, 7] = 0.0
+    reset_rng(seed=4242)
+    r1 = r0.copy(order="F")
+    atpass(line, r1, 3, energy=3e9, particle=at.Particle("electron"))
+    r2 = r1.copy(order="F")
+    refs = np.array([0, 2, 5], dtype=np.uint32)
+    rout = atpass(line, r2, 2, refpts=refs, energy=3e9, particle=at.Particle("electron"))
+    sys.path.insert(0, REPO)
+    from at_b200 import rings
+    lat = ref_lattice(rings.large_ring(seed=1))
+    lmatp = at.gen_quantdiff_elem(lat).Lmatp
+    np.savez_compressed(os.path.join(HERE, "quantdiff.npz"), l0=mats[0], l1=mats[1], rin=r0,
+                        r1=r1, r2=r2, rout=rout, refpts=refs, large_lmatp=lmatp)
+
+
 def m66_fixture():
     """The reference's closed orbit (find_orbit6) and one-turn matrix
     (find_m66, pyat/at/physics/matrix.py:105-165: central differences with
@@ -262,4 +299,5 @@ if __name__ == "__main__":
     hmba_fixture()
     m66_fixture()
     ohmi_fixture()
+    quantdiff_fixture()
     print("golden fixtures written to", HERE)
