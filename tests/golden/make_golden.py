@@ -211,6 +211,33 @@ def quantdiff_fixture():
                         r1=r1, r2=r2, rout=rout, refpts=refs, large_lmatp=lmatp)
 
 
+def acceptance_fixture():
+    """The reference's grid-mode acceptance scans (pyat/at/acceptance) on the
+    radiating large ring: radial and cartesian 2-D grids, two observation
+    points, and a 1-D momentum scan; arrays stored by case name."""
+    sys.path.insert(0, REPO)
+    from at_b200 import rings
+    from at.acceptance import GridMode
+    lat = ref_lattice(rings.large_ring(seed=1))
+    out = {}
+    cases = {
+        "radial": dict(planes=["x", "y"], npoints=[9, 7], amplitudes=[6e-3, 3e-3],
+                       grid_mode=GridMode.RADIAL),
+        "cartesian": dict(planes=["x", "y"], npoints=[11, 6], amplitudes=[6e-3, 3e-3],
+                          grid_mode=GridMode.CARTESIAN),
+        "momentum": dict(planes=["dp"], npoints=[21], amplitudes=[0.04],
+                         grid_mode=GridMode.CARTESIAN),
+    }
+    for name, kw in cases.items():
+        b, sv, g = at.get_acceptance(lat, nturns=32, use_mp=False, **kw)
+        out[name + "_b"], out[name + "_s"], out[name + "_g"] = b, sv, g
+    b, sv, g = at.get_acceptance(lat, ["x", "y"], [7, 5], [6e-3, 3e-3], nturns=16,
+                                 refpts=[0, 61], grid_mode=GridMode.RADIAL, use_mp=False)
+    for k in range(2):
+        out["multi%d_b" % k], out["multi%d_s" % k], out["multi%d_g" % k] = b[k], sv[k], g[k]
+    np.savez_compressed(os.path.join(HERE, "acceptance_large.npz"), **out)
+
+
 def m66_fixture():
     """The reference's closed orbit (find_orbit6) and one-turn matrix
     (find_m66, pyat/at/physics/matrix.py:105-165: central differences with
@@ -300,4 +327,5 @@ if __name__ == "__main__":
     m66_fixture()
     ohmi_fixture()
     quantdiff_fixture()
+    acceptance_fixture()
     print("golden fixtures written to", HERE)
