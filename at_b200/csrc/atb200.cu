@@ -271,7 +271,7 @@ int kernel_config(atb_handle* h, const std::vector<const Lattice*>& lats, int mo
 }
 
 int launch(atb_handle* h, const std::vector<AtbJob>& jobs, const std::vector<AtbTile>& tiles,
-           int smem_bytes, int grid_max, int mode, cudaStream_t st) {
+           int smem_bytes, int grid_max, int mode, cudaStream_t st, int threads) {
     if (tiles.empty()) return ATB_OK;
     if (h->jobs.ensure(jobs.size() * sizeof(AtbJob)) != cudaSuccess ||
         h->tiles.ensure(tiles.size() * sizeof(AtbTile)) != cudaSuccess)
@@ -284,15 +284,25 @@ int launch(atb_handle* h, const std::vector<AtbJob>& jobs, const std::vector<Atb
     int grid = std::min<int64_t>((int64_t)tiles.size(), grid_max);
     int cap = h->seg_cap_words;
     if (mode == ATB_MODE_EXACT)
-        atb_track_kernel_exact<<<grid, h->threads, smem_bytes, st>>>(
+        atb_track_kernel_exact<<<grid, threads, smem_bytes, st>>>(
             h->jobs.as<AtbJob>(), h->tiles.as<AtbTile>(), (int)tiles.size(), h->counter.as<int>(),
             h->status.as<int>(), cap);
     else
-        atb_track_kernel_fast<<<grid, h->threads, smem_bytes, st>>>(
+        atb_track_kernel_fast<<<grid, threads, smem_bytes, st>>>(
             h->jobs.as<AtbJob>(), h->tiles.as<AtbTile>(), (int)tiles.size(), h->counter.as<int>(),
             h->status.as<int>(), cap);
     ATB_CUDA(cudaGetLastError());
     return ATB_OK;
+}
+
+/* Threads per block for a single particle set: the handle's value, reduced
+   (to a multiple of 32) when the set is too small to give every SM a tile,
+   so that a few hundred particles run on many SMs rather than queue on a
+   few.  Results do not depend on it: particles are independent. */
+int threads_for(const atb_handle* h, int64_t np) {
+    const int64_t per_sm = (np + h->sm_count - 1) / std::max(h->sm_count, 1);
+    const int64_t want = std::max<int64_t>(32, ((per_sm + 31) / 32) * 32);
+    return (int)std::min<int64_t>(h->threads, want);
 }
 
 void make_tiles(std::vector<AtbTile>& tiles, int job, int64_t np, int threads) {
@@ -631,8 +641,9 @@ int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns
         J.moments = (alive || moments) ? h->moments.as<double>() + 12 * t0 : nullptr;
         std::vector<AtbJob> jobs{J};
         h->h_tiles.clear();
-        make_tiles(h->h_tiles, 0, np, h->threads);
-        rc = launch(h, jobs, h->h_tiles, smem, grid_max, mode, st);
+        const int thr = threads_for(h, np);
+        make_tiles(h->h_tiles, 0, np, thr);
+        rc = launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr);
         if (rc) return rc;
         if (nref) {
             int64_t slots = (t0 == 0 ? rec_first : rec_turn) + (int64_t)(nt - 1) * rec_turn;
@@ -695,10 +706,11 @@ int atb_track_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t n
     J.moments = moments;
     std::vector<AtbJob> jobs{J};
     h->h_tiles.clear();
-    make_tiles(h->h_tiles, 0, np, h->threads);
+    const int thr = threads_for(h, np);
+    make_tiles(h->h_tiles, 0, np, thr);
     /* pageable-source copies of the launch lists are staged before
        cudaMemcpyAsync returns, so the host vectors may be reused at once */
-    return launch(h, jobs, h->h_tiles, smem, grid_max, mode, st);
+    return launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr);
 }
 
 int atb_element_maps(atb_handle* h, int32_t id, const double* orbits, double* m66,
@@ -842,7 +854,7 @@ int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int3
     h->h_tiles.clear();
     for (int j : order)
         if (J[j].nturns > 0) make_tiles(h->h_tiles, j, J[j].np, h->threads);
-    return launch(h, J, h->h_tiles, smem, grid_max, mode, st);
+    return launch(h, J, h->h_tiles, smem, grid_max, mode, st, h->threads);
 }
 
 int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,

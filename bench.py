@@ -62,6 +62,7 @@ def _args():
                     help="only the tangent-kernel timing (one JSON object)")
     ap.add_argument("--diff-particles", type=int, default=65536)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-variant run")
+    ap.add_argument("--no-acceptance", action="store_true", help="skip the acceptance scan")
     ap.add_argument("--batch-turn-scale", type=float, default=0.01,
                     help="scale of the batched variants' turn counts (1.0: 500-5000 turns)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -380,6 +381,9 @@ def run_b200(a):
     bat = None
     if world == 1 and not a.no_batch:
         bat = run_batching(local, mode, a.batch_turn_scale)
+    acc = None
+    if world == 1 and not a.no_acceptance:
+        acc = run_acceptance(mode, cpu)
 
     traffic = None
     prof = os.path.join(REPO, "profiles", "traffic_%s.json" % a.workload)
@@ -399,7 +403,7 @@ def run_b200(a):
                          "peak_source": "measured live: atb_fp64_peak DFMA chains on this GPU",
                          "flops_per_particle_turn": fpt, "survivor_particle_turns": survivors},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps, "clocks": clk,
-            "serving": serve, "differentiation": dif, "batching": bat,
+            "serving": serve, "differentiation": dif, "batching": bat, "acceptance": acc,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -494,6 +498,31 @@ def run_batching(device, mode, turn_scale):
             "plain_drop_in_per_variant": {"wall_s": seq, "particle_turns_per_s": pt / seq},
             "setup_s_compile_upload_tune_capture": setup,
             "autotune": tuning, "results_identical_sampled": same}
+
+
+def run_acceptance(mode, cpu):
+    """A dynamic-aperture scan as users run it (the reference's
+    get_acceptance, radial grid of 41 x 21 points, 1024 turns, on the large
+    ring): wall time through ``at_b200.acceptance`` (orbit search, grid,
+    tracking with the loss map, boundary), against the time the reference's
+    engine needs for the same particle-turns at the CPU rate measured in
+    this run (tracking only)."""
+    from at_b200 import acceptance, rings
+
+    ring = rings.large_ring(seed=1)
+    kw = dict(planes=["x", "y"], npoints=[41, 21], amplitudes=[6e-3, 3e-3], nturns=1024,
+              grid_mode=acceptance.GridMode.RADIAL, mode=mode)
+    acceptance.get_acceptance(ring, **dict(kw, nturns=2))
+    t0 = time.perf_counter()
+    b, s, g = acceptance.get_acceptance(ring, **kw)
+    wall = time.perf_counter() - t0
+    pt = g.shape[1] * (kw["nturns"] + 1)
+    out = {"grid": "radial 41 x 21 (x up to 6 mm, y up to 3 mm), 1024 turns, large ring",
+           "particles": int(g.shape[1]), "survivors": int(s.shape[1]), "wall_s": wall,
+           "particle_turns_per_s": pt / wall}
+    if cpu and cpu.get("value"):
+        out["reference_engine_tracking_s_at_measured_cpu_rate"] = pt / cpu["value"]
+    return out
 
 
 def run_diff(device, n=65536):
