@@ -33,9 +33,9 @@ __global__ void atb_dfma_probe(double* out, int iters, double a, double b) {
 }
 
 extern "C" __global__ void atb_track_kernel_exact(const AtbJob*, const AtbTile*, int, int*, int*,
-                                                  int);
+                                                  int, double*);
 extern "C" __global__ void atb_track_kernel_fast(const AtbJob*, const AtbTile*, int, int*, int*,
-                                                 int);
+                                                 int, double*);
 extern "C" __global__ void atb_tangent_kernel(const AtbTangent);
 extern "C" __global__ void atb_element_maps_kernel(const AtbElemMaps);
 
@@ -88,7 +88,7 @@ struct Batch {
     int smem = 0;
     int grid = 0;
     int ntiles = 0;
-    DevBuf jobs, tiles, counter;
+    DevBuf jobs, tiles, counter, scratch;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -119,7 +119,7 @@ struct atb_handle {
     int64_t rout_budget = 4LL << 30;
     std::vector<Lattice> lats;
     DevBuf r, rout, lost, lturn, lelem, lcoord, refpts, jobs, tiles, counter, status, alive,
-        moments, tan_pelem, tan_porder;
+        moments, tan_pelem, tan_porder, compact;
     std::vector<int32_t> h_pelem;
     std::vector<AtbTile> h_tiles;
     std::vector<struct Batch> batches;
@@ -283,14 +283,17 @@ int launch(atb_handle* h, const std::vector<AtbJob>& jobs, const std::vector<Atb
     ATB_CUDA(cudaMemsetAsync(h->counter.p, 0, sizeof(int), st));
     int grid = std::min<int64_t>((int64_t)tiles.size(), grid_max);
     int cap = h->seg_cap_words;
+    /* survivor-compaction scratch: 7 doubles per thread of the grid */
+    if (h->compact.ensure((size_t)grid * threads * 7 * sizeof(double)) != cudaSuccess)
+        return fail(ATB_ERR_NOMEM, "cudaMalloc(compaction scratch) failed");
     if (mode == ATB_MODE_EXACT)
         atb_track_kernel_exact<<<grid, threads, smem_bytes, st>>>(
             h->jobs.as<AtbJob>(), h->tiles.as<AtbTile>(), (int)tiles.size(), h->counter.as<int>(),
-            h->status.as<int>(), cap);
+            h->status.as<int>(), cap, h->compact.as<double>());
     else
         atb_track_kernel_fast<<<grid, threads, smem_bytes, st>>>(
             h->jobs.as<AtbJob>(), h->tiles.as<AtbTile>(), (int)tiles.size(), h->counter.as<int>(),
-            h->status.as<int>(), cap);
+            h->status.as<int>(), cap, h->compact.as<double>());
     ATB_CUDA(cudaGetLastError());
     return ATB_OK;
 }
@@ -418,10 +421,11 @@ int atb_destroy(atb_handle* h) {
             B.jobs.release();
             B.tiles.release();
             B.counter.release();
+            B.scratch.release();
         }
         for (DevBuf* b : {&h->r, &h->rout, &h->lost, &h->lturn, &h->lelem, &h->lcoord,
                           &h->refpts, &h->jobs, &h->tiles, &h->counter, &h->status, &h->alive,
-                          &h->moments})
+                          &h->moments, &h->tan_pelem, &h->tan_porder, &h->compact})
             b->release();
         if (h->stream) cudaStreamDestroy(h->stream);
     }
@@ -925,6 +929,10 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
     B.smem = smem;
     B.ntiles = (int)tiles.size();
     B.grid = std::min<int64_t>((int64_t)tiles.size(), std::max(grid_max, 1));
+    if (B.scratch.ensure((size_t)B.grid * B.threads * 7 * sizeof(double)) != cudaSuccess) {
+        B.used = false;
+        return fail(ATB_ERR_NOMEM, "cudaMalloc(compaction scratch) failed");
+    }
     *batch_id = id;
     return ATB_OK;
 }
@@ -940,11 +948,11 @@ static int batch_enqueue(atb_handle* h, Batch& B, cudaStream_t st) {
     if (B.mode == ATB_MODE_EXACT)
         atb_track_kernel_exact<<<B.grid, B.threads, B.smem, st>>>(
             B.jobs.as<AtbJob>(), B.tiles.as<AtbTile>(), B.ntiles, B.counter.as<int>(),
-            h->status.as<int>(), B.seg_cap);
+            h->status.as<int>(), B.seg_cap, B.scratch.as<double>());
     else
         atb_track_kernel_fast<<<B.grid, B.threads, B.smem, st>>>(
             B.jobs.as<AtbJob>(), B.tiles.as<AtbTile>(), B.ntiles, B.counter.as<int>(),
-            h->status.as<int>(), B.seg_cap);
+            h->status.as<int>(), B.seg_cap, B.scratch.as<double>());
     ATB_CUDA(cudaGetLastError());
     return ATB_OK;
 }
@@ -1002,6 +1010,7 @@ int atb_batch_free(atb_handle* h, int32_t batch_id) {
     B->jobs.release();
     B->tiles.release();
     B->counter.release();
+    B->scratch.release();
     B->used = false;
     return ATB_OK;
 }

@@ -450,10 +450,12 @@ extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
 ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
                                        const AtbTile* __restrict__ tiles, int ntiles,
                                        int* __restrict__ tile_counter,
-                                       int* __restrict__ status, int smem_cap_words) {
+                                       int* __restrict__ status, int smem_cap_words,
+                                       double* __restrict__ scratch) {
     extern __shared__ __align__(128) double smem[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_tile;
+    __shared__ int s_warp[ATB_MAX_THREADS / 32];
     double* buf0 = smem;
     double* buf1 = smem + smem_cap_words;
     uint32_t use_count[2] = {0u, 0u};
@@ -476,8 +478,9 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
         if (t >= ntiles) break;
         const AtbTile tile = tiles[t];
         const AtbJob& J = jobs[tile.job];
-        const long long p = tile.first + tid;
-        const bool active = (tid < tile.count);
+        long long p = tile.first + tid;
+        bool active = (tid < tile.count);
+        int nact = tile.count;            /* threads holding a particle (block-uniform) */
         const bool resident = (J.resident != 0);
 
         P6 r;
@@ -622,7 +625,52 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
                would still compute is observable without refpts snapshots) */
             if (J.nref == 0 && tt + 1 < J.nturns) {
                 const bool live = active && !isnan(r.x) && !(J.losses && lost);
-                if (!__syncthreads_or(live)) {
+                const int nlive = __syncthreads_count(live);
+                if (scratch && nlive > 0 && 2 * nlive <= nact && nact > 32) {
+                    /* Half or more of the particles held are lost: move the
+                       survivors to the lowest threads, so that whole warps
+                       fall idle instead of running with masked lanes.  The
+                       lost ones are retired first (their final state and
+                       loss flag are what the end of the tile would store). */
+                    if (active && !live) {
+                        store6(J.r + 6 * p, r);
+                        if (J.losses) J.lost[p] = lost ? 1 : 0;
+                    }
+                    const unsigned ball = __ballot_sync(0xffffffffu, live);
+                    const int lane = tid & 31, warp = tid >> 5;
+                    if (lane == 0) s_warp[warp] = __popc(ball);
+                    __syncthreads();
+                    int dest = __popc(ball & ((1u << lane) - 1u));
+                    for (int w = 0; w < warp; ++w) dest += s_warp[w];
+                    double* sb = scratch + (size_t)blockIdx.x * 7 * blockDim.x;
+                    if (live) {
+                        sb[dest] = r.x;
+                        sb[blockDim.x + dest] = r.px;
+                        sb[2 * blockDim.x + dest] = r.y;
+                        sb[3 * blockDim.x + dest] = r.py;
+                        sb[4 * blockDim.x + dest] = r.dp;
+                        sb[5 * blockDim.x + dest] = r.ct;
+                        sb[6 * blockDim.x + dest] = __longlong_as_double(p);
+                    }
+                    __syncthreads();
+                    active = tid < nlive;
+                    if (active) {
+                        r.x = sb[tid];
+                        r.px = sb[blockDim.x + tid];
+                        r.y = sb[2 * blockDim.x + tid];
+                        r.py = sb[3 * blockDim.x + tid];
+                        r.dp = sb[4 * blockDim.x + tid];
+                        r.ct = sb[5 * blockDim.x + tid];
+                        p = __double_as_longlong(sb[6 * blockDim.x + tid]);
+                        lost = false;
+                    } else {
+                        r.x = nan_d(); r.px = 0.0; r.y = 0.0; r.py = 0.0; r.dp = 0.0; r.ct = 0.0;
+                        lost = true;
+                    }
+                    nact = nlive;
+                    __syncthreads();   /* scratch free for the next compaction */
+                }
+                if (nlive == 0) {
                     if (!resident) {
                         /* wait for the copies this tile has in flight: after q
                            consumed segments, segments [0, min(nq, q + 2)) were
