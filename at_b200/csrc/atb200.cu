@@ -36,6 +36,19 @@ extern "C" __global__ void atb_track_kernel_exact(const AtbJob*, const AtbTile*,
                                                   int, double*);
 extern "C" __global__ void atb_track_kernel_fast(const AtbJob*, const AtbTile*, int, int*, int*,
                                                  int, double*);
+extern "C" __global__ void atb_track_kernel_exact_np2(const AtbJob*, const AtbTile*, int, int*,
+                                                      int*, int, double*);
+extern "C" __global__ void atb_track_kernel_fast_np2(const AtbJob*, const AtbTile*, int, int*,
+                                                     int*, int, double*);
+
+/* the tracking kernel for an arithmetic mode and a number of particles per
+   thread (1 or 2) */
+static const void* track_fn(int mode, int ppt) {
+    if (mode == ATB_MODE_EXACT)
+        return ppt == 2 ? (const void*)atb_track_kernel_exact_np2
+                        : (const void*)atb_track_kernel_exact;
+    return ppt == 2 ? (const void*)atb_track_kernel_fast_np2 : (const void*)atb_track_kernel_fast;
+}
 extern "C" __global__ void atb_tangent_kernel(const AtbTangent);
 extern "C" __global__ void atb_element_maps_kernel(const AtbElemMaps);
 
@@ -84,6 +97,7 @@ struct Batch {
     bool used = false;
     int mode = 1;
     int threads = 256;      /* launch shape fixed when the batch is prepared */
+    int ppt = 1;            /* particles per thread                             */
     int seg_cap = 6144;
     int smem = 0;
     int grid = 0;
@@ -114,6 +128,7 @@ struct atb_handle {
     int sm_count = 0;
     int smem_optin = 0;
     int threads = 256;
+    int ppt = 1;                       /* particles per thread (1 or 2)     */
     int seg_cap_words = 6144;          /* 48 KB per buffer, two buffers    */
     int resident_max_words = 14336;    /* tables up to 112 KB stay resident */
     int64_t rout_budget = 4LL << 30;
@@ -261,8 +276,7 @@ int kernel_config(atb_handle* h, const std::vector<const Lattice*>& lats, int mo
     if (bytes > h->smem_optin)
         return fail(ATB_ERR_ARG, "shared-memory plan exceeds the per-block limit");
     *smem_bytes = bytes;
-    const void* fn = mode == ATB_MODE_EXACT ? (const void*)atb_track_kernel_exact
-                                            : (const void*)atb_track_kernel_fast;
+    const void* fn = track_fn(mode, h->ppt);
     int per_sm = 0;
     ATB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->threads, bytes));
     if (per_sm < 1) return fail(ATB_ERR_ARG, "launch configuration does not fit on an SM");
@@ -271,7 +285,7 @@ int kernel_config(atb_handle* h, const std::vector<const Lattice*>& lats, int mo
 }
 
 int launch(atb_handle* h, const std::vector<AtbJob>& jobs, const std::vector<AtbTile>& tiles,
-           int smem_bytes, int grid_max, int mode, cudaStream_t st, int threads) {
+           int smem_bytes, int grid_max, int mode, cudaStream_t st, int threads, int ppt) {
     if (tiles.empty()) return ATB_OK;
     if (h->jobs.ensure(jobs.size() * sizeof(AtbJob)) != cudaSuccess ||
         h->tiles.ensure(tiles.size() * sizeof(AtbTile)) != cudaSuccess)
@@ -286,14 +300,20 @@ int launch(atb_handle* h, const std::vector<AtbJob>& jobs, const std::vector<Atb
     /* survivor-compaction scratch: 7 doubles per thread of the grid */
     if (h->compact.ensure((size_t)grid * threads * 7 * sizeof(double)) != cudaSuccess)
         return fail(ATB_ERR_NOMEM, "cudaMalloc(compaction scratch) failed");
-    if (mode == ATB_MODE_EXACT)
-        atb_track_kernel_exact<<<grid, threads, smem_bytes, st>>>(
-            h->jobs.as<AtbJob>(), h->tiles.as<AtbTile>(), (int)tiles.size(), h->counter.as<int>(),
-            h->status.as<int>(), cap, h->compact.as<double>());
+    const AtbJob* dj = h->jobs.as<AtbJob>();
+    const AtbTile* dt = h->tiles.as<AtbTile>();
+    const int nt = (int)tiles.size();
+    int* cnt = h->counter.as<int>();
+    int* sts = h->status.as<int>();
+    double* scr = h->compact.as<double>();
+    if (mode == ATB_MODE_EXACT && ppt == 2)
+        atb_track_kernel_exact_np2<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, sts, cap, scr);
+    else if (mode == ATB_MODE_EXACT)
+        atb_track_kernel_exact<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, sts, cap, scr);
+    else if (ppt == 2)
+        atb_track_kernel_fast_np2<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, sts, cap, scr);
     else
-        atb_track_kernel_fast<<<grid, threads, smem_bytes, st>>>(
-            h->jobs.as<AtbJob>(), h->tiles.as<AtbTile>(), (int)tiles.size(), h->counter.as<int>(),
-            h->status.as<int>(), cap, h->compact.as<double>());
+        atb_track_kernel_fast<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, sts, cap, scr);
     ATB_CUDA(cudaGetLastError());
     return ATB_OK;
 }
@@ -306,6 +326,12 @@ int threads_for(const atb_handle* h, int64_t np) {
     const int64_t per_sm = (np + h->sm_count - 1) / std::max(h->sm_count, 1);
     const int64_t want = std::max<int64_t>(32, ((per_sm + 31) / 32) * 32);
     return (int)std::min<int64_t>(h->threads, want);
+}
+
+/* particles per thread for a single set: the handle's choice when the set
+   fills every SM with full tiles, else one */
+int ppt_for(const atb_handle* h, int64_t np) {
+    return np >= (int64_t)h->sm_count * h->threads * h->ppt ? h->ppt : 1;
 }
 
 void make_tiles(std::vector<AtbTile>& tiles, int job, int64_t np, int threads) {
@@ -397,6 +423,10 @@ int atb_create(int device, atb_handle** out) {
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
     ATB_CUDA(cudaFuncSetAttribute(atb_track_kernel_fast,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
+    ATB_CUDA(cudaFuncSetAttribute(atb_track_kernel_exact_np2,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
+    ATB_CUDA(cudaFuncSetAttribute(atb_track_kernel_fast_np2,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
     ATB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     if (h->counter.ensure(sizeof(int)) != cudaSuccess || h->status.ensure(sizeof(int)) != cudaSuccess)
         return fail(ATB_ERR_CUDA, "cudaMalloc failed");
@@ -430,6 +460,15 @@ int atb_destroy(atb_handle* h) {
         if (h->stream) cudaStreamDestroy(h->stream);
     }
     delete h;
+    return ATB_OK;
+}
+
+int atb_set_particles_per_thread(atb_handle* h, int32_t ppt) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    if (ppt != 1 && ppt != 2) return fail(ATB_ERR_ARG, "particles per thread must be 1 or 2");
+    for (const Batch& B : h->batches)
+        if (B.used) return fail(ATB_ERR_ARG, "free the prepared batches before changing the launch shape");
+    h->ppt = ppt;
     return ATB_OK;
 }
 
@@ -645,9 +684,10 @@ int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns
         J.moments = (alive || moments) ? h->moments.as<double>() + 12 * t0 : nullptr;
         std::vector<AtbJob> jobs{J};
         h->h_tiles.clear();
-        const int thr = threads_for(h, np);
-        make_tiles(h->h_tiles, 0, np, thr);
-        rc = launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr);
+        const int pp = ppt_for(h, np);
+        const int thr = pp > 1 ? h->threads : threads_for(h, np);
+        make_tiles(h->h_tiles, 0, np, thr * pp);
+        rc = launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr, pp);
         if (rc) return rc;
         if (nref) {
             int64_t slots = (t0 == 0 ? rec_first : rec_turn) + (int64_t)(nt - 1) * rec_turn;
@@ -710,11 +750,12 @@ int atb_track_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t n
     J.moments = moments;
     std::vector<AtbJob> jobs{J};
     h->h_tiles.clear();
-    const int thr = threads_for(h, np);
-    make_tiles(h->h_tiles, 0, np, thr);
+    const int pp = ppt_for(h, np);
+    const int thr = pp > 1 ? h->threads : threads_for(h, np);
+    make_tiles(h->h_tiles, 0, np, thr * pp);
     /* pageable-source copies of the launch lists are staged before
        cudaMemcpyAsync returns, so the host vectors may be reused at once */
-    return launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr);
+    return launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr, pp);
 }
 
 int atb_element_maps(atb_handle* h, int32_t id, const double* orbits, double* m66,
@@ -857,8 +898,8 @@ int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int3
     });
     h->h_tiles.clear();
     for (int j : order)
-        if (J[j].nturns > 0) make_tiles(h->h_tiles, j, J[j].np, h->threads);
-    return launch(h, J, h->h_tiles, smem, grid_max, mode, st, h->threads);
+        if (J[j].nturns > 0) make_tiles(h->h_tiles, j, J[j].np, h->threads * h->ppt);
+    return launch(h, J, h->h_tiles, smem, grid_max, mode, st, h->threads, h->ppt);
 }
 
 int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,
@@ -904,7 +945,7 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
     });
     std::vector<AtbTile> tiles;
     for (int j : order)
-        if (J[j].nturns > 0) make_tiles(tiles, j, J[j].np, h->threads);
+        if (J[j].nturns > 0) make_tiles(tiles, j, J[j].np, h->threads * h->ppt);
     int id = -1;
     for (int i = 0; i < (int)h->batches.size(); ++i)
         if (!h->batches[i].used) { id = i; break; }
@@ -925,6 +966,7 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
     B.used = true;
     B.mode = mode;
     B.threads = h->threads;
+    B.ppt = h->ppt;
     B.seg_cap = h->seg_cap_words;
     B.smem = smem;
     B.ntiles = (int)tiles.size();
@@ -945,14 +987,23 @@ static Batch* get_batch(atb_handle* h, int id) {
 static int batch_enqueue(atb_handle* h, Batch& B, cudaStream_t st) {
     ATB_CUDA(cudaMemsetAsync(B.counter.p, 0, sizeof(int), st));
     if (B.ntiles == 0) return ATB_OK;
-    if (B.mode == ATB_MODE_EXACT)
-        atb_track_kernel_exact<<<B.grid, B.threads, B.smem, st>>>(
-            B.jobs.as<AtbJob>(), B.tiles.as<AtbTile>(), B.ntiles, B.counter.as<int>(),
-            h->status.as<int>(), B.seg_cap, B.scratch.as<double>());
+    const AtbJob* dj = B.jobs.as<AtbJob>();
+    const AtbTile* dt = B.tiles.as<AtbTile>();
+    int* cnt = B.counter.as<int>();
+    int* sts = h->status.as<int>();
+    double* scr = B.scratch.as<double>();
+    if (B.mode == ATB_MODE_EXACT && B.ppt == 2)
+        atb_track_kernel_exact_np2<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, sts,
+                                                                      B.seg_cap, scr);
+    else if (B.mode == ATB_MODE_EXACT)
+        atb_track_kernel_exact<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, sts,
+                                                                  B.seg_cap, scr);
+    else if (B.ppt == 2)
+        atb_track_kernel_fast_np2<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, sts,
+                                                                     B.seg_cap, scr);
     else
-        atb_track_kernel_fast<<<B.grid, B.threads, B.smem, st>>>(
-            B.jobs.as<AtbJob>(), B.tiles.as<AtbTile>(), B.ntiles, B.counter.as<int>(),
-            h->status.as<int>(), B.seg_cap, B.scratch.as<double>());
+        atb_track_kernel_fast<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, sts,
+                                                                 B.seg_cap, scr);
     ATB_CUDA(cudaGetLastError());
     return ATB_OK;
 }

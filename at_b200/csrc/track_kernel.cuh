@@ -446,12 +446,34 @@ __device__ __forceinline__ int seg_at(const AtbJob& J, long long q) {
 
 #ifndef ATB_NO_TRACK_KERNEL
 
-extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
-ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
-                                       const AtbTile* __restrict__ tiles, int ntiles,
-                                       int* __restrict__ tile_counter,
-                                       int* __restrict__ status, int smem_cap_words,
-                                       double* __restrict__ scratch) {
+/* lost-particle marking of one particle after an element (pyat/at.c:115-161) */
+__device__ __forceinline__ void apply_loss_rule(const AtbJob& J, P6& r, bool& lost, bool active,
+                                                long long p, int nturn, int ei) {
+    if (J.losses) {
+        if (!lost && is_bad(r)) {
+            lost = true;
+            if (active) {
+                J.lturn[p] = (unsigned)nturn;
+                J.lelem[p] = (unsigned)ei;
+                store6(J.lcoord + 6 * p, r);
+            }
+            r.x = nan_d(); r.px = 0.0; r.y = 0.0; r.py = 0.0; r.dp = 0.0; r.ct = 0.0;
+        }
+    } else if (isfinite(r.x) && is_bad(r)) {
+        r.x = nan_d(); r.px = 0.0; r.y = 0.0; r.py = 0.0; r.dp = 0.0; r.ct = 0.0;
+    }
+}
+
+/* The persistent tile loop.  NP particles per thread: particle k of thread t
+ * in a tile is tile.first + k * blockDim + t, so every k stays coalesced; the
+ * element parameters read from shared memory serve all NP particles, whose
+ * dependency chains interleave. */
+template <int NP>
+__device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
+                                            const AtbTile* __restrict__ tiles, int ntiles,
+                                            int* __restrict__ tile_counter,
+                                            int* __restrict__ status, int smem_cap_words,
+                                            double* __restrict__ scratch) {
     extern __shared__ __align__(128) double smem[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_tile;
@@ -460,6 +482,7 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
     double* buf1 = smem + smem_cap_words;
     uint32_t use_count[2] = {0u, 0u};
     const int tid = threadIdx.x;
+    const int nthr = blockDim.x;
 
     if (tid == 0) {
         mbar_init(&bars[0], 1);
@@ -478,19 +501,25 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
         if (t >= ntiles) break;
         const AtbTile tile = tiles[t];
         const AtbJob& J = jobs[tile.job];
-        long long p = tile.first + tid;
-        bool active = (tid < tile.count);
-        int nact = tile.count;            /* threads holding a particle (block-uniform) */
+        long long p[NP];
+        bool active[NP];
+        int nact = tile.count;            /* particles held by the block (uniform) */
         const bool resident = (J.resident != 0);
 
-        P6 r;
-        bool lost = false;
-        if (active) {
-            load6(J.r + 6 * p, r);
-            if (J.losses) lost = J.lost[p] != 0;
-        } else {
-            r.x = nan_d(); r.px = r.py = r.y = r.dp = r.ct = 0.0;
-            lost = true;
+        P6 r[NP];
+        bool lost[NP];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            p[k] = tile.first + (long long)k * nthr + tid;
+            active[k] = (k * nthr + tid) < tile.count;
+            lost[k] = false;
+            if (active[k]) {
+                load6(J.r + 6 * p[k], r[k]);
+                if (J.losses) lost[k] = J.lost[p[k]] != 0;
+            } else {
+                r[k].x = nan_d(); r[k].px = r[k].py = r[k].y = r[k].dp = r[k].ct = 0.0;
+                lost[k] = true;
+            }
         }
 
         /* staging pipeline state for this tile */
@@ -561,25 +590,16 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
                     e.hdr = hp[0];
                     e.opt = hp[1];
                     if ((unsigned)ei == nextref) {
-                        if (active) store6(J.rout + 6 * (p + J.np * slot), r);
+#pragma unroll
+                        for (int k = 0; k < NP; ++k)
+                            if (active[k]) store6(J.rout + 6 * (p[k] + J.np * slot), r[k]);
                         ++slot;
                         nextref = (nri < J.nref) ? J.refpts[nri++] : 0xffffffffu;
                     }
-                    track_element(r, e, nturn, Param{-1, 0.0}, &J.rng_key, p, ei);
-                    if (J.check_loss) {
-                        if (J.losses) {
-                            if (!lost && is_bad(r)) {
-                                lost = true;
-                                if (active) {
-                                    J.lturn[p] = (unsigned)nturn;
-                                    J.lelem[p] = (unsigned)ei;
-                                    store6(J.lcoord + 6 * p, r);
-                                }
-                                r.x = nan_d(); r.px = 0.0; r.y = 0.0; r.py = 0.0; r.dp = 0.0; r.ct = 0.0;
-                            }
-                        } else if (isfinite(r.x) && is_bad(r)) {
-                            r.x = nan_d(); r.px = 0.0; r.y = 0.0; r.py = 0.0; r.dp = 0.0; r.ct = 0.0;
-                        }
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) {
+                        track_element(r[k], e, nturn, Param{-1, 0.0}, &J.rng_key, p[k], ei);
+                        if (J.check_loss) apply_loss_rule(J, r[k], lost[k], active[k], p[k], nturn, ei);
                     }
                     w += e.len();
                 }
@@ -595,80 +615,99 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
             }
             if (timed_out) break;
             if ((unsigned)J.nelem == nextref) {
-                if (active) store6(J.rout + 6 * (p + J.np * slot), r);
+#pragma unroll
+                for (int k = 0; k < NP; ++k)
+                    if (active[k]) store6(J.rout + 6 * (p[k] + J.np * slot), r[k]);
                 ++slot;
             }
             if (J.alive) {
                 /* per-turn survivors and first/second moments: warp ballot
                  * and shuffle reductions, one atomic per warp */
-                const bool alive = active && !isnan(r.x) && !(J.losses && lost);
-                const unsigned m = __ballot_sync(0xffffffffu, alive);
+                unsigned cnt = 0;
                 double v[12];
-                v[0] = alive ? r.x : 0.0; v[1] = alive ? r.px : 0.0; v[2] = alive ? r.y : 0.0;
-                v[3] = alive ? r.py : 0.0; v[4] = alive ? r.dp : 0.0; v[5] = alive ? r.ct : 0.0;
 #pragma unroll
-                for (int k = 0; k < 6; ++k) v[6 + k] = v[k] * v[k];
+                for (int c = 0; c < 12; ++c) v[c] = 0.0;
 #pragma unroll
-                for (int k = 0; k < 12; ++k) {
+                for (int k = 0; k < NP; ++k) {
+                    const bool alive = active[k] && !isnan(r[k].x) && !(J.losses && lost[k]);
+                    cnt += __popc(__ballot_sync(0xffffffffu, alive));
+                    const double c6[6] = {r[k].x, r[k].px, r[k].y, r[k].py, r[k].dp, r[k].ct};
 #pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+                    for (int c = 0; c < 6; ++c) {
+                        const double x = alive ? c6[c] : 0.0;
+                        v[c] += x;
+                        v[6 + c] += x * x;
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < 12; ++c) {
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
                 }
                 if ((tid & 31) == 0) {
-                    atomicAdd(&J.alive[tt], (unsigned)__popc(m));
+                    atomicAdd(&J.alive[tt], cnt);
                     if (J.moments) {
 #pragma unroll
-                        for (int k = 0; k < 12; ++k) atomicAdd(&J.moments[12 * tt + k], v[k]);
+                        for (int c = 0; c < 12; ++c) atomicAdd(&J.moments[12 * tt + c], v[c]);
                     }
                 }
             }
             /* a tile whose particles are all lost stops early (nothing it
                would still compute is observable without refpts snapshots) */
             if (J.nref == 0 && tt + 1 < J.nturns) {
-                const bool live = active && !isnan(r.x) && !(J.losses && lost);
-                const int nlive = __syncthreads_count(live);
-                if (scratch && nlive > 0 && 2 * nlive <= nact && nact > 32) {
-                    /* Half or more of the particles held are lost: move the
-                       survivors to the lowest threads, so that whole warps
-                       fall idle instead of running with masked lanes.  The
-                       lost ones are retired first (their final state and
-                       loss flag are what the end of the tile would store). */
-                    if (active && !live) {
-                        store6(J.r + 6 * p, r);
-                        if (J.losses) J.lost[p] = lost ? 1 : 0;
+                bool any_live = false;
+#pragma unroll
+                for (int k = 0; k < NP; ++k)
+                    any_live |= active[k] && !isnan(r[k].x) && !(J.losses && lost[k]);
+                const int nlive = __syncthreads_count(any_live);
+                if constexpr (NP == 1) {
+                    const bool live = any_live;
+                    if (scratch && nlive > 0 && 2 * nlive <= nact && nact > 32) {
+                        /* Half or more of the particles held are lost: move
+                           the survivors to the lowest threads, so that whole
+                           warps fall idle instead of running with masked
+                           lanes.  The lost ones are retired first (their
+                           final state and loss flag are what the end of the
+                           tile would store). */
+                        if (active[0] && !live) {
+                            store6(J.r + 6 * p[0], r[0]);
+                            if (J.losses) J.lost[p[0]] = lost[0] ? 1 : 0;
+                        }
+                        const unsigned ball = __ballot_sync(0xffffffffu, live);
+                        const int lane = tid & 31, warp = tid >> 5;
+                        if (lane == 0) s_warp[warp] = __popc(ball);
+                        __syncthreads();
+                        int dest = __popc(ball & ((1u << lane) - 1u));
+                        for (int wv = 0; wv < warp; ++wv) dest += s_warp[wv];
+                        double* sb = scratch + (size_t)blockIdx.x * 7 * nthr;
+                        if (live) {
+                            sb[dest] = r[0].x;
+                            sb[nthr + dest] = r[0].px;
+                            sb[2 * nthr + dest] = r[0].y;
+                            sb[3 * nthr + dest] = r[0].py;
+                            sb[4 * nthr + dest] = r[0].dp;
+                            sb[5 * nthr + dest] = r[0].ct;
+                            sb[6 * nthr + dest] = __longlong_as_double(p[0]);
+                        }
+                        __syncthreads();
+                        active[0] = tid < nlive;
+                        if (active[0]) {
+                            r[0].x = sb[tid];
+                            r[0].px = sb[nthr + tid];
+                            r[0].y = sb[2 * nthr + tid];
+                            r[0].py = sb[3 * nthr + tid];
+                            r[0].dp = sb[4 * nthr + tid];
+                            r[0].ct = sb[5 * nthr + tid];
+                            p[0] = __double_as_longlong(sb[6 * nthr + tid]);
+                            lost[0] = false;
+                        } else {
+                            r[0].x = nan_d(); r[0].px = 0.0; r[0].y = 0.0;
+                            r[0].py = 0.0; r[0].dp = 0.0; r[0].ct = 0.0;
+                            lost[0] = true;
+                        }
+                        nact = nlive;
+                        __syncthreads();   /* scratch free for the next compaction */
                     }
-                    const unsigned ball = __ballot_sync(0xffffffffu, live);
-                    const int lane = tid & 31, warp = tid >> 5;
-                    if (lane == 0) s_warp[warp] = __popc(ball);
-                    __syncthreads();
-                    int dest = __popc(ball & ((1u << lane) - 1u));
-                    for (int w = 0; w < warp; ++w) dest += s_warp[w];
-                    double* sb = scratch + (size_t)blockIdx.x * 7 * blockDim.x;
-                    if (live) {
-                        sb[dest] = r.x;
-                        sb[blockDim.x + dest] = r.px;
-                        sb[2 * blockDim.x + dest] = r.y;
-                        sb[3 * blockDim.x + dest] = r.py;
-                        sb[4 * blockDim.x + dest] = r.dp;
-                        sb[5 * blockDim.x + dest] = r.ct;
-                        sb[6 * blockDim.x + dest] = __longlong_as_double(p);
-                    }
-                    __syncthreads();
-                    active = tid < nlive;
-                    if (active) {
-                        r.x = sb[tid];
-                        r.px = sb[blockDim.x + tid];
-                        r.y = sb[2 * blockDim.x + tid];
-                        r.py = sb[3 * blockDim.x + tid];
-                        r.dp = sb[4 * blockDim.x + tid];
-                        r.ct = sb[5 * blockDim.x + tid];
-                        p = __double_as_longlong(sb[6 * blockDim.x + tid]);
-                        lost = false;
-                    } else {
-                        r.x = nan_d(); r.px = 0.0; r.y = 0.0; r.py = 0.0; r.dp = 0.0; r.ct = 0.0;
-                        lost = true;
-                    }
-                    nact = nlive;
-                    __syncthreads();   /* scratch free for the next compaction */
                 }
                 if (nlive == 0) {
                     if (!resident) {
@@ -702,14 +741,37 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
             if (tid == 0) atomicOr(status, ATB_STATUS_WAIT_TIMEOUT);
             break;
         }
-        if (active) {
-            store6(J.r + 6 * p, r);
-            if (J.losses) J.lost[p] = lost ? 1 : 0;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            if (active[k]) {
+                store6(J.r + 6 * p[k], r[k]);
+                if (J.losses) J.lost[p[k]] = lost[k] ? 1 : 0;
+            }
         }
         /* all threads must be past the last segment before the buffers are
            re-filled by the next tile */
         __syncthreads();
     }
+}
+
+extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
+ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
+                                       const AtbTile* __restrict__ tiles, int ntiles,
+                                       int* __restrict__ tile_counter,
+                                       int* __restrict__ status, int smem_cap_words,
+                                       double* __restrict__ scratch) {
+    track_tiles<1>(jobs, tiles, ntiles, tile_counter, status, smem_cap_words, scratch);
+}
+
+/* two particles per thread (the autotuner's particles-per-thread choice) */
+extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
+ATB_CAT(ATB_CAT(atb_track_kernel, ATB_KSUFFIX), _np2)(const AtbJob* __restrict__ jobs,
+                                                      const AtbTile* __restrict__ tiles,
+                                                      int ntiles, int* __restrict__ tile_counter,
+                                                      int* __restrict__ status,
+                                                      int smem_cap_words,
+                                                      double* __restrict__ scratch) {
+    track_tiles<2>(jobs, tiles, ntiles, tile_counter, status, smem_cap_words, scratch);
 }
 
 #endif  // ATB_NO_TRACK_KERNEL

@@ -79,6 +79,13 @@ int atb_device_info(int device, char* name, int name_len, int* cc_major, int* cc
 int atb_create(int device, atb_handle** out);
 int atb_destroy(atb_handle* h);
 
+/* Particles per thread of the tracking kernel (1 or 2): with 2, each thread
+ * carries two particles through every element, reusing the element's
+ * parameters and interleaving two dependency chains; the autotuner picks it.
+ * Small particle sets that would not fill the SMs use 1.  Refused while
+ * prepared batches exist.  No reference counterpart (launch tuning). */
+int atb_set_particles_per_thread(atb_handle* h, int32_t ppt);
+
 /* Launch tuning: threads per block (32..512, multiple of 32), shared-memory
  * segment capacity in 8-byte words, largest table kept resident in shared
  * memory, and the device-memory budget for refpts snapshots.  0 keeps the

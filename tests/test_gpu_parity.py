@@ -270,3 +270,56 @@ def test_all_lost_tiles_stop_early(ring_name, pattern):
     np.testing.assert_array_equal(la["islost"], lo["islost"])
     np.testing.assert_array_equal(la["turn"], lo["turn"])
     np.testing.assert_array_equal(la["elem"], lo["elem"])
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+@pytest.mark.parametrize("ring_name", ["fodo", "large"])
+def test_two_particles_per_thread_match_one(ring_name, mode):
+    """Two particles per thread (particle k of thread t at
+    tile.first + k*blockDim + t) against one.  exact: every particle runs the
+    same correctly rounded operations, so coordinates, refpts snapshots, loss
+    maps and per-turn survivor counts are bit-identical.  fast: the compiler
+    may contract a product shared by the two particles differently, so
+    coordinates agree to 1e-15 of their scale (1-ulp steps measured on these
+    cases) with the same loss map.  The set (ragged, ~10 % lost) fills every
+    SM with full two-particle tiles, the size at which the engine uses them."""
+    from at_b200.engine import device_info
+    eng = Engine.get(0)
+    n = device_info(0)[3] * 128 * 2 + 77
+    if ring_name == "fodo":
+        ring, en, rest = rings.radiating(rings.fodo_ring()), 3e9, ELECTRON_REST
+        r0 = rings.gaussian(n, seed=12)
+        nt, refs = 20, np.array([0, 3, 7], dtype=np.uint32)
+    else:
+        ring = rings.large_ring()
+        en, rest = ring.energy, ring.particle.rest_energy
+        r0 = rings.large_ring_bunch(n, seed=12)
+        nt, refs = 3, np.array([0, 500], dtype=np.uint32)
+    r0[:, 5::10] *= 1e3
+    cl = compile_lattice(ring, en, rest)
+    lid = eng.upload(cl)
+    out = []
+    try:
+        for ppt in (1, 2):
+            eng.set_launch(threads=128, particles_per_thread=ppt)
+            r = r0.copy(order="F")
+            rout, ld, st = eng.track(lid, r, nt, 0, 0, cl.nelem, refpts=refs, losses=True,
+                                     stats=True, mode=mode)
+            out.append((r, rout, ld, st))
+    finally:
+        eng.set_launch(threads=256, particles_per_thread=1)
+        eng.free(lid)
+    (ra, oa, la, sa), (rb, ob, lb, sb) = out
+    if mode == "exact":
+        np.testing.assert_array_equal(ra, rb)
+        np.testing.assert_array_equal(oa, ob)
+        np.testing.assert_array_equal(la["coord"], lb["coord"])
+    else:
+        ok = ~la["islost"]
+        assert scale_rel_diff(rb[:, ok], ra[:, ok]) <= 1e-15
+        assert scale_rel_diff(ob[:, ok], oa[:, ok]) <= 1e-15
+    for k in ("islost", "turn", "elem"):
+        np.testing.assert_array_equal(la[k], lb[k])
+    assert la["islost"].any() and not la["islost"].all()
+    np.testing.assert_array_equal(sa[0], sb[0])
+    np.testing.assert_allclose(sa[1], sb[1], rtol=1e-12, atol=1e-300)
