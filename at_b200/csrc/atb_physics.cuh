@@ -192,6 +192,28 @@ __device__ __forceinline__ void horner_fixed(const double* A, const double* B, c
     for (int i = MO - 1; i >= 0; --i) horner_step(re, im, x, y, B[i], A[i]);
 }
 
+/* The same recursion for an upright magnet (every A_n = 0, fast kernels
+ * only): the first step starts from Im = 0, so it is re B_MO x + B_{MO-1},
+ * im = B_MO y, and later steps add no A_n.  Equal to horner_fixed up to the
+ * sign of a zero. */
+template <int MO, class T>
+__device__ __forceinline__ void horner_upright(const double* B, const T& x, const T& y, T& re,
+                                               T& im) {
+    if constexpr (MO == 0) {
+        re = B[0];
+        im = 0.0;
+    } else {
+        re = fma(B[MO], x, B[MO - 1]);
+        im = B[MO] * y;
+#pragma unroll
+        for (int i = MO - 2; i >= 0; --i) {
+            const T ret = fma(re, x, fma(-im, y, B[i]));
+            im = fma(im, x, re * y);
+            re = ret;
+        }
+    }
+}
+
 template <class T>
 __device__ __forceinline__ void horner_dyn(const double* A, const double* B, int mo, const T& x,
                                            const T& y, T& re, T& im) {
@@ -223,13 +245,16 @@ __device__ __forceinline__ void seed_coef(double x, double y, int k, T& re, T& i
  * registers once per element; MO < 0 reads them (broadcast) from the staged
  * table on every kick.  set_param() (tangent kernel only) replaces B_k by a
  * runtime strength and marks it as the differentiated parameter. */
-template <int MO>
+template <int MO, bool SKEW = true>
 struct Poly {
-    double a[MO + 1], b[MO + 1];
+    double a[SKEW ? MO + 1 : 1], b[MO + 1];
     int sk;
     __device__ __forceinline__ void load(const double* A, const double* B, int) {
 #pragma unroll
-        for (int i = 0; i <= MO; ++i) { a[i] = A[i]; b[i] = B[i]; }
+        for (int i = 0; i <= MO; ++i) {
+            if constexpr (SKEW) a[i] = A[i];
+            b[i] = B[i];
+        }
         sk = -1;
     }
     __device__ __forceinline__ void set_param(int k, double v) {
@@ -240,7 +265,8 @@ struct Poly {
     }
     template <class T>
     __device__ __forceinline__ void field(const T& x, const T& y, T& re, T& im) const {
-        horner_fixed<MO>(a, b, x, y, re, im);
+        if constexpr (SKEW) horner_fixed<MO>(a, b, x, y, re, im);
+        else horner_upright<MO>(b, x, y, re, im);
         seed_coef(val(x), val(y), sk, re, im);
     }
 };

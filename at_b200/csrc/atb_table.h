@@ -68,6 +68,8 @@
 #define ATB_F_FINT_IN      (1u << 15)  /* bend entrance FringeInt1 > 0 and FullGap > 0
                                           (the diffusion-matrix edge term)  */
 #define ATB_F_FINT_OUT     (1u << 16)  /* bend exit FringeInt2 > 0 and FullGap > 0 */
+#define ATB_F_NOSKEW       (1u << 17)  /* thick multipole: every PolynomA
+                                          coefficient (KickAngle folded) is 0 */
 /* bend fringe "method" codes after host normalisation (atphyslib.c:15-79) */
 #define ATB_BM_LEGACY      0   /* method 0 or any value other than 1,2,3   */
 #define ATB_BM_1           1

@@ -163,7 +163,7 @@ __device__ __forceinline__ T fringe_b1(const Rec& e, const Param& pm) {
 
 /* StrMPoleSymplectic4Pass.c:29-109, BndMPoleSymplectic4Pass.c:38-129,
  * StrMPoleSymplectic4RadPass.c:30-115, BndMPoleSymplectic4RadPass.c:39-128 */
-template <int MO, bool BEND, bool RAD, class T>
+template <int MO, bool BEND, bool RAD, bool SKEW = true, class T>
 __device__ __forceinline__ void pass_multipole(P6T<T>& r, const Rec& e, const Param& pm) {
     const uint32_t fl = e.flags();
     const double L1 = e.f(ATB_SM_L1), L2 = e.f(ATB_SM_L2);
@@ -171,7 +171,7 @@ __device__ __forceinline__ void pass_multipole(P6T<T>& r, const Rec& e, const Pa
     const int mo = e.mo();
     const double* A = e.p + (BEND ? ATB_BM_POLY : ATB_SM_POLY);
     const double* B = A + mo + 1;
-    Poly<MO> pl;
+    Poly<MO, SKEW> pl;
     pl.load(A, B, mo);
     if constexpr (is_dual<T>::value) {
         if (pm.k >= 0) pl.set_param(pm.k, pm.v);
@@ -276,11 +276,23 @@ __device__ __forceinline__ void pass_multipole_dispatch(P6T<T>& r, const Rec& e,
         /* one generic instance for the tangent kernel keeps its size sane */
         pass_multipole<-1, BEND, RAD>(r, e, pm);
     } else {
+        /* the fast kernels evaluate upright magnets' fields without the
+           zero skew terms */
+        const bool upright = kFast && (e.flags() & ATB_F_NOSKEW);
         switch (e.mo()) {
             case 0: pass_multipole<0, BEND, RAD>(r, e, pm); break;
-            case 1: pass_multipole<1, BEND, RAD>(r, e, pm); break;
-            case 2: pass_multipole<2, BEND, RAD>(r, e, pm); break;
-            case 3: pass_multipole<3, BEND, RAD>(r, e, pm); break;
+            case 1:
+                if (upright) pass_multipole<1, BEND, RAD, !kFast>(r, e, pm);
+                else pass_multipole<1, BEND, RAD>(r, e, pm);
+                break;
+            case 2:
+                if (upright) pass_multipole<2, BEND, RAD, !kFast>(r, e, pm);
+                else pass_multipole<2, BEND, RAD>(r, e, pm);
+                break;
+            case 3:
+                if (upright) pass_multipole<3, BEND, RAD, !kFast>(r, e, pm);
+                else pass_multipole<3, BEND, RAD>(r, e, pm);
+                break;
             default: pass_multipole<-1, BEND, RAD>(r, e, pm); break;
         }
     }

@@ -385,6 +385,8 @@ def _multipole_common(rec: _Record, el, op: int, bend: bool):
         rec.set(base + i, v)
     for i, v in enumerate(B):
         rec.set(base + mo + 1 + i, v)
+    if all(v == 0.0 for v in A):
+        rec.flags |= T.ATB_F_NOSKEW
 
 
 @dataclass
