@@ -319,11 +319,80 @@ __device__ __forceinline__ void bndthinkick(P6T<T>& r, const PL& pl, double L, d
     r.ct += lirho * r.x;
 }
 
-/* Radiating kicks.  ``pn`` carries 1/(1+delta) between steps in FAST mode,
- * and ``rL`` = radc * L is folded once per element.  The FAST forms group the
- * energy-loss product as (rL q)(h vn) opd^2, q = B2perp before the 1/(1+s)
- * normalisation, and evaluate 1/(1+s) for s = x'^2 + y'^2 < 1e-5 by its
- * series 1 - s + s^2 - s^3 (truncation below 1e-20). */
+/* Radiating kicks and drifts in the reference's expression order
+ * (exact and tangent kernels). */
+
+/* diff_str_kick.c:19-83 with B2perp of diff_str_kick.c:1-17 (bdiff == NULL) */
+template <class PL, class T>
+__device__ __forceinline__ void str_kick_rad(P6T<T>& r, const PL& pl, double L, double radc) {
+    T re, im;
+    pl.field(r.x, r.y, re, im);
+    T p_norm = 1.0 / (1.0 + r.dp);
+    T xpr = r.px * p_norm;
+    T ypr = r.py * p_norm;
+    T v_norm2 = 1.0 / (1.0 + xpr * xpr + ypr * ypr);
+    T bx = im, by = re;
+    T b2p = (by * by + bx * bx + (bx * ypr - by * xpr) * (bx * ypr - by * xpr)) * v_norm2;
+    T factor = (1.0 + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
+    r.dp -= radc * b2p * factor;
+    p_norm = 1.0 / (1.0 + r.dp);
+    r.px = xpr / p_norm;
+    r.py = ypr / p_norm;
+    r.px -= L * re;
+    r.py += L * im;
+}
+
+/* diff_bnd_kick.c:101-174 with its B2perp (:85-99), bdiff == NULL */
+template <class PL, class T>
+__device__ __forceinline__ void bnd_kick_rad(P6T<T>& r, const PL& pl, double L, double irho,
+                                             double lirho, double radc) {
+    T re, im;
+    pl.field(r.x, r.y, re, im);
+    T p_norm = 1.0 / (1.0 + r.dp);
+    T x = r.x;
+    T xpr = r.px * p_norm;
+    T ypr = r.py * p_norm;
+    T bx = im, by = re + irho;
+    T v_norm2 = 1.0 / ((1.0 + x * irho) * (1.0 + x * irho) + xpr * xpr + ypr * ypr);
+    T b2p = ((by * (1 + x * irho)) * (by * (1 + x * irho)) +
+             (bx * (1 + x * irho)) * (bx * (1 + x * irho)) +
+             (bx * ypr - by * xpr) * (bx * ypr - by * xpr)) * v_norm2;
+    T factor = (1.0 + x * irho + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
+    T dp_0 = r.dp;
+    r.dp -= radc * b2p * factor;
+    p_norm = 1.0 / (1.0 + r.dp);
+    r.px = xpr / p_norm;
+    r.py = ypr / p_norm;
+    r.px -= L * (re - (dp_0 - r.x * irho) * irho);
+    r.py += L * im;
+    r.ct += lirho * r.x;
+}
+
+/* diff_drift.c:30-43 (bdiff == NULL) */
+template <class T>
+__device__ __forceinline__ void diff_drift(P6T<T>& r, double L) {
+    T p_norm = 1.0 / (1.0 + r.dp);
+    T NormL = L * p_norm;
+    r.x += NormL * r.px;
+    r.y += NormL * r.py;
+    r.ct += NormL * p_norm * (r.px * r.px + r.py * r.py) / 2.0;
+}
+
+/* The fast kernels' radiating integrator.  Inside a radiating magnet they
+ * carry the angles x' = px/(1+delta), y' = py/(1+delta) in place of px, py:
+ * the reference's drift (diff_drift.c:30-43) advances x by L x', y by L y'
+ * and ct by L (x'^2 + y'^2)/2, and its kicks (diff_str_kick.c:19-83,
+ * diff_bnd_kick.c:101-174) rescale px, py so that x', y' pass through the
+ * energy loss unchanged before the field kick -L Re (px), +L Im (py), which
+ * moves x' by -L Re/(1+delta').  Each drift hands s = x'^2 + y'^2 to the
+ * kick after it.  The energy-loss product is grouped as (rL q)(h vn) opd^2
+ * with rL = radc * L folded per element, q = B2perp before its 1/(1+s)
+ * normalisation, and 1/(1+s) for s < 1e-5 is its series 1 - s + s^2 - s^3
+ * (truncation below 1e-20).  The caller converts px = x'(1+delta),
+ * py = y'(1+delta) at the magnet's exit. */
+struct RadAngles {
+    double xp, yp, s;
+};
 
 __device__ __forceinline__ double inv_one_plus_small(double s) {
     if (s < 1e-5) {
@@ -333,106 +402,52 @@ __device__ __forceinline__ double inv_one_plus_small(double s) {
     return rcp_nr(1.0 + s);
 }
 
-/* diff_str_kick.c:19-83 with B2perp of diff_str_kick.c:1-17 (bdiff == NULL) */
-template <bool FAST, class PL, class T>
-__device__ __forceinline__ void str_kick_rad(P6T<T>& r, const PL& pl, double L, double radc,
-                                             double rL, T& pn) {
-    T re, im;
-    pl.field(r.x, r.y, re, im);
-    if constexpr (FAST) {
-        const double xpr = r.px * pn;
-        const double ypr = r.py * pn;
-        const double s = fma(xpr, xpr, ypr * ypr);
-        const double vn = inv_one_plus_small(s);
-        const double cr = fma(im, ypr, -(re * xpr));
-        const double q = fma(re, re, fma(im, im, cr * cr));
-        const double opd = 1.0 + r.dp;
-        const double h = fma(0.5, s, 1.0);
-        r.dp = fma(-(rL * q) * (h * vn), opd * opd, r.dp);
-        const double opd2 = 1.0 + r.dp;
-        pn = rcp_nr(opd2);
-        r.px = fma(xpr, opd2, -L * re);
-        r.py = fma(ypr, opd2, L * im);
-    } else {
-        T p_norm = 1.0 / (1.0 + r.dp);
-        T xpr = r.px * p_norm;
-        T ypr = r.py * p_norm;
-        T v_norm2 = 1.0 / (1.0 + xpr * xpr + ypr * ypr);
-        T bx = im, by = re;
-        T b2p = (by * by + bx * bx + (bx * ypr - by * xpr) * (bx * ypr - by * xpr)) * v_norm2;
-        T factor = (1.0 + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
-        r.dp -= radc * b2p * factor;
-        p_norm = 1.0 / (1.0 + r.dp);
-        r.px = xpr / p_norm;
-        r.py = ypr / p_norm;
-        r.px -= L * re;
-        r.py += L * im;
-    }
+/* drift of length L, hL = L/2 */
+__device__ __forceinline__ void rad_drift_fast(P6T<double>& r, RadAngles& a, double L,
+                                               double hL) {
+    r.x = fma(L, a.xp, r.x);
+    r.y = fma(L, a.yp, r.y);
+    a.s = fma(a.xp, a.xp, a.yp * a.yp);
+    r.ct = fma(hL, a.s, r.ct);
 }
 
-/* diff_bnd_kick.c:101-174 with its B2perp (:85-99), bdiff == NULL */
-template <bool FAST, class PL, class T>
-__device__ __forceinline__ void bnd_kick_rad(P6T<T>& r, const PL& pl, double L, double irho,
-                                             double lirho, double radc, double rL, T& pn) {
-    T re, im;
+template <class PL>
+__device__ __forceinline__ void str_kick_rad_fast(P6T<double>& r, RadAngles& a, const PL& pl,
+                                                  double L, double rL) {
+    double re, im;
     pl.field(r.x, r.y, re, im);
-    if constexpr (FAST) {
-        const double xpr = r.px * pn;
-        const double ypr = r.py * pn;
-        const double hx = fma(r.x, irho, 1.0);
-        const double hx2 = hx * hx;
-        const double s = fma(xpr, xpr, ypr * ypr);
-        const double vn = rcp_nr(hx2 + s);
-        const double by = re + irho;
-        const double cr = fma(im, ypr, -(by * xpr));
-        const double q = fma(fma(by, by, im * im), hx2, cr * cr);
-        const double opd = 1.0 + r.dp;
-        const double h = fma(0.5, s, hx);
-        const double dp0 = r.dp;
-        r.dp = fma(-(rL * q) * (h * vn), opd * opd, r.dp);
-        const double opd2 = 1.0 + r.dp;
-        pn = rcp_nr(opd2);
-        const double u = fma(-fma(-r.x, irho, dp0), irho, re);
-        r.px = fma(xpr, opd2, -L * u);
-        r.py = fma(ypr, opd2, L * im);
-        r.ct = fma(lirho, r.x, r.ct);
-    } else {
-        T p_norm = 1.0 / (1.0 + r.dp);
-        T x = r.x;
-        T xpr = r.px * p_norm;
-        T ypr = r.py * p_norm;
-        T bx = im, by = re + irho;
-        T v_norm2 = 1.0 / ((1.0 + x * irho) * (1.0 + x * irho) + xpr * xpr + ypr * ypr);
-        T b2p = ((by * (1 + x * irho)) * (by * (1 + x * irho)) +
-                 (bx * (1 + x * irho)) * (bx * (1 + x * irho)) +
-                 (bx * ypr - by * xpr) * (bx * ypr - by * xpr)) * v_norm2;
-        T factor = (1.0 + x * irho + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
-        T dp_0 = r.dp;
-        r.dp -= radc * b2p * factor;
-        p_norm = 1.0 / (1.0 + r.dp);
-        r.px = xpr / p_norm;
-        r.py = ypr / p_norm;
-        r.px -= L * (re - (dp_0 - r.x * irho) * irho);
-        r.py += L * im;
-        r.ct += lirho * r.x;
-    }
+    const double vn = inv_one_plus_small(a.s);
+    const double cr = fma(im, a.yp, -(re * a.xp));
+    const double q = fma(re, re, fma(im, im, cr * cr));
+    const double opd = 1.0 + r.dp;
+    const double h = fma(0.5, a.s, 1.0);
+    r.dp = fma(-(rL * q) * (h * vn), opd * opd, r.dp);
+    const double pn = rcp_nr(1.0 + r.dp);
+    a.xp = fma(-L * re, pn, a.xp);
+    a.yp = fma(L * im, pn, a.yp);
 }
 
-/* diff_drift.c:30-43 inside a radiating magnet; FAST reuses pn = 1/(1+delta) */
-template <bool FAST, class T>
-__device__ __forceinline__ void diff_drift(P6T<T>& r, double L, const T& pn) {
-    if constexpr (FAST) {
-        double nl = L * pn;
-        r.x += nl * r.px;
-        r.y += nl * r.py;
-        r.ct += (0.5 * nl * pn) * (r.px * r.px + r.py * r.py);
-    } else {
-        T p_norm = 1.0 / (1.0 + r.dp);
-        T NormL = L * p_norm;
-        r.x += NormL * r.px;
-        r.y += NormL * r.py;
-        r.ct += NormL * p_norm * (r.px * r.px + r.py * r.py) / 2.0;
-    }
+template <class PL>
+__device__ __forceinline__ void bnd_kick_rad_fast(P6T<double>& r, RadAngles& a, const PL& pl,
+                                                  double L, double irho, double lirho,
+                                                  double rL) {
+    double re, im;
+    pl.field(r.x, r.y, re, im);
+    const double hx = fma(r.x, irho, 1.0);
+    const double hx2 = hx * hx;
+    const double vn = rcp_nr(hx2 + a.s);
+    const double by = re + irho;
+    const double cr = fma(im, a.yp, -(by * a.xp));
+    const double q = fma(fma(by, by, im * im), hx2, cr * cr);
+    const double opd = 1.0 + r.dp;
+    const double h = fma(0.5, a.s, hx);
+    const double dp0 = r.dp;
+    r.dp = fma(-(rL * q) * (h * vn), opd * opd, r.dp);
+    const double pn = rcp_nr(1.0 + r.dp);
+    const double u = fma(-fma(-r.x, irho, dp0), irho, re);
+    a.xp = fma(-L * u, pn, a.xp);
+    a.yp = fma(L * im, pn, a.yp);
+    r.ct = fma(lirho, r.x, r.ct);
 }
 
 /* quadfringe.c:3-51 QuadFringePassP (sign=+1) / QuadFringePassN (sign=-1) */

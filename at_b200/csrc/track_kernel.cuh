@@ -213,20 +213,41 @@ __device__ __forceinline__ void pass_multipole(P6T<T>& r, const Rec& e, const Pa
     const int ns = e.nsteps();
     if (RAD) {
         const double radc = e.f(ATB_SM_RADC);
-        const double rk1 = kFast ? radc * K1 : 0.0, rk2 = kFast ? radc * K2 : 0.0;
-        T pn = 0.0;
-        if (kFast) pn = 1.0 / (1.0 + r.dp);
-        for (int m = 0; m < ns; ++m) {
-            diff_drift<kFast>(r, L1, pn);
-            if (BEND) bnd_kick_rad<kFast>(r, pl, K1, irho, k1i, radc, rk1, pn);
-            else str_kick_rad<kFast>(r, pl, K1, radc, rk1, pn);
-            diff_drift<kFast>(r, L2, pn);
-            if (BEND) bnd_kick_rad<kFast>(r, pl, K2, irho, k2i, radc, rk2, pn);
-            else str_kick_rad<kFast>(r, pl, K2, radc, rk2, pn);
-            diff_drift<kFast>(r, L2, pn);
-            if (BEND) bnd_kick_rad<kFast>(r, pl, K1, irho, k1i, radc, rk1, pn);
-            else str_kick_rad<kFast>(r, pl, K1, radc, rk1, pn);
-            diff_drift<kFast>(r, L1, pn);
+        if constexpr (kFast && !is_dual<T>::value) {
+            if (ns > 0) {
+                const double rk1 = radc * K1, rk2 = radc * K2;
+                const double h1 = 0.5 * L1, h2 = 0.5 * L2;
+                const double pn = 1.0 / (1.0 + r.dp);
+                RadAngles a{r.px * pn, r.py * pn, 0.0};
+                for (int m = 0; m < ns; ++m) {
+                    rad_drift_fast(r, a, L1, h1);
+                    if (BEND) bnd_kick_rad_fast(r, a, pl, K1, irho, k1i, rk1);
+                    else str_kick_rad_fast(r, a, pl, K1, rk1);
+                    rad_drift_fast(r, a, L2, h2);
+                    if (BEND) bnd_kick_rad_fast(r, a, pl, K2, irho, k2i, rk2);
+                    else str_kick_rad_fast(r, a, pl, K2, rk2);
+                    rad_drift_fast(r, a, L2, h2);
+                    if (BEND) bnd_kick_rad_fast(r, a, pl, K1, irho, k1i, rk1);
+                    else str_kick_rad_fast(r, a, pl, K1, rk1);
+                    rad_drift_fast(r, a, L1, h1);
+                }
+                const double opd = 1.0 + r.dp;
+                r.px = a.xp * opd;
+                r.py = a.yp * opd;
+            }
+        } else {
+            for (int m = 0; m < ns; ++m) {
+                diff_drift(r, L1);
+                if (BEND) bnd_kick_rad(r, pl, K1, irho, k1i, radc);
+                else str_kick_rad(r, pl, K1, radc);
+                diff_drift(r, L2);
+                if (BEND) bnd_kick_rad(r, pl, K2, irho, k2i, radc);
+                else str_kick_rad(r, pl, K2, radc);
+                diff_drift(r, L2);
+                if (BEND) bnd_kick_rad(r, pl, K1, irho, k1i, radc);
+                else str_kick_rad(r, pl, K1, radc);
+                diff_drift(r, L1);
+            }
         }
     } else {
         T c1 = 0.0, c2 = 0.0;

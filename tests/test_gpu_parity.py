@@ -341,8 +341,13 @@ def _clear_flag(cl, bit):
 @pytest.mark.parametrize("ring_name", ["fodo", "fodo_rad", "large"])
 def test_upright_field_evaluation_matches_general(ring_name):
     """The fast kernel evaluates upright magnets (every PolynomA zero) from
-    Im = 0 without the skew terms; the result equals the general recursion
-    on the same table with the upright flag cleared."""
+    Im = 0 without the skew terms, the same values as the general recursion
+    up to the sign of a zero.  The two instances of the magnet code around it
+    are compiled apart, so the compiler's FMA contraction may differ between
+    them: on the same table with the upright flag cleared the results agree
+    within the fast mode's one-turn bound (measured: identical on the
+    radiating rings, one coordinate one ulp apart on the plain FODO ring),
+    with the same loss map."""
     from at_b200 import table as T
     if ring_name.startswith("fodo"):
         ring, en, rest = rings.fodo_ring(), 3e9, ELECTRON_REST
@@ -365,5 +370,6 @@ def test_upright_field_evaluation_matches_general(ring_name):
         finally:
             eng.free(lid)
         out.append((r, ld))
-    np.testing.assert_array_equal(out[0][0], out[1][0])
     np.testing.assert_array_equal(out[0][1]["islost"], out[1][1]["islost"])
+    ok = ~out[0][1]["islost"]
+    assert scale_rel_diff(out[0][0][:, ok], out[1][0][:, ok]) <= 2e-13
