@@ -192,7 +192,7 @@ __device__ __forceinline__ void bd_edge(P6& r, double irho, double edge, double 
     r.py -= r.y * fy;
 }
 
-/* a radiating multipole with B, as pass_multipole<RAD> in the exact kernel */
+/* a radiating multipole with B, as the radiating multipole pass of the exact kernel */
 template <bool BEND>
 __device__ void bd_multipole(P6& r, const Rec& e, double diffc, double* B) {
     const uint32_t fl = e.flags();

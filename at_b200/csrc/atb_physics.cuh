@@ -385,22 +385,17 @@ __device__ __forceinline__ void diff_drift(P6T<T>& r, double L) {
  * diff_bnd_kick.c:101-174) rescale px, py so that x', y' pass through the
  * energy loss unchanged before the field kick -L Re (px), +L Im (py), which
  * moves x' by -L Re/(1+delta').  Each drift hands s = x'^2 + y'^2 to the
- * kick after it.  The energy-loss product is grouped as (rL q)(h vn) opd^2
- * with rL = radc * L folded per element, q = B2perp before its 1/(1+s)
- * normalisation, and 1/(1+s) for s < 1e-5 is its series 1 - s + s^2 - s^3
- * (truncation below 1e-20).  The caller converts px = x'(1+delta),
- * py = y'(1+delta) at the magnet's exit. */
+ * kick after it, and each kick hands opd = 1 + delta to the next (drifts
+ * leave delta alone).  The energy-loss product is grouped as
+ * (rL q) g opd^2 with rL = radc * L folded per element, q = B2perp before
+ * its normalisation and g the normalisation times the path-length factor:
+ * (1 + s/2)/(1 + s) in a straight magnet, evaluated for s < 1e-5 as its
+ * series 1 - s/2 + s^2/2 (truncation below 5e-16 of a loss that is itself
+ * ~1e-8 of delta), and (h_x + s/2)/(h_x^2 + s) in a bend.  The caller
+ * converts px = x' opd, py = y' opd at the magnet's exit. */
 struct RadAngles {
-    double xp, yp, s;
+    double xp, yp, s, opd;
 };
-
-__device__ __forceinline__ double inv_one_plus_small(double s) {
-    if (s < 1e-5) {
-        const double t = fma(-s, 1.0 - s, 1.0);
-        return fma(-s, t, 1.0);
-    }
-    return rcp_nr(1.0 + s);
-}
 
 /* drift of length L, hL = L/2 */
 __device__ __forceinline__ void rad_drift_fast(P6T<double>& r, RadAngles& a, double L,
@@ -416,13 +411,13 @@ __device__ __forceinline__ void str_kick_rad_fast(P6T<double>& r, RadAngles& a, 
                                                   double L, double rL) {
     double re, im;
     pl.field(r.x, r.y, re, im);
-    const double vn = inv_one_plus_small(a.s);
+    const double g = a.s < 1e-5 ? fma(a.s, fma(0.5, a.s, -0.5), 1.0)
+                                : fma(0.5, a.s, 1.0) * rcp_nr(1.0 + a.s);
     const double cr = fma(im, a.yp, -(re * a.xp));
     const double q = fma(re, re, fma(im, im, cr * cr));
-    const double opd = 1.0 + r.dp;
-    const double h = fma(0.5, a.s, 1.0);
-    r.dp = fma(-(rL * q) * (h * vn), opd * opd, r.dp);
-    const double pn = rcp_nr(1.0 + r.dp);
+    r.dp = fma(-(rL * q) * g, a.opd * a.opd, r.dp);
+    a.opd = 1.0 + r.dp;
+    const double pn = rcp_nr(a.opd);
     a.xp = fma(-L * re, pn, a.xp);
     a.yp = fma(L * im, pn, a.yp);
 }
@@ -439,11 +434,11 @@ __device__ __forceinline__ void bnd_kick_rad_fast(P6T<double>& r, RadAngles& a, 
     const double by = re + irho;
     const double cr = fma(im, a.yp, -(by * a.xp));
     const double q = fma(fma(by, by, im * im), hx2, cr * cr);
-    const double opd = 1.0 + r.dp;
     const double h = fma(0.5, a.s, hx);
     const double dp0 = r.dp;
-    r.dp = fma(-(rL * q) * (h * vn), opd * opd, r.dp);
-    const double pn = rcp_nr(1.0 + r.dp);
+    r.dp = fma(-(rL * q) * (h * vn), a.opd * a.opd, r.dp);
+    a.opd = 1.0 + r.dp;
+    const double pn = rcp_nr(a.opd);
     const double u = fma(-fma(-r.x, irho, dp0), irho, re);
     a.xp = fma(-L * u, pn, a.xp);
     a.yp = fma(L * im, pn, a.yp);

@@ -162,9 +162,14 @@ __device__ __forceinline__ T fringe_b1(const Rec& e, const Param& pm) {
 }
 
 /* StrMPoleSymplectic4Pass.c:29-109, BndMPoleSymplectic4Pass.c:38-129,
- * StrMPoleSymplectic4RadPass.c:30-115, BndMPoleSymplectic4RadPass.c:39-128 */
-template <int MO, bool BEND, bool RAD, bool SKEW = true, class T>
-__device__ __forceinline__ void pass_multipole(P6T<T>& r, const Rec& e, const Param& pm) {
+ * StrMPoleSymplectic4RadPass.c:30-115, BndMPoleSymplectic4RadPass.c:39-128.
+ * NP particles of one thread pass the element together: every per-particle
+ * step is an unrolled loop over them, so in the slice loop their drifts and
+ * kicks form one straight-line block whose independent chains the compiler
+ * interleaves (NP = 2), while the element's parameters are read once.  Each
+ * particle sees the same operations as alone (NP = 1). */
+template <int NP, int MO, bool BEND, bool RAD, bool SKEW = true, class T>
+__device__ __forceinline__ void pass_multipole_n(P6T<T>* r, const Rec& e, const Param& pm) {
     const uint32_t fl = e.flags();
     const double L1 = e.f(ATB_SM_L1), L2 = e.f(ATB_SM_L2);
     const double K1 = e.f(ATB_SM_K1), K2 = e.f(ATB_SM_K2);
@@ -177,37 +182,50 @@ __device__ __forceinline__ void pass_multipole(P6T<T>& r, const Rec& e, const Pa
         if (pm.k >= 0) pl.set_param(pm.k, pm.v);
     }
 
-    if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_SM_SCALE));
-    T nl1 = 0.0, nl2 = 0.0;
-    if (!RAD) {
-        T p_norm = 1.0 / (1.0 + r.dp);
-        nl1 = L1 * p_norm;
-        nl2 = L2 * p_norm;
+    T nl1[NP], nl2[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        if (fl & ATB_F_SCALING) change_pref<kFast>(r[k], e.f(ATB_SM_SCALE));
+        nl1[k] = 0.0;
+        nl2[k] = 0.0;
+        if (!RAD) {
+            T p_norm = 1.0 / (1.0 + r[k].dp);
+            nl1[k] = L1 * p_norm;
+            nl2[k] = L2 * p_norm;
+        }
+        entrance_misalign(r[k], e);
+        apertures(r[k], e);
     }
-    entrance_misalign(r, e);
-    apertures(r, e);
     double irho = 0.0, k1i = 0.0, k2i = 0.0;
     if (BEND) {
         irho = e.f(ATB_BM_IRHO);
         k1i = e.f(ATB_BM_K1IRHO);
         k2i = e.f(ATB_BM_K2IRHO);
         const int m_in = (int)((fl >> ATB_F_BM_IN_SHIFT) & ATB_F_BM_MASK);
-        if (RAD)
-            edge_fringe_rad<kFast>(r, irho, e.f(ATB_BM_EIN), e.f(ATB_BM_FCIN), e.f(ATB_BM_FXIN),
-                                   e.f(ATB_BM_FYIN), m_in, fl & ATB_F_FC0_IN, 1.0);
-        else
-            edge_fringe<kFast>(r, irho, e.f(ATB_BM_EIN), e.f(ATB_BM_FCIN), e.f(ATB_BM_FXIN),
-                               e.f(ATB_BM_FYIN), m_in, fl & ATB_F_FC0_IN, 1.0);
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            if (RAD)
+                edge_fringe_rad<kFast>(r[k], irho, e.f(ATB_BM_EIN), e.f(ATB_BM_FCIN),
+                                       e.f(ATB_BM_FXIN), e.f(ATB_BM_FYIN), m_in,
+                                       fl & ATB_F_FC0_IN, 1.0);
+            else
+                edge_fringe<kFast>(r[k], irho, e.f(ATB_BM_EIN), e.f(ATB_BM_FCIN),
+                                   e.f(ATB_BM_FXIN), e.f(ATB_BM_FYIN), m_in, fl & ATB_F_FC0_IN,
+                                   1.0);
+        }
     }
     if (fl & ATB_F_FQ_IN) {
         const T b1 = fringe_b1<T>(e, pm);
-        if (fl & ATB_F_FQ_IN_LIN) {
-            const double* fm = e.blk(ATB_OPT_FRINGE);
-            lin_fringe_map(r, fm);
-            quad_fringe<kFast>(r, b1, true);
-            lin_fringe_map(r, fm + 8);
-        } else {
-            quad_fringe<kFast>(r, b1, true);
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            if (fl & ATB_F_FQ_IN_LIN) {
+                const double* fm = e.blk(ATB_OPT_FRINGE);
+                lin_fringe_map(r[k], fm);
+                quad_fringe<kFast>(r[k], b1, true);
+                lin_fringe_map(r[k], fm + 8);
+            } else {
+                quad_fringe<kFast>(r[k], b1, true);
+            }
         }
     }
     const int ns = e.nsteps();
@@ -217,106 +235,160 @@ __device__ __forceinline__ void pass_multipole(P6T<T>& r, const Rec& e, const Pa
             if (ns > 0) {
                 const double rk1 = radc * K1, rk2 = radc * K2;
                 const double h1 = 0.5 * L1, h2 = 0.5 * L2;
-                const double pn = 1.0 / (1.0 + r.dp);
-                RadAngles a{r.px * pn, r.py * pn, 0.0};
-                for (int m = 0; m < ns; ++m) {
-                    rad_drift_fast(r, a, L1, h1);
-                    if (BEND) bnd_kick_rad_fast(r, a, pl, K1, irho, k1i, rk1);
-                    else str_kick_rad_fast(r, a, pl, K1, rk1);
-                    rad_drift_fast(r, a, L2, h2);
-                    if (BEND) bnd_kick_rad_fast(r, a, pl, K2, irho, k2i, rk2);
-                    else str_kick_rad_fast(r, a, pl, K2, rk2);
-                    rad_drift_fast(r, a, L2, h2);
-                    if (BEND) bnd_kick_rad_fast(r, a, pl, K1, irho, k1i, rk1);
-                    else str_kick_rad_fast(r, a, pl, K1, rk1);
-                    rad_drift_fast(r, a, L1, h1);
+                RadAngles a[NP];
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    const double pn = 1.0 / (1.0 + r[k].dp);
+                    a[k] = RadAngles{r[k].px * pn, r[k].py * pn, 0.0, 1.0 + r[k].dp};
                 }
-                const double opd = 1.0 + r.dp;
-                r.px = a.xp * opd;
-                r.py = a.yp * opd;
+                for (int m = 0; m < ns; ++m) {
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) rad_drift_fast(r[k], a[k], L1, h1);
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) {
+                        if (BEND) bnd_kick_rad_fast(r[k], a[k], pl, K1, irho, k1i, rk1);
+                        else str_kick_rad_fast(r[k], a[k], pl, K1, rk1);
+                    }
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) rad_drift_fast(r[k], a[k], L2, h2);
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) {
+                        if (BEND) bnd_kick_rad_fast(r[k], a[k], pl, K2, irho, k2i, rk2);
+                        else str_kick_rad_fast(r[k], a[k], pl, K2, rk2);
+                    }
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) rad_drift_fast(r[k], a[k], L2, h2);
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) {
+                        if (BEND) bnd_kick_rad_fast(r[k], a[k], pl, K1, irho, k1i, rk1);
+                        else str_kick_rad_fast(r[k], a[k], pl, K1, rk1);
+                    }
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) rad_drift_fast(r[k], a[k], L1, h1);
+                }
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    r[k].px = a[k].xp * a[k].opd;
+                    r[k].py = a[k].yp * a[k].opd;
+                }
             }
         } else {
             for (int m = 0; m < ns; ++m) {
-                diff_drift(r, L1);
-                if (BEND) bnd_kick_rad(r, pl, K1, irho, k1i, radc);
-                else str_kick_rad(r, pl, K1, radc);
-                diff_drift(r, L2);
-                if (BEND) bnd_kick_rad(r, pl, K2, irho, k2i, radc);
-                else str_kick_rad(r, pl, K2, radc);
-                diff_drift(r, L2);
-                if (BEND) bnd_kick_rad(r, pl, K1, irho, k1i, radc);
-                else str_kick_rad(r, pl, K1, radc);
-                diff_drift(r, L1);
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    diff_drift(r[k], L1);
+                    if (BEND) bnd_kick_rad(r[k], pl, K1, irho, k1i, radc);
+                    else str_kick_rad(r[k], pl, K1, radc);
+                    diff_drift(r[k], L2);
+                    if (BEND) bnd_kick_rad(r[k], pl, K2, irho, k2i, radc);
+                    else str_kick_rad(r[k], pl, K2, radc);
+                    diff_drift(r[k], L2);
+                    if (BEND) bnd_kick_rad(r[k], pl, K1, irho, k1i, radc);
+                    else str_kick_rad(r[k], pl, K1, radc);
+                    diff_drift(r[k], L1);
+                }
             }
         }
     } else {
-        T c1 = 0.0, c2 = 0.0;
-        if (kFast) {
-            T h = 0.5 / (1.0 + r.dp);
-            c1 = nl1 * h;
-            c2 = nl2 * h;
+        T c1[NP], c2[NP];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            c1[k] = 0.0;
+            c2[k] = 0.0;
+            if (kFast) {
+                T h = 0.5 / (1.0 + r[k].dp);
+                c1[k] = nl1[k] * h;
+                c2[k] = nl2[k] * h;
+            }
         }
         for (int m = 0; m < ns; ++m) {
-            fastdrift<kFast>(r, nl1, c1);
-            if (BEND) bndthinkick(r, pl, K1, irho, k1i); else strthinkick(r, pl, K1);
-            fastdrift<kFast>(r, nl2, c2);
-            if (BEND) bndthinkick(r, pl, K2, irho, k2i); else strthinkick(r, pl, K2);
-            fastdrift<kFast>(r, nl2, c2);
-            if (BEND) bndthinkick(r, pl, K1, irho, k1i); else strthinkick(r, pl, K1);
-            fastdrift<kFast>(r, nl1, c1);
+#pragma unroll
+            for (int k = 0; k < NP; ++k) fastdrift<kFast>(r[k], nl1[k], c1[k]);
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                if (BEND) bndthinkick(r[k], pl, K1, irho, k1i); else strthinkick(r[k], pl, K1);
+            }
+#pragma unroll
+            for (int k = 0; k < NP; ++k) fastdrift<kFast>(r[k], nl2[k], c2[k]);
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                if (BEND) bndthinkick(r[k], pl, K2, irho, k2i); else strthinkick(r[k], pl, K2);
+            }
+#pragma unroll
+            for (int k = 0; k < NP; ++k) fastdrift<kFast>(r[k], nl2[k], c2[k]);
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                if (BEND) bndthinkick(r[k], pl, K1, irho, k1i); else strthinkick(r[k], pl, K1);
+            }
+#pragma unroll
+            for (int k = 0; k < NP; ++k) fastdrift<kFast>(r[k], nl1[k], c1[k]);
         }
     }
     if (fl & ATB_F_FQ_OUT) {
         const T b1 = fringe_b1<T>(e, pm);
-        if (fl & ATB_F_FQ_OUT_LIN) {
-            const double* fm = e.blk(ATB_OPT_FRINGE);
-            lin_fringe_map(r, fm + 16);
-            quad_fringe<kFast>(r, b1, false);
-            lin_fringe_map(r, fm + 24);
-        } else {
-            quad_fringe<kFast>(r, b1, false);
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            if (fl & ATB_F_FQ_OUT_LIN) {
+                const double* fm = e.blk(ATB_OPT_FRINGE);
+                lin_fringe_map(r[k], fm + 16);
+                quad_fringe<kFast>(r[k], b1, false);
+                lin_fringe_map(r[k], fm + 24);
+            } else {
+                quad_fringe<kFast>(r[k], b1, false);
+            }
         }
     }
-    if (BEND) {
-        const int m_out = (int)((fl >> ATB_F_BM_OUT_SHIFT) & ATB_F_BM_MASK);
-        if (RAD)
-            edge_fringe_rad<kFast>(r, irho, e.f(ATB_BM_EOUT), e.f(ATB_BM_FCOUT), e.f(ATB_BM_FXOUT),
-                                   e.f(ATB_BM_FYOUT), m_out, fl & ATB_F_FC0_OUT, -1.0);
-        else
-            edge_fringe<kFast>(r, irho, e.f(ATB_BM_EOUT), e.f(ATB_BM_FCOUT), e.f(ATB_BM_FXOUT),
-                               e.f(ATB_BM_FYOUT), m_out, fl & ATB_F_FC0_OUT, -1.0);
+    const int m_out = (int)((fl >> ATB_F_BM_OUT_SHIFT) & ATB_F_BM_MASK);
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        if (BEND) {
+            if (RAD)
+                edge_fringe_rad<kFast>(r[k], irho, e.f(ATB_BM_EOUT), e.f(ATB_BM_FCOUT),
+                                       e.f(ATB_BM_FXOUT), e.f(ATB_BM_FYOUT), m_out,
+                                       fl & ATB_F_FC0_OUT, -1.0);
+            else
+                edge_fringe<kFast>(r[k], irho, e.f(ATB_BM_EOUT), e.f(ATB_BM_FCOUT),
+                                   e.f(ATB_BM_FXOUT), e.f(ATB_BM_FYOUT), m_out,
+                                   fl & ATB_F_FC0_OUT, -1.0);
+        }
+        apertures(r[k], e);
+        exit_misalign(r[k], e);
+        if (fl & ATB_F_SCALING) change_pref<kFast>(r[k], e.f(ATB_SM_ISCALE));
     }
-    apertures(r, e);
-    exit_misalign(r, e);
-    if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_SM_ISCALE));
 }
 
-template <bool BEND, bool RAD, class T>
-__device__ __forceinline__ void pass_multipole_dispatch(P6T<T>& r, const Rec& e, const Param& pm) {
+template <int NP, bool BEND, bool RAD, class T>
+__device__ __forceinline__ void pass_multipole_dispatch_n(P6T<T>* r, const Rec& e,
+                                                          const Param& pm) {
     if constexpr (is_dual<T>::value) {
         /* one generic instance for the tangent kernel keeps its size sane */
-        pass_multipole<-1, BEND, RAD>(r, e, pm);
+        pass_multipole_n<NP, -1, BEND, RAD>(r, e, pm);
     } else {
         /* the fast kernels evaluate upright magnets' fields without the
            zero skew terms */
         const bool upright = kFast && (e.flags() & ATB_F_NOSKEW);
         switch (e.mo()) {
-            case 0: pass_multipole<0, BEND, RAD>(r, e, pm); break;
+            case 0: pass_multipole_n<NP, 0, BEND, RAD>(r, e, pm); break;
             case 1:
-                if (upright) pass_multipole<1, BEND, RAD, !kFast>(r, e, pm);
-                else pass_multipole<1, BEND, RAD>(r, e, pm);
+                if (upright) pass_multipole_n<NP, 1, BEND, RAD, !kFast>(r, e, pm);
+                else pass_multipole_n<NP, 1, BEND, RAD>(r, e, pm);
                 break;
             case 2:
-                if (upright) pass_multipole<2, BEND, RAD, !kFast>(r, e, pm);
-                else pass_multipole<2, BEND, RAD>(r, e, pm);
+                if (upright) pass_multipole_n<NP, 2, BEND, RAD, !kFast>(r, e, pm);
+                else pass_multipole_n<NP, 2, BEND, RAD>(r, e, pm);
                 break;
             case 3:
-                if (upright) pass_multipole<3, BEND, RAD, !kFast>(r, e, pm);
-                else pass_multipole<3, BEND, RAD>(r, e, pm);
+                if (upright) pass_multipole_n<NP, 3, BEND, RAD, !kFast>(r, e, pm);
+                else pass_multipole_n<NP, 3, BEND, RAD>(r, e, pm);
                 break;
-            default: pass_multipole<-1, BEND, RAD>(r, e, pm); break;
+            default: pass_multipole_n<NP, -1, BEND, RAD>(r, e, pm); break;
         }
     }
+}
+
+template <bool BEND, bool RAD, class T>
+__device__ __forceinline__ void pass_multipole_dispatch(P6T<T>& r, const Rec& e, const Param& pm) {
+    pass_multipole_dispatch_n<1, BEND, RAD>(&r, e, pm);
 }
 
 /* DriftPass.c:16-48 */
@@ -446,6 +518,31 @@ __device__ __forceinline__ void track_element(P6T<T>& r, const Rec& e, int nturn
         case ATB_OP_APERTURE: check_rect(r, e.p + ATB_AP_LIM); break;
         case ATB_OP_QUANTDIFF: pass_quantdiff(r, e, rng_key, p, nturn, ei); break;
         default: break;
+    }
+}
+
+/* The particles of a thread go through a thick multipole together when none
+ * of them is lost (a lost particle skips every element). */
+template <int NP>
+__device__ __forceinline__ bool track_together(const P6 (&r)[NP], const Rec& e) {
+    const int op = e.op();
+    if (op != ATB_OP_STRMPOLE && op != ATB_OP_STRMPOLE_RAD && op != ATB_OP_BNDMPOLE &&
+        op != ATB_OP_BNDMPOLE_RAD)
+        return false;
+    bool all = true;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) all &= !isnan(r[k].x);
+    return all;
+}
+
+template <int NP>
+__device__ __forceinline__ void pass_multipoles_together(P6 (&r)[NP], const Rec& e) {
+    const Param none{-1, 0.0};
+    switch (e.op()) {
+        case ATB_OP_STRMPOLE: pass_multipole_dispatch_n<NP, false, false>(r, e, none); break;
+        case ATB_OP_STRMPOLE_RAD: pass_multipole_dispatch_n<NP, false, true>(r, e, none); break;
+        case ATB_OP_BNDMPOLE: pass_multipole_dispatch_n<NP, true, false>(r, e, none); break;
+        default: pass_multipole_dispatch_n<NP, true, true>(r, e, none); break;
     }
 }
 
@@ -629,11 +726,18 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                         ++slot;
                         nextref = (nri < J.nref) ? J.refpts[nri++] : 0xffffffffu;
                     }
+                    bool together = false;
+                    if constexpr (NP > 1) together = track_together(r, e);
+                    if (together) {
+                        if constexpr (NP > 1) pass_multipoles_together(r, e);
+                    } else {
 #pragma unroll
-                    for (int k = 0; k < NP; ++k) {
-                        track_element(r[k], e, nturn, Param{-1, 0.0}, &J.rng_key, p[k], ei);
-                        if (J.check_loss) apply_loss_rule(J, r[k], lost[k], active[k], p[k], nturn, ei);
+                        for (int k = 0; k < NP; ++k)
+                            track_element(r[k], e, nturn, Param{-1, 0.0}, &J.rng_key, p[k], ei);
                     }
+#pragma unroll
+                    for (int k = 0; k < NP; ++k)
+                        if (J.check_loss) apply_loss_rule(J, r[k], lost[k], active[k], p[k], nturn, ei);
                     w += e.len();
                 }
                 if (!resident) {
