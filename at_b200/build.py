@@ -51,7 +51,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     os.makedirs(BUILD, exist_ok=True)
     nv = nvcc()
     deps = [os.path.join(CSRC, d) for d in DEPS] + [os.path.join(INCLUDE, "atb200.h"), __file__]
-    objs = []
+    objs, jobs = [], []
     for src, flags in UNITS:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
@@ -62,11 +62,19 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
                 cmd += ["-Xptxas", "-v"]
             if verbose:
                 print(" ".join(cmd))
-            p = subprocess.run(cmd, capture_output=True, text=True)
-            if p.returncode != 0:
-                raise RuntimeError("nvcc failed for %s:\n%s" % (src, p.stderr))
-            if ptxas_info or verbose:
-                sys.stderr.write(p.stderr)
+            jobs.append((src, cmd))
+    # the units are independent: compile them side by side
+    running = [(src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                      text=True)) for src, cmd in jobs]
+    failed = []
+    for src, proc in running:
+        _, err = proc.communicate()
+        if proc.returncode != 0:
+            failed.append("nvcc failed for %s:\n%s" % (src, err))
+        elif ptxas_info or verbose:
+            sys.stderr.write(err)
+    if failed:
+        raise RuntimeError("\n".join(failed))
     if force or _stale(LIB, objs):
         tmp = LIB + ".tmp"
         cmd = [nv, *ARCH, "-shared", "-o", tmp, *objs, "-cudart", "static", "-lrt", "-lpthread", "-ldl"]
