@@ -55,6 +55,7 @@ _SIGS = {
     "atb_destroy": ([_vp], C.c_int),
     "atb_set_launch": ([_vp, C.c_int, C.c_int, C.c_int, _i64], C.c_int),
     "atb_set_particles_per_thread": ([_vp, _i32], C.c_int),
+    "atb_set_refill_factor": ([_vp, _i32], C.c_int),
     "atb_lattice_upload": ([_vp, _vp, _i64, _vp, _i32, C.POINTER(_i32)], C.c_int),
     "atb_lattice_update": ([_vp, _i32, _vp, _i64], C.c_int),
     "atb_lattice_free": ([_vp, _i32], C.c_int),

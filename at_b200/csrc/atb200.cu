@@ -32,14 +32,14 @@ __global__ void atb_dfma_probe(double* out, int iters, double a, double b) {
     if (s == 12345.678) out[0] = s;   /* keeps the chains live */
 }
 
-extern "C" __global__ void atb_track_kernel_exact(const AtbJob*, const AtbTile*, int, int*, int*,
-                                                  int, double*);
-extern "C" __global__ void atb_track_kernel_fast(const AtbJob*, const AtbTile*, int, int*, int*,
-                                                 int, double*);
+extern "C" __global__ void atb_track_kernel_exact(const AtbJob*, const AtbTile*, int, int*,
+                                       unsigned long long*, int*, int, double*);
+extern "C" __global__ void atb_track_kernel_fast(const AtbJob*, const AtbTile*, int, int*,
+                                       unsigned long long*, int*, int, double*);
 extern "C" __global__ void atb_track_kernel_exact_np2(const AtbJob*, const AtbTile*, int, int*,
-                                                      int*, int, double*);
+                                       unsigned long long*, int*, int, double*);
 extern "C" __global__ void atb_track_kernel_fast_np2(const AtbJob*, const AtbTile*, int, int*,
-                                                     int*, int, double*);
+                                       unsigned long long*, int*, int, double*);
 
 /* the tracking kernel for an arithmetic mode and a number of particles per
    thread (1 or 2) */
@@ -102,7 +102,8 @@ struct Batch {
     int smem = 0;
     int grid = 0;
     int ntiles = 0;
-    DevBuf jobs, tiles, counter, scratch;
+    int njobs = 0;
+    DevBuf jobs, tiles, counter, scratch, jobnext;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -129,12 +130,13 @@ struct atb_handle {
     int smem_optin = 0;
     int threads = 256;
     int ppt = 1;                       /* particles per thread (1 or 2)     */
+    int refill_k = 8;                  /* batch jobs: tiles per initial claim */
     int seg_cap_words = 6144;          /* 48 KB per buffer, two buffers    */
     int resident_max_words = 14336;    /* tables up to 112 KB stay resident */
     int64_t rout_budget = 4LL << 30;
     std::vector<Lattice> lats;
     DevBuf r, rout, lost, lturn, lelem, lcoord, refpts, jobs, tiles, counter, status, alive,
-        moments, tan_pelem, tan_porder, compact;
+        moments, tan_pelem, tan_porder, compact, jobnext;
     std::vector<int32_t> h_pelem;
     std::vector<AtbTile> h_tiles;
     std::vector<struct Batch> batches;
@@ -295,25 +297,35 @@ int launch(atb_handle* h, const std::vector<AtbJob>& jobs, const std::vector<Atb
     ATB_CUDA(cudaMemcpyAsync(h->tiles.p, tiles.data(), tiles.size() * sizeof(AtbTile),
                              cudaMemcpyHostToDevice, st));
     ATB_CUDA(cudaMemsetAsync(h->counter.p, 0, sizeof(int), st));
+    /* per-job particle cursors of the refilling tile loop */
+    if (h->jobnext.ensure(jobs.size() * sizeof(unsigned long long)) != cudaSuccess)
+        return fail(ATB_ERR_NOMEM, "cudaMalloc(job cursors) failed");
+    ATB_CUDA(cudaMemsetAsync(h->jobnext.p, 0, jobs.size() * sizeof(unsigned long long), st));
     int grid = std::min<int64_t>((int64_t)tiles.size(), grid_max);
     int cap = h->seg_cap_words;
-    /* survivor-compaction scratch: 7 doubles per thread of the grid */
-    if (h->compact.ensure((size_t)grid * threads * 7 * sizeof(double)) != cudaSuccess)
+    /* survivor-compaction scratch: ATB_COMPACT_WORDS doubles per thread of the grid */
+    if (h->compact.ensure((size_t)grid * threads * ATB_COMPACT_WORDS * sizeof(double)) !=
+        cudaSuccess)
         return fail(ATB_ERR_NOMEM, "cudaMalloc(compaction scratch) failed");
     const AtbJob* dj = h->jobs.as<AtbJob>();
     const AtbTile* dt = h->tiles.as<AtbTile>();
     const int nt = (int)tiles.size();
     int* cnt = h->counter.as<int>();
+    unsigned long long* jn = h->jobnext.as<unsigned long long>();
     int* sts = h->status.as<int>();
     double* scr = h->compact.as<double>();
     if (mode == ATB_MODE_EXACT && ppt == 2)
-        atb_track_kernel_exact_np2<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, sts, cap, scr);
+        atb_track_kernel_exact_np2<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, jn, sts,
+                                                                      cap, scr);
     else if (mode == ATB_MODE_EXACT)
-        atb_track_kernel_exact<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, sts, cap, scr);
+        atb_track_kernel_exact<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, jn, sts, cap,
+                                                                  scr);
     else if (ppt == 2)
-        atb_track_kernel_fast_np2<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, sts, cap, scr);
+        atb_track_kernel_fast_np2<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, jn, sts,
+                                                                     cap, scr);
     else
-        atb_track_kernel_fast<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, sts, cap, scr);
+        atb_track_kernel_fast<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, jn, sts, cap,
+                                                                 scr);
     ATB_CUDA(cudaGetLastError());
     return ATB_OK;
 }
@@ -341,6 +353,38 @@ void make_tiles(std::vector<AtbTile>& tiles, int job, int64_t np, int threads) {
         t.first = f;
         t.count = (int32_t)std::min<int64_t>(threads, np - f);
         tiles.push_back(t);
+    }
+}
+
+/* The claims of a multi-job launch.  A job whose lanes refill (one particle
+   per thread) gets one claim per refill_k tiles: each claim starts a block on
+   a tile's worth of the job's particles and the block takes the rest of the
+   job through its freed lanes, so blocks stay full while particles are lost;
+   other jobs get one claim per tile.  The factor is halved until the launch
+   has at least two claims per resident block. */
+void make_claims(const atb_handle* h, std::vector<AtbTile>& tiles,
+                 const std::vector<AtbJob>& J, const std::vector<int>& order, int grid_max) {
+    const int size = h->threads * h->ppt;
+    int k = h->ppt == 1 ? std::max(1, h->refill_k) : 1;
+    for (;; k /= 2) {
+        tiles.clear();
+        for (int j : order) {
+            if (J[j].nturns <= 0) continue;
+            if (k > 1 && atb_job_refills(&J[j])) {
+                const int64_t n = std::max<int64_t>(1, (J[j].np + (int64_t)size * k - 1) /
+                                                           ((int64_t)size * k));
+                for (int64_t i = 0; i < n; ++i) {
+                    AtbTile t;
+                    t.job = j;
+                    t.first = 0;   /* refilling jobs take particles from their cursor */
+                    t.count = (int32_t)std::min<int64_t>(size, J[j].np);
+                    if (t.count > 0) tiles.push_back(t);
+                }
+            } else {
+                make_tiles(tiles, j, J[j].np, size);
+            }
+        }
+        if (k <= 1 || (int64_t)tiles.size() >= 2LL * grid_max) break;
     }
 }
 
@@ -452,14 +496,25 @@ int atb_destroy(atb_handle* h) {
             B.tiles.release();
             B.counter.release();
             B.scratch.release();
+            B.jobnext.release();
         }
         for (DevBuf* b : {&h->r, &h->rout, &h->lost, &h->lturn, &h->lelem, &h->lcoord,
                           &h->refpts, &h->jobs, &h->tiles, &h->counter, &h->status, &h->alive,
-                          &h->moments, &h->tan_pelem, &h->tan_porder, &h->compact})
+                          &h->moments, &h->tan_pelem, &h->tan_porder, &h->compact,
+                          &h->jobnext})
             b->release();
         if (h->stream) cudaStreamDestroy(h->stream);
     }
     delete h;
+    return ATB_OK;
+}
+
+int atb_set_refill_factor(atb_handle* h, int32_t k) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    if (k < 1 || k > 64) return fail(ATB_ERR_ARG, "refill factor must be in [1, 64]");
+    for (const Batch& B : h->batches)
+        if (B.used) return fail(ATB_ERR_ARG, "free the prepared batches before changing the launch shape");
+    h->refill_k = k;
     return ATB_OK;
 }
 
@@ -896,9 +951,7 @@ int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int3
         double cb = (double)J[b].nturns * (lats[b]->nwords + 1);
         return ca > cb;
     });
-    h->h_tiles.clear();
-    for (int j : order)
-        if (J[j].nturns > 0) make_tiles(h->h_tiles, j, J[j].np, h->threads * h->ppt);
+    make_claims(h, h->h_tiles, J, order, grid_max);
     return launch(h, J, h->h_tiles, smem, grid_max, mode, st, h->threads, h->ppt);
 }
 
@@ -944,8 +997,7 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
                (double)J[b].nturns * (lats[b]->nwords + 1) * 1.0;
     });
     std::vector<AtbTile> tiles;
-    for (int j : order)
-        if (J[j].nturns > 0) make_tiles(tiles, j, J[j].np, h->threads * h->ppt);
+    make_claims(h, tiles, J, order, grid_max);
     int id = -1;
     for (int i = 0; i < (int)h->batches.size(); ++i)
         if (!h->batches[i].used) { id = i; break; }
@@ -956,7 +1008,9 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
     Batch& B = h->batches[id];
     if (B.jobs.ensure(std::max<size_t>(1, J.size()) * sizeof(AtbJob)) != cudaSuccess ||
         B.tiles.ensure(std::max<size_t>(1, tiles.size()) * sizeof(AtbTile)) != cudaSuccess ||
-        B.counter.ensure(sizeof(int)) != cudaSuccess)
+        B.counter.ensure(sizeof(int)) != cudaSuccess ||
+        B.jobnext.ensure(std::max<size_t>(1, J.size()) * sizeof(unsigned long long)) !=
+            cudaSuccess)
         return fail(ATB_ERR_NOMEM, "cudaMalloc(batch lists) failed");
     if (!J.empty())
         ATB_CUDA(cudaMemcpy(B.jobs.p, J.data(), J.size() * sizeof(AtbJob), cudaMemcpyHostToDevice));
@@ -970,8 +1024,10 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
     B.seg_cap = h->seg_cap_words;
     B.smem = smem;
     B.ntiles = (int)tiles.size();
+    B.njobs = (int)J.size();
     B.grid = std::min<int64_t>((int64_t)tiles.size(), std::max(grid_max, 1));
-    if (B.scratch.ensure((size_t)B.grid * B.threads * 7 * sizeof(double)) != cudaSuccess) {
+    if (B.scratch.ensure((size_t)B.grid * B.threads * ATB_COMPACT_WORDS * sizeof(double)) !=
+        cudaSuccess) {
         B.used = false;
         return fail(ATB_ERR_NOMEM, "cudaMalloc(compaction scratch) failed");
     }
@@ -987,22 +1043,24 @@ static Batch* get_batch(atb_handle* h, int id) {
 static int batch_enqueue(atb_handle* h, Batch& B, cudaStream_t st) {
     ATB_CUDA(cudaMemsetAsync(B.counter.p, 0, sizeof(int), st));
     if (B.ntiles == 0) return ATB_OK;
+    ATB_CUDA(cudaMemsetAsync(B.jobnext.p, 0, (size_t)B.njobs * sizeof(unsigned long long), st));
     const AtbJob* dj = B.jobs.as<AtbJob>();
     const AtbTile* dt = B.tiles.as<AtbTile>();
     int* cnt = B.counter.as<int>();
+    unsigned long long* jn = B.jobnext.as<unsigned long long>();
     int* sts = h->status.as<int>();
     double* scr = B.scratch.as<double>();
     if (B.mode == ATB_MODE_EXACT && B.ppt == 2)
-        atb_track_kernel_exact_np2<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, sts,
-                                                                      B.seg_cap, scr);
+        atb_track_kernel_exact_np2<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, jn,
+                                                                      sts, B.seg_cap, scr);
     else if (B.mode == ATB_MODE_EXACT)
-        atb_track_kernel_exact<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, sts,
+        atb_track_kernel_exact<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, jn, sts,
                                                                   B.seg_cap, scr);
     else if (B.ppt == 2)
-        atb_track_kernel_fast_np2<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, sts,
-                                                                     B.seg_cap, scr);
+        atb_track_kernel_fast_np2<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, jn,
+                                                                     sts, B.seg_cap, scr);
     else
-        atb_track_kernel_fast<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, sts,
+        atb_track_kernel_fast<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, jn, sts,
                                                                  B.seg_cap, scr);
     ATB_CUDA(cudaGetLastError());
     return ATB_OK;
@@ -1062,6 +1120,7 @@ int atb_batch_free(atb_handle* h, int32_t batch_id) {
     B->tiles.release();
     B->counter.release();
     B->scratch.release();
+    B->jobnext.release();
     B->used = false;
     return ATB_OK;
 }

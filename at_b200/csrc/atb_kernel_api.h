@@ -13,6 +13,9 @@
 #include <stdint.h>
 
 #define ATB_MAX_THREADS 512
+/* doubles per thread in the survivor-compaction scratch area: the six
+   coordinates, the particle index and the turn at which it joined */
+#define ATB_COMPACT_WORDS 8
 /* bounded mbarrier wait: 1 s, then the kernel reports and returns */
 #define ATB_WAIT_NS 1000000000ULL
 #define ATB_STATUS_WAIT_TIMEOUT 1
@@ -55,6 +58,21 @@ typedef struct AtbJob {
     double* moments;            /* optional: 12 sums per turn              */
     uint64_t rng_key;           /* key of the quantum-diffusion kicks      */
 } AtbJob;
+
+/* Whether a job's particles may be handed out through a per-job cursor with
+ * lanes refilled at turn boundaries (the tracking kernel's refill, used with
+ * one particle per thread when the launch provides compaction scratch and
+ * job cursors): whole turns, no refpts snapshots, no per-turn statistics,
+ * loss checks on, at least one table segment per turn.  Shared by the kernel
+ * and the host, which may then issue fewer claims than tiles for the job. */
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+static inline int atb_job_refills(const AtbJob* J) {
+    return J->nref == 0 && J->alive == 0 && J->check_loss && J->start_elem == 0 &&
+           J->end_elem == J->nelem && J->nturns > 0 && J->nturns < (1 << 30) &&
+           J->nseg_turn > 0 && J->nseg_first == J->nseg_turn;
+}
 
 typedef struct AtbTile {
     int32_t job;

@@ -27,10 +27,10 @@
 #include "atb_kernel_api.h"
 #include "atb_table.h"
 
-extern "C" __global__ void atb_track_kernel_exact(const AtbJob*, const AtbTile*, int, int*, int*,
-                                                  int, double*);
-extern "C" __global__ void atb_track_kernel_fast(const AtbJob*, const AtbTile*, int, int*, int*,
-                                                 int, double*);
+extern "C" __global__ void atb_track_kernel_exact(const AtbJob*, const AtbTile*, int, int*,
+                                                  unsigned long long*, int*, int, double*);
+extern "C" __global__ void atb_track_kernel_fast(const AtbJob*, const AtbTile*, int, int*,
+                                                 unsigned long long*, int*, int, double*);
 extern "C" const char* atb_last_error(void);
 void atb_set_error_message(const char* msg);
 
@@ -220,10 +220,12 @@ extern "C" int atb_track_noalloc(int32_t device, const double* table, int64_t nw
     int* counter = reinterpret_cast<int*>(base + NA_COUNTER);
     int* status = reinterpret_cast<int*>(base + NA_STATUS);
     if (mode == ATB_MODE_EXACT)
-        atb_track_kernel_exact<<<grid, NA_THREADS, smem, st>>>(dj, tiles, ntiles, counter, status,
+        atb_track_kernel_exact<<<grid, NA_THREADS, smem, st>>>(dj, tiles, ntiles, counter,
+                                                               nullptr, status,
                                                                NA_SEG_CAP_WORDS, nullptr);
     else
-        atb_track_kernel_fast<<<grid, NA_THREADS, smem, st>>>(dj, tiles, ntiles, counter, status,
+        atb_track_kernel_fast<<<grid, NA_THREADS, smem, st>>>(dj, tiles, ntiles, counter,
+                                                              nullptr, status,
                                                               NA_SEG_CAP_WORDS, nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return na_fail(ATB_ERR_CUDA, cudaGetErrorString(e));

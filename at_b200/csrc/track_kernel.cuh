@@ -597,16 +597,29 @@ __device__ __forceinline__ void apply_loss_rule(const AtbJob& J, P6& r, bool& lo
 /* The persistent tile loop.  NP particles per thread: particle k of thread t
  * in a tile is tile.first + k * blockDim + t, so every k stays coalesced; the
  * element parameters read from shared memory serve all NP particles, whose
- * dependency chains interleave. */
+ * dependency chains interleave.
+ *
+ * Refill (NP = 1, a compaction scratch area and a job cursor given): a job
+ * tracked over whole turns with no refpts snapshots and no per-turn
+ * statistics hands out its particles through job_next[job] instead of fixed
+ * tile ranges.  At the end of every turn a block retires the particles that
+ * were lost or finished their turns (final state and loss flag stored), moves
+ * the survivors to its lowest threads when that frees a warp, and takes
+ * not-yet-started particles of the same job into its free lanes; each lane
+ * counts its own turns (RF phase, loss turn and random kicks use the
+ * particle's turn).  Blocks so stay full while their job has particles left
+ * instead of running a few survivors for all remaining turns. */
 template <int NP>
 __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                                             const AtbTile* __restrict__ tiles, int ntiles,
                                             int* __restrict__ tile_counter,
+                                            unsigned long long* __restrict__ job_next,
                                             int* __restrict__ status, int smem_cap_words,
                                             double* __restrict__ scratch) {
     extern __shared__ __align__(128) double smem[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_tile;
+    __shared__ unsigned long long s_first;
     __shared__ int s_warp[ATB_MAX_THREADS / 32];
     double* buf0 = smem;
     double* buf1 = smem + smem_cap_words;
@@ -631,17 +644,32 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
         if (t >= ntiles) break;
         const AtbTile tile = tiles[t];
         const AtbJob& J = jobs[tile.job];
+        const bool refill =
+            NP == 1 && scratch != nullptr && job_next != nullptr && atb_job_refills(&J);
+        long long first = tile.first;
+        int count = tile.count;
+        if (refill) {
+            if (tid == 0) s_first = atomicAdd(&job_next[tile.job], (unsigned long long)count);
+            __syncthreads();
+            first = (long long)s_first;
+            const long long left = J.np - first;
+            if (left < count) count = left > 0 ? (int)left : 0;
+            if (count == 0) continue;   /* the job's particles are all taken */
+        }
         long long p[NP];
         bool active[NP];
-        int nact = tile.count;            /* particles held by the block (uniform) */
+        int lt0[NP];                    /* turn of the block at which the lane's particle joined */
+        int tt_end = J.nturns;          /* the block tracks until this turn */
+        bool exhausted = false;         /* the job cursor has no particle left */
         const bool resident = (J.resident != 0);
 
         P6 r[NP];
         bool lost[NP];
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
-            p[k] = tile.first + (long long)k * nthr + tid;
-            active[k] = (k * nthr + tid) < tile.count;
+            p[k] = first + (long long)k * nthr + tid;
+            active[k] = (k * nthr + tid) < count;
+            lt0[k] = 0;
             lost[k] = false;
             if (active[k]) {
                 load6(J.r + 6 * p[k], r[k]);
@@ -653,8 +681,12 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
         }
 
         /* staging pipeline state for this tile */
+        /* segments the tile visits; a refilling block runs until its lanes
+           are empty and leaves through the drain below */
         const long long nq = (J.nturns <= 0) ? 0
-                             : (long long)J.nseg_first + (long long)(J.nturns - 1) * J.nseg_turn;
+                             : refill ? (1LL << 60)
+                                      : (long long)J.nseg_first +
+                                            (long long)(J.nturns - 1) * J.nseg_turn;
         bool timed_out = false;
         if (resident) {
             if (resident_job != tile.job) {
@@ -686,8 +718,10 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
 
         long long slot = J.rout_slot0;
         long long q = 0;
-        for (int tt = 0; tt < J.nturns && !timed_out; ++tt) {
-            const int nturn = J.turn0 + tt;
+        for (int tt = 0; tt < tt_end && !timed_out; ++tt) {
+            int nturn[NP];
+#pragma unroll
+            for (int k = 0; k < NP; ++k) nturn[k] = J.turn0 + tt - lt0[k];
             const int estart = (tt == 0) ? J.start_elem : 0;
             const int eend = J.end_elem;
             int nri = 0;
@@ -733,11 +767,13 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                     } else {
 #pragma unroll
                         for (int k = 0; k < NP; ++k)
-                            track_element(r[k], e, nturn, Param{-1, 0.0}, &J.rng_key, p[k], ei);
+                            track_element(r[k], e, nturn[k], Param{-1, 0.0}, &J.rng_key, p[k],
+                                          ei);
                     }
 #pragma unroll
                     for (int k = 0; k < NP; ++k)
-                        if (J.check_loss) apply_loss_rule(J, r[k], lost[k], active[k], p[k], nturn, ei);
+                        if (J.check_loss)
+                            apply_loss_rule(J, r[k], lost[k], active[k], p[k], nturn[k], ei);
                     w += e.len();
                 }
                 if (!resident) {
@@ -791,17 +827,35 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
             }
             /* a tile whose particles are all lost stops early (nothing it
                would still compute is observable without refpts snapshots) */
-            if (J.nref == 0 && tt + 1 < J.nturns) {
+            if (refill || (J.nref == 0 && tt + 1 < tt_end)) {
+                if constexpr (NP == 1) {
+                    if (refill && active[0]) {
+                        /* retire a particle that is lost or has done its turns */
+                        const bool done = tt + 1 - lt0[0] == J.nturns;
+                        if (done || isnan(r[0].x) || (J.losses && lost[0])) {
+                            store6(J.r + 6 * p[0], r[0]);
+                            if (J.losses) J.lost[p[0]] = lost[0] ? 1 : 0;
+                            active[0] = false;
+                            r[0].x = nan_d(); r[0].px = 0.0; r[0].y = 0.0;
+                            r[0].py = 0.0; r[0].dp = 0.0; r[0].ct = 0.0;
+                            lost[0] = true;
+                        }
+                    }
+                }
                 bool any_live = false;
 #pragma unroll
                 for (int k = 0; k < NP; ++k)
                     any_live |= active[k] && !isnan(r[k].x) && !(J.losses && lost[k]);
-                const int nlive = __syncthreads_count(any_live);
+                int nlive = __syncthreads_count(any_live);
                 if constexpr (NP == 1) {
                     const bool live = any_live;
-                    if (scratch && nlive > 0 && 2 * nlive <= nact && nact > 32) {
-                        /* Half or more of the particles held are lost: move
-                           the survivors to the lowest threads, so that whole
+                    const unsigned ball = __ballot_sync(0xffffffffu, live);
+                    const int lane = tid & 31, warp = tid >> 5;
+                    /* warps that still hold a live particle */
+                    const int held = __syncthreads_count(lane == 0 && ball != 0u);
+                    if (scratch && nlive > 0 && (nlive + 31) / 32 < held) {
+                        /* The survivors fit in fewer warps than hold them:
+                           move them to the lowest threads, so that whole
                            warps fall idle instead of running with masked
                            lanes.  The lost ones are retired first (their
                            final state and loss flag are what the end of the
@@ -810,13 +864,11 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                             store6(J.r + 6 * p[0], r[0]);
                             if (J.losses) J.lost[p[0]] = lost[0] ? 1 : 0;
                         }
-                        const unsigned ball = __ballot_sync(0xffffffffu, live);
-                        const int lane = tid & 31, warp = tid >> 5;
                         if (lane == 0) s_warp[warp] = __popc(ball);
                         __syncthreads();
                         int dest = __popc(ball & ((1u << lane) - 1u));
                         for (int wv = 0; wv < warp; ++wv) dest += s_warp[wv];
-                        double* sb = scratch + (size_t)blockIdx.x * 7 * nthr;
+                        double* sb = scratch + (size_t)blockIdx.x * ATB_COMPACT_WORDS * nthr;
                         if (live) {
                             sb[dest] = r[0].x;
                             sb[nthr + dest] = r[0].px;
@@ -825,6 +877,7 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                             sb[4 * nthr + dest] = r[0].dp;
                             sb[5 * nthr + dest] = r[0].ct;
                             sb[6 * nthr + dest] = __longlong_as_double(p[0]);
+                            sb[7 * nthr + dest] = __longlong_as_double(lt0[0]);
                         }
                         __syncthreads();
                         active[0] = tid < nlive;
@@ -836,14 +889,45 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                             r[0].dp = sb[4 * nthr + tid];
                             r[0].ct = sb[5 * nthr + tid];
                             p[0] = __double_as_longlong(sb[6 * nthr + tid]);
+                            lt0[0] = (int)__double_as_longlong(sb[7 * nthr + tid]);
                             lost[0] = false;
                         } else {
                             r[0].x = nan_d(); r[0].px = 0.0; r[0].y = 0.0;
                             r[0].py = 0.0; r[0].dp = 0.0; r[0].ct = 0.0;
                             lost[0] = true;
                         }
-                        nact = nlive;
                         __syncthreads();   /* scratch free for the next compaction */
+                    }
+                    if (refill && !exhausted) {
+                        /* free lanes take the job's next particles */
+                        const bool fr = !active[0];
+                        const unsigned fb = __ballot_sync(0xffffffffu, fr);
+                        if (lane == 0) s_warp[warp] = __popc(fb);
+                        const int nfree = __syncthreads_count(fr);
+                        if (nfree > 0) {
+                            if (tid == 0)
+                                s_first = atomicAdd(&job_next[tile.job],
+                                                    (unsigned long long)nfree);
+                            __syncthreads();
+                            const long long c = (long long)s_first;
+                            long long take = J.np - c;
+                            if (take > nfree) take = nfree;
+                            if (take < nfree) exhausted = true;
+                            if (take > 0) {
+                                int rank = __popc(fb & ((1u << lane) - 1u));
+                                for (int wv = 0; wv < warp; ++wv) rank += s_warp[wv];
+                                if (fr && rank < take) {
+                                    p[0] = c + rank;
+                                    active[0] = true;
+                                    lt0[0] = tt + 1;
+                                    load6(J.r + 6 * p[0], r[0]);
+                                    lost[0] = J.losses ? J.lost[p[0]] != 0 : false;
+                                }
+                                nlive += (int)take;
+                                if (tt + 1 + J.nturns > tt_end) tt_end = tt + 1 + J.nturns;
+                            }
+                            __syncthreads();   /* s_warp and s_first free again */
+                        }
                     }
                 }
                 if (nlive == 0) {
@@ -869,8 +953,9 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
         if (timed_out) {
             /* drain our own copies still in flight before leaving */
             if (!resident) {
+                const long long issued = (q + 2 < nq) ? q + 2 : nq;
                 for (int b = 0; b < 2; ++b) {
-                    if (use_count[b] < (uint32_t)((nq + 1 - b) / 2)) {
+                    if (use_count[b] < (uint32_t)((issued + 1 - b) / 2)) {
                         mbar_wait_bounded(&bars[b], use_count[b] & 1u);
                     }
                 }
@@ -895,9 +980,11 @@ extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
 ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
                                        const AtbTile* __restrict__ tiles, int ntiles,
                                        int* __restrict__ tile_counter,
+                                       unsigned long long* __restrict__ job_next,
                                        int* __restrict__ status, int smem_cap_words,
                                        double* __restrict__ scratch) {
-    track_tiles<1>(jobs, tiles, ntiles, tile_counter, status, smem_cap_words, scratch);
+    track_tiles<1>(jobs, tiles, ntiles, tile_counter, job_next, status, smem_cap_words,
+                   scratch);
 }
 
 /* two particles per thread (the autotuner's particles-per-thread choice) */
@@ -905,10 +992,12 @@ extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
 ATB_CAT(ATB_CAT(atb_track_kernel, ATB_KSUFFIX), _np2)(const AtbJob* __restrict__ jobs,
                                                       const AtbTile* __restrict__ tiles,
                                                       int ntiles, int* __restrict__ tile_counter,
+                                                      unsigned long long* __restrict__ job_next,
                                                       int* __restrict__ status,
                                                       int smem_cap_words,
                                                       double* __restrict__ scratch) {
-    track_tiles<2>(jobs, tiles, ntiles, tile_counter, status, smem_cap_words, scratch);
+    track_tiles<2>(jobs, tiles, ntiles, tile_counter, job_next, status, smem_cap_words,
+                   scratch);
 }
 
 #endif  // ATB_NO_TRACK_KERNEL

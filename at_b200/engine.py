@@ -72,11 +72,14 @@ class Engine:
 
     # -- launch tuning ------------------------------------------------------
     def set_launch(self, threads: int = 0, seg_cap_words: int = 0, resident_max_words: int = 0,
-                   rout_budget_bytes: int = 0, particles_per_thread: int = 0):
+                   rout_budget_bytes: int = 0, particles_per_thread: int = 0,
+                   refill_factor: int = 0):
         check(lib().atb_set_launch(self.h, int(threads), int(seg_cap_words),
                                    int(resident_max_words), int(rout_budget_bytes)))
         if particles_per_thread:
             check(lib().atb_set_particles_per_thread(self.h, int(particles_per_thread)))
+        if refill_factor:
+            check(lib().atb_set_refill_factor(self.h, int(refill_factor)))
 
     # -- lattices -----------------------------------------------------------
     def upload(self, cl: CompiledLattice) -> int:

@@ -79,6 +79,16 @@ int atb_device_info(int device, char* name, int name_len, int* cc_major, int* cc
 int atb_create(int device, atb_handle** out);
 int atb_destroy(atb_handle* h);
 
+/* Refill factor of multi-job launches (atb_track_batch, atb_batch_prepare),
+ * 1..64, default 8: a job tracked over whole turns without refpts snapshots
+ * or per-turn statistics starts on one block per k tiles' worth of its
+ * particles, and each block takes the job's remaining particles into the
+ * lanes that lost or finished particles free at turn boundaries (halved
+ * until the launch has two claims per resident block).  Results do not
+ * depend on it.  Refused while prepared batches exist.  No reference
+ * counterpart (launch tuning). */
+int atb_set_refill_factor(atb_handle* h, int32_t k);
+
 /* Particles per thread of the tracking kernel (1 or 2): with 2, each thread
  * carries two particles through every element, reusing the element's
  * parameters and interleaving two dependency chains; the autotuner picks it.

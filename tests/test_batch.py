@@ -95,3 +95,45 @@ def test_batched_variants_equal_individual_runs(tmp_path, monkeypatch):
             np.testing.assert_array_equal(ld[k], lr[k])
     assert any(ld["islost"].any() for _, ld in res1)       # +/-3 % particles get lost
     assert (tmp_path / "tune.json").exists()
+
+
+@pytest.mark.gpu
+def test_refill_claims_give_the_same_results(tmp_path, monkeypatch):
+    """Jobs large enough that the launch starts on one block per several
+    tiles (refill factor 8, halved to keep two claims per resident block):
+    blocks take the rest of each job into the lanes that lost particles free
+    at turn boundaries.  Every particle's result and loss record equal the
+    run with one claim per tile and the plain drop-in call."""
+    monkeypatch.setenv("AT_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    from at_b200 import tracking
+    from at_b200.batch import BatchTracker
+    from at_b200.engine import Engine
+
+    lats = [rings.large_ring_variant(s) for s in (2, 3, 4, 5)]
+    parts = [rings.da_grid(160000, seed=s) for s in (2, 3, 4, 5)]
+    turns = [6, 4, 5, 3]
+    eng = Engine.get(0)
+    out = {}
+    try:
+        for k in (1, 8):
+            eng.set_launch(threads=256, seg_cap_words=3072, particles_per_thread=1,
+                           refill_factor=k)
+            bt = BatchTracker(lats, parts, turns, mode="fast", tune=False, graph=True)
+            try:
+                bt.run()
+                out[k] = bt.results()
+            finally:
+                bt.close()
+    finally:
+        eng.set_launch(threads=256, seg_cap_words=6144, particles_per_thread=1, refill_factor=8)
+    lost = 0
+    for (ra, la), (rb, lb) in zip(out[1], out[8]):
+        np.testing.assert_array_equal(ra, rb)
+        for key in ("islost", "turn", "elem", "coord"):
+            np.testing.assert_array_equal(la[key], lb[key])
+        lost += int(la["islost"].sum())
+    assert 0 < lost < sum(p.shape[1] for p in parts)
+    ref = parts[0].copy(order="F")
+    _, lr = tracking.gpupass(lats[0], ref, turns[0], losses=True, mode="fast")
+    np.testing.assert_array_equal(out[8][0][0], ref)
+    np.testing.assert_array_equal(out[8][0][1]["islost"], lr["islost"])

@@ -233,14 +233,15 @@ def test_find_orbit6_matches_constant():
     np.testing.assert_allclose(orb, rings.LARGE_ORBIT, rtol=0, atol=1e-12)
 
 
-@pytest.mark.parametrize("pattern", ["tiles", "alternate"])
+@pytest.mark.parametrize("pattern", ["tiles", "alternate", "sparse"])
 @pytest.mark.parametrize("ring_name", ["fodo", "large"])
 def test_all_lost_tiles_stop_early(ring_name, pattern):
     """Tiles whose particles are all lost leave the turn loop early (after
     draining their in-flight table copies when the table streams in
-    segments), and tiles that lost half their particles move the survivors
-    to the lowest threads; the results equal a run that does neither (with
-    a refpts snapshot) and the oracle's loss map."""
+    segments), and tiles whose survivors fit in fewer warps than hold them
+    move the survivors to the lowest threads (every other particle lost, or
+    one in six, which frees one warp of eight); the results equal a run that
+    does neither (with a refpts snapshot) and the oracle's loss map."""
     if ring_name == "fodo":
         ring, en, rest = rings.fodo_ring(), 3e9, ELECTRON_REST
         r0 = rings.gaussian(2048, seed=8)
@@ -252,9 +253,11 @@ def test_all_lost_tiles_stop_early(ring_name, pattern):
         nt = 6
     if pattern == "tiles":
         r0[:, 256:768] *= 1e3        # two whole tiles lost in the first turn
-    else:
+    elif pattern == "alternate":
         r0[:, 1::2] = 2.0            # every other particle lost at the first element
         r0[:, 600:700] = 2.0         # and a run of them
+    else:
+        r0[:, 5::6] = 2.0            # one particle in six lost at the first element
     ra = r0.copy(order="F")
     _, la, _ = _gpu_track(ring, ra, nt, en, rest, "exact", losses=True)
     rb = r0.copy(order="F")
@@ -263,8 +266,10 @@ def test_all_lost_tiles_stop_early(ring_name, pattern):
     np.testing.assert_array_equal(ra, rb)
     if pattern == "tiles":
         assert la["islost"][256:768].all() and not la["islost"].all()
-    else:
+    elif pattern == "alternate":
         assert la["islost"][1::2].all() and not la["islost"].all()
+    else:
+        assert la["islost"][5::6].all() and not la["islost"].all()
     ro = r0.copy(order="F")
     _, lo = oracle.track(ring, ro, nt, energy=en, rest_energy=rest, losses=True)
     np.testing.assert_array_equal(la["islost"], lo["islost"])
