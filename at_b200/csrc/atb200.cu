@@ -130,7 +130,7 @@ struct atb_handle {
     int smem_optin = 0;
     int threads = 256;
     int ppt = 1;                       /* particles per thread (1 or 2)     */
-    int refill_k = 8;                  /* batch jobs: tiles per initial claim */
+    int refill_k = 8;                  /* prepared batches: tiles per initial claim */
     int seg_cap_words = 6144;          /* 48 KB per buffer, two buffers    */
     int resident_max_words = 14336;    /* tables up to 112 KB stay resident */
     int64_t rout_budget = 4LL << 30;
@@ -356,16 +356,17 @@ void make_tiles(std::vector<AtbTile>& tiles, int job, int64_t np, int threads) {
     }
 }
 
-/* The claims of a multi-job launch.  A job whose lanes refill (one particle
-   per thread) gets one claim per refill_k tiles: each claim starts a block on
-   a tile's worth of the job's particles and the block takes the rest of the
-   job through its freed lanes, so blocks stay full while particles are lost;
-   other jobs get one claim per tile.  The factor is halved until the launch
-   has at least two claims per resident block. */
+/* The claims of a multi-job launch.  With factor k > 1 a job whose lanes
+   refill (one particle per thread) gets one claim per k tiles: each claim
+   starts a block on a tile's worth of the job's particles and the block takes
+   the rest of the job through its freed lanes, so blocks stay full while
+   particles are lost; other jobs get one claim per tile.  The factor is
+   halved until the launch has at least two claims per resident block. */
 void make_claims(const atb_handle* h, std::vector<AtbTile>& tiles,
-                 const std::vector<AtbJob>& J, const std::vector<int>& order, int grid_max) {
+                 const std::vector<AtbJob>& J, const std::vector<int>& order, int grid_max,
+                 int refill_k) {
     const int size = h->threads * h->ppt;
-    int k = h->ppt == 1 ? std::max(1, h->refill_k) : 1;
+    int k = h->ppt == 1 ? std::max(1, refill_k) : 1;
     for (;; k /= 2) {
         tiles.clear();
         for (int j : order) {
@@ -951,7 +952,7 @@ int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int3
         double cb = (double)J[b].nturns * (lats[b]->nwords + 1);
         return ca > cb;
     });
-    make_claims(h, h->h_tiles, J, order, grid_max);
+    make_claims(h, h->h_tiles, J, order, grid_max, 1);
     return launch(h, J, h->h_tiles, smem, grid_max, mode, st, h->threads, h->ppt);
 }
 
@@ -997,7 +998,7 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
                (double)J[b].nturns * (lats[b]->nwords + 1) * 1.0;
     });
     std::vector<AtbTile> tiles;
-    make_claims(h, tiles, J, order, grid_max);
+    make_claims(h, tiles, J, order, grid_max, h->refill_k);
     int id = -1;
     for (int i = 0; i < (int)h->batches.size(); ++i)
         if (!h->batches[i].used) { id = i; break; }

@@ -79,12 +79,14 @@ int atb_device_info(int device, char* name, int name_len, int* cc_major, int* cc
 int atb_create(int device, atb_handle** out);
 int atb_destroy(atb_handle* h);
 
-/* Refill factor of multi-job launches (atb_track_batch, atb_batch_prepare),
- * 1..64, default 8: a job tracked over whole turns without refpts snapshots
- * or per-turn statistics starts on one block per k tiles' worth of its
- * particles, and each block takes the job's remaining particles into the
- * lanes that lost or finished particles free at turn boundaries (halved
- * until the launch has two claims per resident block).  Results do not
+/* Refill factor of prepared batches (atb_batch_prepare), 1..64, default 8:
+ * a job tracked over whole turns without refpts snapshots or per-turn
+ * statistics starts on one block per k tiles' worth of its particles, and
+ * each block takes the job's remaining particles into the lanes that lost or
+ * finished particles free at turn boundaries (halved until the launch has
+ * two claims per resident block).  It pays where many particles are lost
+ * early (dynamic-aperture studies over lattice variants) and costs where
+ * they survive, so atb_track_batch keeps one claim per tile.  Results do not
  * depend on it.  Refused while prepared batches exist.  No reference
  * counterpart (launch tuning). */
 int atb_set_refill_factor(atb_handle* h, int32_t k);
