@@ -29,7 +29,7 @@ UNITS = [
     ("atb_noalloc.cu", []),
 ]
 DEPS = ["atb_physics.cuh", "atb_dual.cuh", "track_kernel.cuh", "tangent_kernel.cuh",
-        "atb_diffusion.cuh",
+        "atb_diffusion.cuh", "atb_integrators.h",
         "atb_kernel_api.h", "atb_table.h"]
 
 

@@ -36,14 +36,22 @@ extern "C" __global__ void atb_track_kernel_exact(const AtbJob*, const AtbTile*,
                                        unsigned long long*, int*, int, double*);
 extern "C" __global__ void atb_track_kernel_fast(const AtbJob*, const AtbTile*, int, int*,
                                        unsigned long long*, int*, int, double*);
+extern "C" __global__ void atb_track_kernel_exact_gen(const AtbJob*, const AtbTile*, int, int*,
+                                       unsigned long long*, int*, int, double*);
+extern "C" __global__ void atb_track_kernel_fast_gen(const AtbJob*, const AtbTile*, int, int*,
+                                       unsigned long long*, int*, int, double*);
 extern "C" __global__ void atb_track_kernel_exact_np2(const AtbJob*, const AtbTile*, int, int*,
                                        unsigned long long*, int*, int, double*);
 extern "C" __global__ void atb_track_kernel_fast_np2(const AtbJob*, const AtbTile*, int, int*,
                                        unsigned long long*, int*, int, double*);
 
 /* the tracking kernel for an arithmetic mode and a number of particles per
-   thread (1 or 2) */
-static const void* track_fn(int mode, int ppt) {
+   thread (1 or 2); gen: the kernels with the other integrators of the GPU
+   call (one particle per thread) */
+static const void* track_fn(int mode, int ppt, bool gen = false) {
+    if (gen)
+        return mode == ATB_MODE_EXACT ? (const void*)atb_track_kernel_exact_gen
+                                      : (const void*)atb_track_kernel_fast_gen;
     if (mode == ATB_MODE_EXACT)
         return ppt == 2 ? (const void*)atb_track_kernel_exact_np2
                         : (const void*)atb_track_kernel_exact;
@@ -98,6 +106,7 @@ struct Batch {
     int mode = 1;
     int threads = 256;      /* launch shape fixed when the batch is prepared */
     int ppt = 1;            /* particles per thread                             */
+    bool gen = false;       /* the kernels with the other integrators           */
     int seg_cap = 6144;
     int smem = 0;
     int grid = 0;
@@ -116,6 +125,7 @@ struct Lattice {
     std::vector<uint64_t> hdr;  /* every element's header word              */
     std::vector<AtbSeg> segs;   /* pipelined segments (empty when resident) */
     bool resident = false;
+    bool integ = false;         /* some element needs another integrator    */
     int plan_cap = 0;           /* seg capacity used to build the plan      */
     DevBuf words, doff, dsegs;
 };
@@ -265,10 +275,12 @@ void fill_job_lattice(AtbJob& J, const Lattice& L, int start_elem, int end_elem)
 }
 
 int kernel_config(atb_handle* h, const std::vector<const Lattice*>& lats, int mode,
-                  int* smem_bytes, int* grid_max) {
+                  int* smem_bytes, int* grid_max, bool* gen) {
     bool any_pipe = false;
     int64_t res_words = 0;
+    *gen = false;
     for (const Lattice* L : lats) {
+        if (L->integ) *gen = true;
         if (L->resident) res_words = std::max<int64_t>(res_words, L->nwords + (L->nwords & 1));
         else if (!L->segs.empty()) any_pipe = true;
     }
@@ -278,7 +290,7 @@ int kernel_config(atb_handle* h, const std::vector<const Lattice*>& lats, int mo
     if (bytes > h->smem_optin)
         return fail(ATB_ERR_ARG, "shared-memory plan exceeds the per-block limit");
     *smem_bytes = bytes;
-    const void* fn = track_fn(mode, h->ppt);
+    const void* fn = track_fn(mode, *gen ? 1 : h->ppt, *gen);
     int per_sm = 0;
     ATB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, h->threads, bytes));
     if (per_sm < 1) return fail(ATB_ERR_ARG, "launch configuration does not fit on an SM");
@@ -287,7 +299,8 @@ int kernel_config(atb_handle* h, const std::vector<const Lattice*>& lats, int mo
 }
 
 int launch(atb_handle* h, const std::vector<AtbJob>& jobs, const std::vector<AtbTile>& tiles,
-           int smem_bytes, int grid_max, int mode, cudaStream_t st, int threads, int ppt) {
+           int smem_bytes, int grid_max, int mode, cudaStream_t st, int threads, int ppt,
+           bool gen) {
     if (tiles.empty()) return ATB_OK;
     if (h->jobs.ensure(jobs.size() * sizeof(AtbJob)) != cudaSuccess ||
         h->tiles.ensure(tiles.size() * sizeof(AtbTile)) != cudaSuccess)
@@ -314,7 +327,13 @@ int launch(atb_handle* h, const std::vector<AtbJob>& jobs, const std::vector<Atb
     unsigned long long* jn = h->jobnext.as<unsigned long long>();
     int* sts = h->status.as<int>();
     double* scr = h->compact.as<double>();
-    if (mode == ATB_MODE_EXACT && ppt == 2)
+    if (gen && mode == ATB_MODE_EXACT)
+        atb_track_kernel_exact_gen<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, jn, sts,
+                                                                      cap, scr);
+    else if (gen)
+        atb_track_kernel_fast_gen<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, jn, sts,
+                                                                     cap, scr);
+    else if (mode == ATB_MODE_EXACT && ppt == 2)
         atb_track_kernel_exact_np2<<<grid, threads, smem_bytes, st>>>(dj, dt, nt, cnt, jn, sts,
                                                                       cap, scr);
     else if (mode == ATB_MODE_EXACT)
@@ -364,9 +383,9 @@ void make_tiles(std::vector<AtbTile>& tiles, int job, int64_t np, int threads) {
    halved until the launch has at least two claims per resident block. */
 void make_claims(const atb_handle* h, std::vector<AtbTile>& tiles,
                  const std::vector<AtbJob>& J, const std::vector<int>& order, int grid_max,
-                 int refill_k) {
-    const int size = h->threads * h->ppt;
-    int k = h->ppt == 1 ? std::max(1, refill_k) : 1;
+                 int refill_k, int ppt) {
+    const int size = h->threads * ppt;
+    int k = ppt == 1 ? std::max(1, refill_k) : 1;
     for (;; k /= 2) {
         tiles.clear();
         for (int j : order) {
@@ -402,6 +421,12 @@ int check_status(atb_handle* h, cudaStream_t st) {
         cudaMemsetAsync(h->status.p, 0, sizeof(int), st);
         cudaStreamSynchronize(st);
         return fail(ATB_ERR_TIMEOUT, "a bounded shared-memory staging wait timed out");
+    }
+    if (s & ATB_STATUS_INTEGRATOR) {
+        cudaMemsetAsync(h->status.p, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
+        return fail(ATB_ERR_ARG, "an element compiled for another integrator reached a kernel "
+                                 "built without them");
     }
     return ATB_OK;
 }
@@ -469,6 +494,10 @@ int atb_create(int device, atb_handle** out) {
     ATB_CUDA(cudaFuncSetAttribute(atb_track_kernel_fast,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
     ATB_CUDA(cudaFuncSetAttribute(atb_track_kernel_exact_np2,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
+    ATB_CUDA(cudaFuncSetAttribute(atb_track_kernel_exact_gen,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
+    ATB_CUDA(cudaFuncSetAttribute(atb_track_kernel_fast_gen,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
     ATB_CUDA(cudaFuncSetAttribute(atb_track_kernel_fast_np2,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
@@ -598,6 +627,9 @@ int atb_lattice_upload(atb_handle* h, const double* words, int64_t nwords,
     if (nelem == 0) L.off.assign(1, 0u);
     L.hdr.resize(nelem);
     for (int i = 0; i < nelem; ++i) std::memcpy(&L.hdr[i], words + elem_off[i], 8);
+    L.integ = false;
+    for (int i = 0; i < nelem; ++i)
+        if ((L.hdr[i] >> ATB_H_FL_SHIFT) & ATB_F_INTEG) L.integ = true;
     size_t wbytes = (size_t)(nwords + 2) * 8;
     if (L.words.ensure(wbytes) != cudaSuccess || L.doff.ensure(L.off.size() * 4) != cudaSuccess) {
         L.used = false;
@@ -624,6 +656,9 @@ int atb_lattice_update(atb_handle* h, int32_t id, const double* words, int64_t n
     ATB_CUDA(cudaStreamSynchronize(h->stream));
     if (nwords) ATB_CUDA(cudaMemcpy(L->words.p, words, nwords * 8, cudaMemcpyHostToDevice));
     for (int i = 0; i < L->nelem; ++i) std::memcpy(&L->hdr[i], words + L->off[i], 8);
+    L->integ = false;
+    for (int i = 0; i < L->nelem; ++i)
+        if ((L->hdr[i] >> ATB_H_FL_SHIFT) & ATB_F_INTEG) L->integ = true;
     return ATB_OK;
 }
 
@@ -712,7 +747,8 @@ int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns
 
     std::vector<const Lattice*> lats{L};
     int smem = 0, grid_max = 0;
-    int rc = kernel_config(h, lats, mode, &smem, &grid_max);
+    bool gen = false;
+    int rc = kernel_config(h, lats, mode, &smem, &grid_max, &gen);
     if (rc) return rc;
 
     int64_t slot_done = 0;
@@ -740,10 +776,10 @@ int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns
         J.moments = (alive || moments) ? h->moments.as<double>() + 12 * t0 : nullptr;
         std::vector<AtbJob> jobs{J};
         h->h_tiles.clear();
-        const int pp = ppt_for(h, np);
+        const int pp = gen ? 1 : ppt_for(h, np);
         const int thr = pp > 1 ? h->threads : threads_for(h, np);
         make_tiles(h->h_tiles, 0, np, thr * pp);
-        rc = launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr, pp);
+        rc = launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr, pp, gen);
         if (rc) return rc;
         if (nref) {
             int64_t slots = (t0 == 0 ? rec_first : rec_turn) + (int64_t)(nt - 1) * rec_turn;
@@ -786,7 +822,8 @@ int atb_track_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t n
     cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
     std::vector<const Lattice*> lats{L};
     int smem = 0, grid_max = 0;
-    int rc = kernel_config(h, lats, mode, &smem, &grid_max);
+    bool gen = false;
+    int rc = kernel_config(h, lats, mode, &smem, &grid_max, &gen);
     if (rc) return rc;
     AtbJob J;
     std::memset(&J, 0, sizeof(J));
@@ -806,12 +843,12 @@ int atb_track_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t n
     J.moments = moments;
     std::vector<AtbJob> jobs{J};
     h->h_tiles.clear();
-    const int pp = ppt_for(h, np);
+    const int pp = gen ? 1 : ppt_for(h, np);
     const int thr = pp > 1 ? h->threads : threads_for(h, np);
     make_tiles(h->h_tiles, 0, np, thr * pp);
     /* pageable-source copies of the launch lists are staged before
        cudaMemcpyAsync returns, so the host vectors may be reused at once */
-    return launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr, pp);
+    return launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr, pp, gen);
 }
 
 int atb_element_maps(atb_handle* h, int32_t id, const double* orbits, double* m66,
@@ -821,6 +858,10 @@ int atb_element_maps(atb_handle* h, int32_t id, const double* orbits, double* m6
     if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
     if (L->nelem == 0) return ATB_OK;
     if (!orbits || !m66 || !b66) return fail(ATB_ERR_ARG, "NULL buffer");
+    for (int e = 0; e < L->nelem; ++e)
+        if ((L->hdr[e] >> ATB_H_FL_SHIFT) & ATB_F_INTEG)
+            return fail(ATB_ERR_ARG, "element maps need a lattice compiled for the default "
+                                     "integrator (4)");
     DeviceGuard g(h->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
     AtbElemMaps A;
@@ -849,6 +890,11 @@ int atb_tangent_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t
     if (np > 0 && (!r || !jac)) return fail(ATB_ERR_ARG, "r or jac is NULL");
     if (nparam > 0 && (!param_elem || !param_order || !param_value || (np > 0 && !grad)))
         return fail(ATB_ERR_ARG, "parameter arrays missing");
+    /* the tangent kernel integrates with the CPU engine's Forest-Ruth steps */
+    for (int e = 0; e < L->nelem; ++e)
+        if ((L->hdr[e] >> ATB_H_FL_SHIFT) & ATB_F_INTEG)
+            return fail(ATB_ERR_ARG, "the tangent kernel needs a lattice compiled for the "
+                                     "default integrator (4)");
     /* validate the differentiated strengths against the element headers */
     h->h_pelem.assign((size_t)std::max(L->nelem, 1), -1);
     for (int q = 0; q < nparam; ++q) {
@@ -942,7 +988,8 @@ int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int3
         J[j].lcoord = d.lcoord;
     }
     int smem = 0, grid_max = 0;
-    int rc = kernel_config(h, lats, mode, &smem, &grid_max);
+    bool gen = false;
+    int rc = kernel_config(h, lats, mode, &smem, &grid_max, &gen);
     if (rc) return rc;
     /* longest-processing-time first: order jobs by turns x elements */
     std::vector<int> order(njobs);
@@ -952,8 +999,9 @@ int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int3
         double cb = (double)J[b].nturns * (lats[b]->nwords + 1);
         return ca > cb;
     });
-    make_claims(h, h->h_tiles, J, order, grid_max, 1);
-    return launch(h, J, h->h_tiles, smem, grid_max, mode, st, h->threads, h->ppt);
+    const int pp = gen ? 1 : h->ppt;
+    make_claims(h, h->h_tiles, J, order, grid_max, 1, pp);
+    return launch(h, J, h->h_tiles, smem, grid_max, mode, st, h->threads, pp, gen);
 }
 
 int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,
@@ -987,8 +1035,9 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
         J[j].lcoord = d.lcoord;
     }
     int smem = 0, grid_max = 0;
+    bool gen = false;
     if (!lats.empty()) {
-        int rc = kernel_config(h, lats, mode, &smem, &grid_max);
+        int rc = kernel_config(h, lats, mode, &smem, &grid_max, &gen);
         if (rc) return rc;
     }
     std::vector<int> order(J.size());
@@ -998,7 +1047,7 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
                (double)J[b].nturns * (lats[b]->nwords + 1) * 1.0;
     });
     std::vector<AtbTile> tiles;
-    make_claims(h, tiles, J, order, grid_max, h->refill_k);
+    make_claims(h, tiles, J, order, grid_max, h->refill_k, gen ? 1 : h->ppt);
     int id = -1;
     for (int i = 0; i < (int)h->batches.size(); ++i)
         if (!h->batches[i].used) { id = i; break; }
@@ -1021,7 +1070,8 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
     B.used = true;
     B.mode = mode;
     B.threads = h->threads;
-    B.ppt = h->ppt;
+    B.ppt = gen ? 1 : h->ppt;
+    B.gen = gen;
     B.seg_cap = h->seg_cap_words;
     B.smem = smem;
     B.ntiles = (int)tiles.size();
@@ -1051,7 +1101,13 @@ static int batch_enqueue(atb_handle* h, Batch& B, cudaStream_t st) {
     unsigned long long* jn = B.jobnext.as<unsigned long long>();
     int* sts = h->status.as<int>();
     double* scr = B.scratch.as<double>();
-    if (B.mode == ATB_MODE_EXACT && B.ppt == 2)
+    if (B.gen && B.mode == ATB_MODE_EXACT)
+        atb_track_kernel_exact_gen<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, jn,
+                                                                      sts, B.seg_cap, scr);
+    else if (B.gen)
+        atb_track_kernel_fast_gen<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, jn,
+                                                                     sts, B.seg_cap, scr);
+    else if (B.mode == ATB_MODE_EXACT && B.ppt == 2)
         atb_track_kernel_exact_np2<<<B.grid, B.threads, B.smem, st>>>(dj, dt, B.ntiles, cnt, jn,
                                                                       sts, B.seg_cap, scr);
     else if (B.mode == ATB_MODE_EXACT)

@@ -19,6 +19,8 @@
 /* bounded mbarrier wait: 1 s, then the kernel reports and returns */
 #define ATB_WAIT_NS 1000000000ULL
 #define ATB_STATUS_WAIT_TIMEOUT 1
+#define ATB_STATUS_INTEGRATOR 2   /* an element compiled for another integrator
+                                     reached a kernel built without them */
 
 /* one staged lattice segment: consecutive element records */
 typedef struct AtbSeg {

@@ -236,5 +236,8 @@ extern "C" int atb_track_noalloc(int32_t device, const double* table, int64_t nw
     if (e != cudaSuccess) return na_fail(ATB_ERR_CUDA, cudaGetErrorString(e));
     if (s & ATB_STATUS_WAIT_TIMEOUT)
         return na_fail(ATB_ERR_TIMEOUT, "a bounded shared-memory staging wait timed out");
+    if (s & ATB_STATUS_INTEGRATOR)
+        return na_fail(ATB_ERR_ARG, "atb_track_noalloc: the table uses another integrator than "
+                                    "the default (4); use atb_track");
     return ATB_OK;
 }

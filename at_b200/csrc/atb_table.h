@@ -70,6 +70,9 @@
 #define ATB_F_FINT_OUT     (1u << 16)  /* bend exit FringeInt2 > 0 and FullGap > 0 */
 #define ATB_F_NOSKEW       (1u << 17)  /* thick multipole: every PolynomA
                                           coefficient (KickAngle folded) is 0 */
+#define ATB_F_INTEG        (1u << 18)  /* thick multipole integrated by the
+                                          integrator whose id (1-6) is stored at
+                                          ATB_SM_INTEG, with step ATB_SM_SL */
 /* bend fringe "method" codes after host normalisation (atphyslib.c:15-79) */
 #define ATB_BM_LEGACY      0   /* method 0 or any value other than 1,2,3   */
 #define ATB_BM_1           1
@@ -112,6 +115,11 @@
 #define ATB_SM_B1      8   /* PolynomB[1] as seen by the quad fringe         */
 #define ATB_SM_RADC    9   /* RAD_CONST*gamma^3 (Rad variants)               */
 #define ATB_SM_POLY   10   /* A[0..n], then B[0..n]                          */
+/* with ATB_F_INTEG set, the Forest-Ruth words carry the step and the id */
+#define ATB_SM_SL     ATB_SM_L1   /* Length/NumIntSteps                     */
+#define ATB_SM_ONE    ATB_SM_L2   /* 1.0: the entrance L2 x 1/(1+delta) is then
+                                     1/(1+delta) itself                     */
+#define ATB_SM_INTEG  ATB_SM_K1   /* integrator id, as a double             */
 
 /* BNDMPOLE / BNDMPOLE_RAD share words 2-9 with STRMPOLE                     */
 #define ATB_BM_IRHO    10

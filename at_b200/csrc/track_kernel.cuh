@@ -20,6 +20,7 @@
 
 #include <cstdint>
 #include "atb_physics.cuh"
+#include "atb_integrators.h"
 #include "atb_kernel_api.h"
 
 #ifndef ATB_FAST
@@ -161,6 +162,99 @@ __device__ __forceinline__ T fringe_b1(const Rec& e, const Param& pm) {
     return b1;
 }
 
+/* The integration steps of a thick multipole under integrator id
+ * e.f(ATB_SM_INTEG) (1-6, atb_integrators.h), step SL = e.f(ATB_SM_SL): per
+ * step, for each stage a drift of SL*c[i] and a kick of SL*d[i], skipping zero
+ * coefficients.  The drift and kick are the ones the Forest-Ruth steps use:
+ * fastdrift with the entrance 1/(1+delta) in plain magnets (pnorm: the
+ * entrance L2 x 1/(1+delta) with the table's L2 word set to 1.0), the
+ * radiating drift and kicks otherwise (the angle-carrying forms in the fast
+ * kernels). */
+template <int NP, bool BEND, bool RAD, class PL, class T>
+__device__ __forceinline__ void multipole_steps_generic(P6T<T>* r, const Rec& e, const PL& pl,
+                                                        const T* pnorm, double irho, int ns) {
+    const double SL = e.f(ATB_SM_SL);
+    int id = (int)e.f(ATB_SM_INTEG);
+    if (id < 1 || id >= ATB_INTEG_COUNT) id = 4;   /* the host writes 1-6 only */
+    const AtbInteg& ig = atb_integ[id];
+    if (RAD) {
+        const double radc = e.f(ATB_SM_RADC);
+        if constexpr (kFast && !is_dual<T>::value) {
+            if (ns <= 0) return;
+            RadAngles a[NP];
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                const double pn = 1.0 / (1.0 + r[k].dp);
+                a[k] = RadAngles{r[k].px * pn, r[k].py * pn, 0.0, 1.0 + r[k].dp};
+            }
+            for (int m = 0; m < ns; ++m) {
+                for (int i = 0; i < ig.n; ++i) {
+                    if (ig.c[i] != 0.0) {
+                        const double ld = SL * ig.c[i];
+#pragma unroll
+                        for (int k = 0; k < NP; ++k) rad_drift_fast(r[k], a[k], ld, 0.5 * ld);
+                    }
+                    if (ig.d[i] != 0.0) {
+                        const double lk = SL * ig.d[i];
+#pragma unroll
+                        for (int k = 0; k < NP; ++k) {
+                            if (BEND) bnd_kick_rad_fast(r[k], a[k], pl, lk, irho, lk * irho, radc * lk);
+                            else str_kick_rad_fast(r[k], a[k], pl, lk, radc * lk);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                r[k].px = a[k].xp * a[k].opd;
+                r[k].py = a[k].yp * a[k].opd;
+            }
+        } else {
+            for (int m = 0; m < ns; ++m) {
+                for (int i = 0; i < ig.n; ++i) {
+                    if (ig.c[i] != 0.0) {
+                        const double ld = SL * ig.c[i];
+#pragma unroll
+                        for (int k = 0; k < NP; ++k) diff_drift(r[k], ld);
+                    }
+                    if (ig.d[i] != 0.0) {
+                        const double lk = SL * ig.d[i];
+#pragma unroll
+                        for (int k = 0; k < NP; ++k) {
+                            if (BEND) bnd_kick_rad(r[k], pl, lk, irho, lk * irho, radc);
+                            else str_kick_rad(r[k], pl, lk, radc);
+                        }
+                    }
+                }
+            }
+        }
+    } else {
+        T h[NP];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) h[k] = kFast ? T(0.5 / (1.0 + r[k].dp)) : T(0.0);
+        for (int m = 0; m < ns; ++m) {
+            for (int i = 0; i < ig.n; ++i) {
+                if (ig.c[i] != 0.0) {
+                    const double ld = SL * ig.c[i];
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) {
+                        const T nl = ld * pnorm[k];
+                        fastdrift<kFast>(r[k], nl, kFast ? T(nl * h[k]) : T(0.0));
+                    }
+                }
+                if (ig.d[i] != 0.0) {
+                    const double lk = SL * ig.d[i];
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) {
+                        if (BEND) bndthinkick(r[k], pl, lk, irho, lk * irho);
+                        else strthinkick(r[k], pl, lk);
+                    }
+                }
+            }
+        }
+    }
+}
+
 /* StrMPoleSymplectic4Pass.c:29-109, BndMPoleSymplectic4Pass.c:38-129,
  * StrMPoleSymplectic4RadPass.c:30-115, BndMPoleSymplectic4RadPass.c:39-128.
  * NP particles of one thread pass the element together: every per-particle
@@ -168,7 +262,7 @@ __device__ __forceinline__ T fringe_b1(const Rec& e, const Param& pm) {
  * kicks form one straight-line block whose independent chains the compiler
  * interleaves (NP = 2), while the element's parameters are read once.  Each
  * particle sees the same operations as alone (NP = 1). */
-template <int NP, int MO, bool BEND, bool RAD, bool SKEW = true, class T>
+template <int NP, int MO, bool BEND, bool RAD, bool SKEW = true, bool GEN = false, class T>
 __device__ __forceinline__ void pass_multipole_n(P6T<T>* r, const Rec& e, const Param& pm) {
     const uint32_t fl = e.flags();
     const double L1 = e.f(ATB_SM_L1), L2 = e.f(ATB_SM_L2);
@@ -229,7 +323,11 @@ __device__ __forceinline__ void pass_multipole_n(P6T<T>* r, const Rec& e, const 
         }
     }
     const int ns = e.nsteps();
-    if (RAD) {
+    if constexpr (GEN) {
+        /* another integrator of the GPU call: steps of SL*c[i] drift and
+           SL*d[i] kick (atgpu/SymplecticIntegrator.cpp:140-171) */
+        multipole_steps_generic<NP, BEND, RAD>(r, e, pl, nl2, irho, ns);
+    } else if (RAD) {
         const double radc = e.f(ATB_SM_RADC);
         if constexpr (kFast && !is_dual<T>::value) {
             if (ns > 0) {
@@ -357,13 +455,23 @@ __device__ __forceinline__ void pass_multipole_n(P6T<T>* r, const Rec& e, const 
     }
 }
 
-template <int NP, bool BEND, bool RAD, class T>
+template <int NP, bool BEND, bool RAD, bool GEN = false, class T>
 __device__ __forceinline__ void pass_multipole_dispatch_n(P6T<T>* r, const Rec& e,
                                                           const Param& pm) {
     if constexpr (is_dual<T>::value) {
         /* one generic instance for the tangent kernel keeps its size sane */
         pass_multipole_n<NP, -1, BEND, RAD>(r, e, pm);
     } else {
+        /* tables compiled for another integrator of the GPU call take one
+           generic instance, in the kernels built with them (GEN); the tile
+           loop of the others flags such elements, and the tangent kernel's
+           host refuses them */
+        if constexpr (GEN) {
+            if (e.flags() & ATB_F_INTEG) {
+                pass_multipole_n<NP, -1, BEND, RAD, true, true>(r, e, pm);
+                return;
+            }
+        }
         /* the fast kernels evaluate upright magnets' fields without the
            zero skew terms */
         const bool upright = kFast && (e.flags() & ATB_F_NOSKEW);
@@ -386,9 +494,9 @@ __device__ __forceinline__ void pass_multipole_dispatch_n(P6T<T>* r, const Rec& 
     }
 }
 
-template <bool BEND, bool RAD, class T>
+template <bool BEND, bool RAD, bool GEN = false, class T>
 __device__ __forceinline__ void pass_multipole_dispatch(P6T<T>& r, const Rec& e, const Param& pm) {
-    pass_multipole_dispatch_n<1, BEND, RAD>(&r, e, pm);
+    pass_multipole_dispatch_n<1, BEND, RAD, GEN>(&r, e, pm);
 }
 
 /* DriftPass.c:16-48 */
@@ -499,7 +607,7 @@ __device__ __forceinline__ void pass_quantdiff(P6T<T>& r, const Rec& e, const ui
     }
 }
 
-template <class T>
+template <bool GEN = false, class T>
 __device__ __forceinline__ void track_element(P6T<T>& r, const Rec& e, int nturn,
                                               const Param& pm = Param{-1, 0.0},
                                               const uint64_t* rng_key = nullptr, long long p = 0,
@@ -508,10 +616,10 @@ __device__ __forceinline__ void track_element(P6T<T>& r, const Rec& e, int nturn
     switch (e.op()) {
         case ATB_OP_IDENTITY: pass_identity(r, e); break;
         case ATB_OP_DRIFT: pass_drift(r, e); break;
-        case ATB_OP_STRMPOLE: pass_multipole_dispatch<false, false>(r, e, pm); break;
-        case ATB_OP_STRMPOLE_RAD: pass_multipole_dispatch<false, true>(r, e, pm); break;
-        case ATB_OP_BNDMPOLE: pass_multipole_dispatch<true, false>(r, e, pm); break;
-        case ATB_OP_BNDMPOLE_RAD: pass_multipole_dispatch<true, true>(r, e, pm); break;
+        case ATB_OP_STRMPOLE: pass_multipole_dispatch<false, false, GEN>(r, e, pm); break;
+        case ATB_OP_STRMPOLE_RAD: pass_multipole_dispatch<false, true, GEN>(r, e, pm); break;
+        case ATB_OP_BNDMPOLE: pass_multipole_dispatch<true, false, GEN>(r, e, pm); break;
+        case ATB_OP_BNDMPOLE_RAD: pass_multipole_dispatch<true, true, GEN>(r, e, pm); break;
         case ATB_OP_THINMPOLE: pass_thinmpole(r, e, pm); break;
         case ATB_OP_RFCAVITY: pass_rfcavity(r, e, nturn); break;
         case ATB_OP_CORRECTOR: pass_corrector(r, e); break;
@@ -609,7 +717,7 @@ __device__ __forceinline__ void apply_loss_rule(const AtbJob& J, P6& r, bool& lo
  * counts its own turns (RF phase, loss turn and random kicks use the
  * particle's turn).  Blocks so stay full while their job has particles left
  * instead of running a few survivors for all remaining turns. */
-template <int NP>
+template <int NP, bool GEN = false>
 __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                                             const AtbTile* __restrict__ tiles, int ntiles,
                                             int* __restrict__ tile_counter,
@@ -762,13 +870,22 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                     }
                     bool together = false;
                     if constexpr (NP > 1) together = track_together(r, e);
+                    if constexpr (!GEN) {
+                        /* an element compiled for another integrator needs the
+                           kernels built with them: flag it and leave it out */
+                        if (e.flags() & ATB_F_INTEG) {
+                            if (tid == 0) atomicOr(status, ATB_STATUS_INTEGRATOR);
+                            w += e.len();
+                            continue;
+                        }
+                    }
                     if (together) {
                         if constexpr (NP > 1) pass_multipoles_together(r, e);
                     } else {
 #pragma unroll
                         for (int k = 0; k < NP; ++k)
-                            track_element(r[k], e, nturn[k], Param{-1, 0.0}, &J.rng_key, p[k],
-                                          ei);
+                            track_element<GEN>(r[k], e, nturn[k], Param{-1, 0.0}, &J.rng_key,
+                                               p[k], ei);
                     }
 #pragma unroll
                     for (int k = 0; k < NP; ++k)
@@ -985,6 +1102,19 @@ ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
                                        double* __restrict__ scratch) {
     track_tiles<1>(jobs, tiles, ntiles, tile_counter, job_next, status, smem_cap_words,
                    scratch);
+}
+
+/* with the other integrators of the GPU call (tables with ATB_F_INTEG) */
+extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
+ATB_CAT(ATB_CAT(atb_track_kernel, ATB_KSUFFIX), _gen)(const AtbJob* __restrict__ jobs,
+                                                      const AtbTile* __restrict__ tiles,
+                                                      int ntiles, int* __restrict__ tile_counter,
+                                                      unsigned long long* __restrict__ job_next,
+                                                      int* __restrict__ status,
+                                                      int smem_cap_words,
+                                                      double* __restrict__ scratch) {
+    track_tiles<1, true>(jobs, tiles, ntiles, tile_counter, job_next, status, smem_cap_words,
+                         scratch);
 }
 
 /* two particles per thread (the autotuner's particles-per-thread choice) */

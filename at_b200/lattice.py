@@ -282,7 +282,7 @@ def _gamma(energy: float, rest_energy: float) -> float:
     return energy / rest_energy
 
 
-def _multipole_common(rec: _Record, el, op: int, bend: bool):
+def _multipole_common(rec: _Record, el, op: int, bend: bool, integrator: int = 4):
     le = _get_double(el, "Length")
     pa = _get_array(el, "PolynomA")
     pb = _get_array(el, "PolynomB")
@@ -323,6 +323,14 @@ def _multipole_common(rec: _Record, el, op: int, bend: bool):
     rec.set(T.ATB_SM_L2, sl * DRIFT2)
     rec.set(T.ATB_SM_K1, sl * KICK1)
     rec.set(T.ATB_SM_K2, sl * KICK2)
+    if integrator != 4:
+        # another integrator of the GPU call: the step and the id replace the
+        # Forest-Ruth lengths (atgpu/SymplecticIntegrator.cpp:140-171)
+        rec.flags |= T.ATB_F_INTEG
+        rec.set(T.ATB_SM_SL, sl)
+        rec.set(T.ATB_SM_ONE, 1.0)
+        rec.set(T.ATB_SM_INTEG, float(integrator))
+        rec.set(T.ATB_SM_K2, 0.0)
     if ka is not None:
         B[0] = B[0] - _div(math.sin(ka[0]), le)
         A[0] = A[0] + _div(math.sin(ka[1]), le)
@@ -457,7 +465,7 @@ class CompiledLattice:
 
 
 def _compile_element(el, idx: int, energy: float, rest_energy: float, t0: float,
-                     cl_fields: list, voltages: dict):
+                     cl_fields: list, voltages: dict, integrator: int = 4):
     pm = getattr(el, "PassMethod")
     op = T.PASS_OPCODES[pm]
     if op == T.ATB_OP_IDENTITY:
@@ -469,10 +477,10 @@ def _compile_element(el, idx: int, energy: float, rest_energy: float, t0: float,
         _add_misalign_entrance(rec, el)
     elif op in (T.ATB_OP_STRMPOLE, T.ATB_OP_STRMPOLE_RAD):
         rec = _Record(op, T.ATB_SM_POLY)
-        _multipole_common(rec, el, op, bend=False)
+        _multipole_common(rec, el, op, bend=False, integrator=integrator)
     elif op in (T.ATB_OP_BNDMPOLE, T.ATB_OP_BNDMPOLE_RAD):
         rec = _Record(op, T.ATB_BM_POLY)
-        _multipole_common(rec, el, op, bend=True)
+        _multipole_common(rec, el, op, bend=True, integrator=integrator)
     elif op == T.ATB_OP_THINMPOLE:
         rec = _Record(op, T.ATB_TM_POLY)
         pa = _get_array(el, "PolynomA")
@@ -597,14 +605,28 @@ def check_pass_methods(line) -> list[str]:
     return names
 
 
+def check_integrator(integrator) -> int:
+    """The GPU call's ``integrator`` (1-6, atgpu/PyInterface.cpp:44-50); other
+    values fail as the reference backend's lattice build does
+    (atgpu/SymplecticIntegrator.cpp:82-84, PyInterface.cpp:292-296)."""
+    k = int(integrator)
+    if k < 1 or k > 6:
+        raise RuntimeError("at_gpupass() build lattice failed: SymplecticIntegrator, type %d "
+                           "not supported" % k)
+    return k
+
+
 def compile_lattice(line, energy: float = 0.0, rest_energy: float = 0.0,
-                    charge: float = -1.0, t0: float | None = None) -> CompiledLattice:
+                    charge: float = -1.0, t0: float | None = None,
+                    integrator: int = 4) -> CompiledLattice:
     """Compile ``line`` (a sequence of elements) to a flat element table.
 
     ``t0`` defaults to the revolution time ``RingLength/C0`` of the line
     (pyat/at.c:540-551); single-element tracking passes ``t0=0``
-    (pyat/at.c:728-729).
+    (pyat/at.c:728-729).  ``integrator`` selects the thick multipoles'
+    symplectic integrator (4, Forest-Ruth, is the CPU engine's).
     """
+    integrator = check_integrator(integrator)
     names = check_pass_methods(line)
     ring_length = 0.0
     for el in line:
@@ -621,7 +643,8 @@ def compile_lattice(line, energy: float = 0.0, rest_energy: float = 0.0,
         op = T.PASS_OPCODES[pm]
         local: list = []
         try:
-            rec = _compile_element(el, i, energy, rest_energy, t0, local, voltages)
+            rec = _compile_element(el, i, energy, rest_energy, t0, local, voltages,
+                                   integrator)
             w = rec.words()
             info = ElementInfo(op, pm, element_length(el), rec.max_order, rec.nsteps, rec.flags)
             if local and not energy > 0.0:

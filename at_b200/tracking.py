@@ -17,7 +17,7 @@ from concurrent.futures import ThreadPoolExecutor
 import numpy as np
 
 from . import engine as _eng
-from .lattice import C0, CompiledLattice, compile_lattice
+from .lattice import C0, CompiledLattice, check_integrator, compile_lattice
 
 __all__ = ["gpupass", "atpass", "elempass", "gpuinfo", "reset_cache"]
 
@@ -30,6 +30,7 @@ class _State:
     def __init__(self):
         self.lattice = None            # the list last tracked successfully
         self.compiled: CompiledLattice | None = None
+        self.integrator = 4                # integrator the cached table was compiled for
         self.lids: dict[int, int] = {}  # device -> uploaded lattice id
         self.last_turn = 0
         self.lock = threading.RLock()
@@ -171,7 +172,11 @@ def gpupass(line, r_in, nturns, refpts=_defref, *, turn=0, energy=None, particle
     ``(rout, {"islost", "turn", "elem", "coord"})`` when ``losses`` is true.
     ``gpu_pool`` may list several devices: the particles are then split into
     contiguous shards, one per device (the reference accepts one).
-    ``integrator`` must be 4 (Forest-Ruth, the reference CPU integrator).
+    ``integrator`` selects the thick multipoles' symplectic integrator as in
+    the reference GPU backend: 1 Euler, 2 McLachlan-Atela 2nd order, 3 Ruth 3rd
+    order, 4 Forest-Ruth 4th order (the default, the CPU engine's), 5
+    McLachlan-Atela 4th order, 6 Yoshida 6th order; changing it recompiles the
+    lattice even with ``reuse``.
     ``mode`` selects "fast" (default) or "exact" arithmetic; ``stats=True``
     adds per-turn survivor counts and coordinate sums as a third result.
     ``omp_num_threads``, ``bunch_spos``, ``bunch_currents``,
@@ -191,20 +196,21 @@ def gpupass(line, r_in, nturns, refpts=_defref, *, turn=0, energy=None, particle
         raise TypeError("energy must be float, not %s" % type(energy).__name__)
     start_elem = _as_int(start_elem if start_elem is not None else 0, "start_elem")
     end_elem = _as_int(end_elem if end_elem is not None else 0, "end_elem")
-    if integrator != 4:
-        raise ValueError("only the 4th-order Forest-Ruth integrator (integrator=4) is supported")
+    integrator = check_integrator(integrator)
     _check_rin(r_in)
     npart = r_in.size // 6
     devs = _devices(gpu_pool)
 
     with _state.lock:
         # -- lattice cache (pyat/at.c:445-512) --------------------------------
-        if not (reuse and _state.lattice is line and _state.compiled is not None):
+        if not (reuse and _state.lattice is line and _state.compiled is not None and
+                _state.integrator == integrator):
             _drop_uploads()
             _state.lattice = None
             _state.compiled = None
             e, rest, charge = _energy_particle(line, energy, particle)
-            _state.compiled = compile_lattice(line, e, rest, charge)
+            _state.compiled = compile_lattice(line, e, rest, charge, integrator=integrator)
+            _state.integrator = integrator
         cl = _state.compiled
         nelem = cl.nelem
         # -- partial turns (pyat/at.c:514-536) ---------------------------------

@@ -152,7 +152,8 @@ int atb_track_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np, i
  * read from param_value (device, nparam), which replaces the table's values
  * for those coefficients, so a caller can move them without re-uploading the
  * lattice.  Lost particles come back NaN in r, jac and grad (islost, optional,
- * marks them).  Replaces the finite-difference Jacobian of
+ * marks them).  The lattice must be compiled for the default integrator
+ * (ATB_ERR_ARG otherwise).  Replaces the finite-difference Jacobian of
  * pyat/at/physics/matrix.py:105-165 (find_m66) and the finite differences a
  * caller of lattice_pass would take for strength sensitivities; the
  * reference has no exact-derivative tracking. */
@@ -165,7 +166,8 @@ int atb_tangent_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np,
  * for a particle entering element i at orbits[6 i .. 6 i + 5], its transfer
  * matrix m66[i] (exact derivatives, row-major d out / d in) and its radiation
  * diffusion matrix b66[i] (row-major; zero for non-radiating pass methods),
- * with `diff_const` = DIF_CONST gamma^5, all elements in one launch.  Replaces
+ * with `diff_const` = DIF_CONST gamma^5, all elements in one launch (the
+ * lattice compiled for the default integrator, ATB_ERR_ARG otherwise).  Replaces
  * the per-element loop of pyat/at/physics/radiation.py:76-148 (_dmatr), i.e.
  * find_elem_m66 and pyat/at.c:755-831 (diffusion_matrix) per element. */
 int atb_element_maps(atb_handle* h, int32_t lattice_id, const double* orbits, double* m66,

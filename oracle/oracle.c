@@ -51,7 +51,7 @@ typedef struct {
     int32_t FringeBendExit;
     int32_t FringeQuadEntrance;
     int32_t FringeQuadExit;
-    int32_t pad;
+    int32_t Integrator;   /* 0 or 4: Forest-Ruth; 1-6: the GPU call's integrators */
     double Length, BendingAngle, EntranceAngle, ExitAngle;
     double FringeInt1, FringeInt2, FullGap, Scaling;
     double Voltage, Frequency, TimeLag, PhaseLag;
@@ -440,6 +440,50 @@ static double o_gamma(double energy, double rest) {
     return (rest == 0.0) ? 1.0E-9 * energy / O_E0 : energy / rest;
 }
 
+/* The symplectic integrators of the reference GPU backend's gpupass
+ * (atgpu/SymplecticIntegrator.cpp:28-80): per step SL, stages of a drift
+ * SL*c[i] and a kick SL*d[i].  Euler; McLachlan-Atela optimal 2nd order;
+ * Ruth 3rd order; Forest-Ruth 4th order; McLachlan-Atela optimal 4th order;
+ * Yoshida 6th order (solution A).  Returns the number of stages. */
+static int o_integ(int id, double *c, double *d) {
+    static const double mc5[4] = {0.1288461583653843, 0.4415830236164665,
+                                  -0.0857820194129737, 0.5153528374311229};
+    static const double md5[4] = {0.3340036032863214, 0.7563200005156683,
+                                  -0.2248198030794208, 0.1344961992774311};
+    static const double yc6[8] = {0.3922568052387800, 0.5100434119184585, -0.4710533854097566,
+                                  0.0687531682525181, 0.0687531682525181, -0.4710533854097566,
+                                  0.5100434119184585, 0.3922568052387800};
+    static const double yd6[8] = {0.7845136104775600, 0.2355732133593570, -1.1776799841788701,
+                                  1.3151863206839063, -1.1776799841788701, 0.2355732133593570,
+                                  0.7845136104775600, 0.0};
+    switch (id) {
+        case 1:
+            c[0] = 1.0; d[0] = 1.0;
+            return 1;
+        case 2:
+            c[0] = d[0] = 1.0 - 1.0 / sqrt(2.0);
+            c[1] = d[1] = 1.0 / sqrt(2.0);
+            return 2;
+        case 3:
+            c[0] = 1.0; c[1] = -2.0 / 3.0; c[2] = 2.0 / 3.0;
+            d[0] = -1.0 / 24.0; d[1] = 3.0 / 4.0; d[2] = 7.0 / 24.0;
+            return 3;
+        case 5:
+            for (int i = 0; i < 4; i++) { c[i] = mc5[i]; d[i] = md5[i]; }
+            return 4;
+        case 6:
+            for (int i = 0; i < 8; i++) { c[i] = yc6[i]; d[i] = yd6[i]; }
+            return 8;
+        default:
+            c[0] = O_DRIFT1; c[1] = O_DRIFT2; c[2] = O_DRIFT2; c[3] = O_DRIFT1;
+            d[0] = O_KICK1; d[1] = O_KICK2; d[2] = O_KICK1; d[3] = 0.0;
+            return 4;
+    }
+}
+
+/* the coefficient table of integrator ``id`` (for the tests) */
+int oracle_integ(int id, double *c, double *d) { return o_integ(id, c, d); }
+
 /* StrMPole/BndMPole (Rad) Symplectic4: StrMPoleSymplectic4Pass.c:29-109,
  * BndMPoleSymplectic4Pass.c:38-129, StrMPoleSymplectic4RadPass.c:30-115,
  * BndMPoleSymplectic4RadPass.c:39-128 */
@@ -453,10 +497,10 @@ static void o_multipole(real *r, const OElem *e, const real *A, const real *B, i
     int lin_in = (e->fringeIntM0 && e->fringeIntP0 && e->FringeQuadEntrance == 2);
     int lin_out = (e->fringeIntM0 && e->fringeIntP0 && e->FringeQuadExit == 2);
     real s = e->Scaling;
-    real nl1 = 0, nl2 = 0;
+    real nl1 = 0, nl2 = 0, pn = 0;
     if (s != 1.0) o_pref(r, s);
     if (!rad) {
-        real pn = 1.0 / (1.0 + r[4]);
+        pn = 1.0 / (1.0 + r[4]);
         nl1 = L1 * pn;
         nl2 = L2 * pn;
     }
@@ -472,7 +516,28 @@ static void o_multipole(real *r, const OElem *e, const real *A, const real *B, i
         if (lin_in) o_lin_fringe(r, B[1], e->fringeIntM0, e->fringeIntP0, 1);
         else o_quad_fringe(r, B[1], +1);
     }
-    for (int m = 0; m < e->NumIntSteps; m++) {
+    if (e->Integrator > 0 && e->Integrator != 4) {
+        double c[8], d[8];
+        const int ni = o_integ(e->Integrator, c, d);
+        for (int m = 0; m < e->NumIntSteps; m++) {
+            for (int i = 0; i < ni; i++) {
+                if (c[i] != 0.0) {
+                    real ld = SL * c[i];
+                    if (rad) o_ddrift(r, ld, bd); else o_fastdrift(r, ld * pn);
+                }
+                if (d[i] != 0.0) {
+                    real lk = SL * d[i];
+                    if (rad) {
+                        if (bend) o_bndkick_rad(r, A, B, n, lk, h, radc, diffc, bd);
+                        else o_strkick_rad(r, A, B, n, lk, radc, diffc, bd);
+                    } else {
+                        if (bend) o_bndkick(r, A, B, lk, h, n); else o_strkick(r, A, B, lk, n);
+                    }
+                }
+            }
+        }
+    }
+    for (int m = 0; m < e->NumIntSteps && !(e->Integrator > 0 && e->Integrator != 4); m++) {
         if (rad) {
             o_ddrift(r, L1, bd);
             if (bend) o_bndkick_rad(r, A, B, n, K1, h, radc, diffc, bd);

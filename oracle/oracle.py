@@ -50,7 +50,7 @@ class OElem(C.Structure):
     _fields_ = [
         ("pass_", C.c_int32), ("MaxOrder", C.c_int32), ("NumIntSteps", C.c_int32),
         ("FringeBendEntrance", C.c_int32), ("FringeBendExit", C.c_int32),
-        ("FringeQuadEntrance", C.c_int32), ("FringeQuadExit", C.c_int32), ("pad", C.c_int32),
+        ("FringeQuadEntrance", C.c_int32), ("FringeQuadExit", C.c_int32), ("Integrator", C.c_int32),
         ("Length", C.c_double), ("BendingAngle", C.c_double), ("EntranceAngle", C.c_double),
         ("ExitAngle", C.c_double), ("FringeInt1", C.c_double), ("FringeInt2", C.c_double),
         ("FullGap", C.c_double), ("Scaling", C.c_double), ("Voltage", C.c_double),
@@ -129,7 +129,7 @@ def _arr(el, name, keep):
     return a.ctypes.data_as(_dp)
 
 
-def _elements(line, keep):
+def _elements(line, keep, integrator=4):
     arr = (OElem * max(len(line), 1))()
     for o, el in zip(arr, line):
         pm = el.PassMethod
@@ -139,6 +139,7 @@ def _elements(line, keep):
         o.Length = float(getattr(el, "Length", 0.0))
         o.MaxOrder = int(getattr(el, "MaxOrder", 0))
         o.NumIntSteps = int(getattr(el, "NumIntSteps", 0))
+        o.Integrator = int(integrator)
         o.BendingAngle = float(getattr(el, "BendingAngle", 0.0)) if pm.startswith("Bnd") else 0.0
         o.EntranceAngle = float(getattr(el, "EntranceAngle", 0.0))
         o.ExitAngle = float(getattr(el, "ExitAngle", 0.0))
@@ -168,14 +169,26 @@ def _elements(line, keep):
     return arr
 
 
+def integrator_table(k: int):
+    """The oracle's (c, d) coefficient lists of integrator ``k``."""
+    lib = _load()
+    c = (C.c_double * 8)()
+    d = (C.c_double * 8)()
+    lib.oracle_integ.restype = C.c_int
+    n = lib.oracle_integ(int(k), c, d)
+    return list(c[:n]), list(d[:n])
+
+
 def track(line, r, nturns, refpts=None, turn=0, energy=0.0, rest_energy=0.0, losses=False,
-          start_elem=0, end_elem=None, nthreads=None, t0=None, element=False):
+          start_elem=0, end_elem=None, nthreads=None, t0=None, element=False, integrator=4):
     """Track the (6, N) Fortran-ordered ``r`` in place with the C oracle.
+    ``integrator`` (1-6) selects the thick multipoles' symplectic integrator
+    as the reference GPU backend's gpupass does (4 is the CPU engine's).
 
     Returns ``(rout, lossdict or None)`` with the reference's layouts."""
     lib = _load()
     keep: list = []
-    els = _elements(line, keep)
+    els = _elements(line, keep, integrator)
     nelem = len(line)
     # pyat/at.c:504 accumulates the lengths one by one; Python's sum() of
     # floats is compensated (3.12+) and can differ in the last bits

@@ -1,0 +1,152 @@
+"""The six symplectic integrators of the GPU call's ``integrator`` argument.
+
+The coefficient tables of the kernel header and of the oracle are pinned to
+the reference GPU backend's (``golden/integrators.json``, read from
+atgpu/SymplecticIntegrator.cpp by ``golden/make_golden_integrators.py``);
+the oracle's integrators show the orders of accuracy of those tables
+(1, 1, 3, 4, 4, 6) on a thick quadrupole and sextupole; the compiler's table words and error
+behaviour follow the reference's lattice build; on the GPU every integrator
+matches the oracle on the FODO ring, plain and radiating, in both arithmetic
+modes, through the engine and through gpupass.
+"""
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+from at_b200 import elements as E
+from at_b200 import rings
+from at_b200 import table as T
+from at_b200.lattice import compile_lattice
+from conftest import ELECTRON_REST, GOLDEN, scale_rel_diff
+from oracle import oracle
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                      "at_b200", "csrc", "atb_integrators.h")
+# Integrator 2 is named second order, but the reference's table gives drifts
+# and kicks the same coefficients (1 - 1/sqrt 2, 1/sqrt 2), which violates the
+# second-order condition sum_i d_i (c_1 + .. + c_i) = 1/2 (it is 0.79): as
+# tabulated it is a first-order method.  The table is kept for identical
+# results, and this test pins the order it actually has.
+ORDERS = {1: 1, 2: 1, 3: 3, 4: 4, 5: 4, 6: 6}
+
+
+@pytest.fixture(scope="module")
+def golden():
+    with open(os.path.join(GOLDEN, "integrators.json")) as f:
+        g = json.load(f)
+    return {int(k): ([float.fromhex(x) for x in v["c"]], [float.fromhex(x) for x in v["d"]])
+            for k, v in g.items()}
+
+
+def _kernel_tables():
+    src = open(HEADER).read()
+    body = src[src.index("atb_integ[ATB_INTEG_COUNT] = {"):]
+    ents = re.findall(r"\{(\d+),\s*\{([^}]*)\},\s*\{([^}]*)\}\}", body)
+    out = {}
+    for k, (n, c, d) in enumerate(ents):
+        n = int(n)
+        out[k] = ([float(x) for x in c.split(",")][:n], [float(x) for x in d.split(",")][:n])
+    return out
+
+
+def test_kernel_table_is_the_reference_backends(golden):
+    tab = _kernel_tables()
+    for k in range(1, 7):
+        assert tab[k] == golden[k], k
+
+
+def test_oracle_table_is_the_reference_backends(golden):
+    for k in range(1, 7):
+        assert oracle.integrator_table(k) == golden[k], k
+
+
+def _quad_sext():
+    return [E.Quadrupole("Q", 1.0, 3.0, NumIntSteps=1),
+            E.Sextupole("S", 0.5, 40.0, NumIntSteps=1)]
+
+
+def _one_pass(line, k, nsteps):
+    for el in line:
+        el.NumIntSteps = nsteps
+    r = np.asfortranarray(np.array([[2e-3], [1e-4], [1.5e-3], [-1e-4], [1e-3], [0.0]]))
+    oracle.track(line, r, 1, energy=3e9, rest_energy=ELECTRON_REST, integrator=k)
+    return r[:, 0].copy()
+
+
+@pytest.mark.parametrize("k", sorted(ORDERS))
+def test_oracle_orders_of_accuracy(k):
+    """Halving the step divides the error of integrator k by about 2^order
+    (reference: Yoshida's method with 512 steps)."""
+    line = _quad_sext()
+    ref = _one_pass(line, 6, 512)
+    n0 = {1: 64, 2: 16, 3: 8, 4: 8, 5: 8, 6: 4}[k]
+    e1 = np.abs(_one_pass(line, k, n0) - ref).max()
+    e2 = np.abs(_one_pass(line, k, 2 * n0) - ref).max()
+    order = np.log2(e1 / e2)
+    assert abs(order - ORDERS[k]) < 0.35, (k, order)
+
+
+def test_compiled_words_for_another_integrator():
+    q = E.Quadrupole("Q", 0.5, 1.2, NumIntSteps=10)
+    d = compile_lattice([q], 3e9, ELECTRON_REST)
+    y = compile_lattice([q], 3e9, ELECTRON_REST, integrator=6)
+    assert np.array_equal(d.words, compile_lattice([q], 3e9, ELECTRON_REST, integrator=4).words)
+    hdr = int(y.words.view(np.uint64)[0])
+    assert (hdr >> T.ATB_H_FL_SHIFT) & T.ATB_F_INTEG
+    assert y.words[T.ATB_SM_SL] == 0.5 / 10 and y.words[T.ATB_SM_INTEG] == 6.0
+    assert y.words[T.ATB_SM_ONE] == 1.0
+    for bad in (0, 7, -1):
+        with pytest.raises(RuntimeError, match="not supported"):
+            compile_lattice([q], 3e9, ELECTRON_REST, integrator=bad)
+
+
+# ---------------------------------------------------------------- GPU tests --
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+@pytest.mark.parametrize("rad", [False, True])
+@pytest.mark.parametrize("k", [1, 2, 3, 5, 6])
+def test_integrators_match_oracle(k, rad, mode):
+    from at_b200.engine import Engine
+    ring = rings.fodo_ring()
+    if rad:
+        ring = rings.radiating(ring)
+    r0 = rings.gaussian(2048, seed=21)
+    ro = r0.copy(order="F")
+    oracle.track(ring, ro, 3, energy=3e9, rest_energy=ELECTRON_REST, integrator=k)
+    eng = Engine.get(0)
+    cl = compile_lattice(ring, 3e9, ELECTRON_REST, integrator=k)
+    lid = eng.upload(cl)
+    try:
+        rg = r0.copy(order="F")
+        eng.track(lid, rg, 3, 0, 0, cl.nelem, mode=mode)
+    finally:
+        eng.free(lid)
+    ok = ~np.isnan(ro[0])
+    assert np.array_equal(ok, ~np.isnan(rg[0]))
+    assert scale_rel_diff(rg[:, ok], ro[:, ok]) <= (1e-14 if mode == "exact" else 2e-13)
+
+
+@pytest.mark.gpu
+def test_gpupass_integrator_argument():
+    """gpupass(integrator=k) tracks with integrator k, recompiles when k
+    changes under reuse=True, and rejects unknown ids as the reference does."""
+    from at_b200 import gpupass
+    ring = list(rings.fodo_ring())
+    r0 = rings.gaussian(512, seed=22)
+    out = {}
+    for k in (4, 2, 4):
+        r = r0.copy(order="F")
+        gpupass(ring, r, 2, energy=3e9, particle=E.Particle("electron"), reuse=True,
+                integrator=k, mode="exact")
+        out.setdefault(k, []).append(r)
+    np.testing.assert_array_equal(out[4][0], out[4][1])
+    assert not np.array_equal(out[4][0], out[2][0])
+    ro = r0.copy(order="F")
+    oracle.track(ring, ro, 2, energy=3e9, rest_energy=ELECTRON_REST, integrator=2)
+    assert scale_rel_diff(out[2][0], ro) <= 1e-14
+    with pytest.raises(RuntimeError, match="not supported"):
+        gpupass(ring, r0.copy(order="F"), 1, energy=3e9, integrator=9)
