@@ -107,6 +107,19 @@ int na_setup(int device, unsigned char** out) {
 
 }  // namespace
 
+/* Flags a table element compiled for another integrator of the GPU call:
+   this entry point runs the default tracking kernels, which have only the
+   Forest-Ruth steps; the call then fails instead of tracking it. */
+__global__ void atb_noalloc_scan(const double* __restrict__ table,
+                                 const uint32_t* __restrict__ elem_off, int nelem,
+                                 int* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nelem) {
+        const uint64_t h = reinterpret_cast<const uint64_t*>(table)[elem_off[i]];
+        if ((h >> ATB_H_FL_SHIFT) & ATB_F_INTEG) atomicOr(status, ATB_STATUS_INTEGRATOR);
+    }
+}
+
 extern "C" int atb_track_noalloc(int32_t device, const double* table, int64_t nwords,
                                  const uint32_t* elem_off_host, const uint32_t* elem_off,
                                  int32_t nelem, double* r, int64_t np, int32_t nturns,
@@ -207,6 +220,9 @@ extern "C" int atb_track_noalloc(int32_t device, const double* table, int64_t nw
     const int ntiles = (int)ntiles64;
     AtbTile* tiles = reinterpret_cast<AtbTile*>(base + NA_TILES);
     atb_noalloc_tiles<<<(ntiles + 255) / 256, 256, 0, st>>>(tiles, ntiles, np, NA_THREADS);
+    if (nelem > 0)
+        atb_noalloc_scan<<<(nelem + 255) / 256, 256, 0, st>>>(table, elem_off, nelem,
+                                                             reinterpret_cast<int*>(base + NA_STATUS));
 
     const int smem = resident ? segs[0].nwords * 8 : 2 * NA_SEG_CAP_WORDS * 8;
     const void* fn = mode == ATB_MODE_EXACT ? (const void*)atb_track_kernel_exact

@@ -463,9 +463,9 @@ __device__ __forceinline__ void pass_multipole_dispatch_n(P6T<T>* r, const Rec& 
         pass_multipole_n<NP, -1, BEND, RAD>(r, e, pm);
     } else {
         /* tables compiled for another integrator of the GPU call take one
-           generic instance, in the kernels built with them (GEN); the tile
-           loop of the others flags such elements, and the tangent kernel's
-           host refuses them */
+           generic instance, in the kernels built with them (GEN); the hosts
+           of the other kernels send them none (atb_track_noalloc checks its
+           raw table with a scan kernel, the tangent host refuses it) */
         if constexpr (GEN) {
             if (e.flags() & ATB_F_INTEG) {
                 pass_multipole_n<NP, -1, BEND, RAD, true, true>(r, e, pm);
@@ -870,15 +870,6 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                     }
                     bool together = false;
                     if constexpr (NP > 1) together = track_together(r, e);
-                    if constexpr (!GEN) {
-                        /* an element compiled for another integrator needs the
-                           kernels built with them: flag it and leave it out */
-                        if (e.flags() & ATB_F_INTEG) {
-                            if (tid == 0) atomicOr(status, ATB_STATUS_INTEGRATOR);
-                            w += e.len();
-                            continue;
-                        }
-                    }
                     if (together) {
                         if constexpr (NP > 1) pass_multipoles_together(r, e);
                     } else {

@@ -150,3 +150,25 @@ def test_gpupass_integrator_argument():
     assert scale_rel_diff(out[2][0], ro) <= 1e-14
     with pytest.raises(RuntimeError, match="not supported"):
         gpupass(ring, r0.copy(order="F"), 1, energy=3e9, integrator=9)
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_a_table_for_another_integrator():
+    """atb_track_noalloc runs the default kernels, which have only the
+    Forest-Ruth steps: a raw table compiled for another integrator fails the
+    call (its header scan sets the status word) instead of tracking."""
+    import ctypes as C
+    import torch
+    from at_b200 import _lib
+    dev = torch.device("cuda", 0)
+    cl = compile_lattice(rings.fodo_ring(), 3e9, ELECTRON_REST, integrator=3)
+    words = torch.from_numpy(np.ascontiguousarray(cl.words)).to(dev)
+    off = torch.from_numpy(np.ascontiguousarray(cl.offsets).view(np.int32)).to(dev)
+    off_host = np.ascontiguousarray(cl.offsets, dtype=np.uint32)
+    rd = torch.from_numpy(np.ascontiguousarray(rings.gaussian(64, seed=3).T)).to(dev)
+    L = _lib.lib()
+    rc = L.atb_track_noalloc(0, words.data_ptr(), int(cl.words.size), off_host.ctypes.data,
+                             off.data_ptr(), int(cl.nelem), rd.data_ptr(), 64, 1, 0, 0,
+                             None, None, None, None, _lib.MODE_FAST, None)
+    assert rc == _lib.ATB_ERR_ARG
+    assert b"another integrator" in L.atb_last_error()
