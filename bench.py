@@ -66,6 +66,8 @@ def _args():
     ap.add_argument("--batch-turn-scale", type=float, default=0.01,
                     help="scale of the batched variants' turn counts (1.0: 500-5000 turns)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-exact-line", action="store_true",
+                    help="skip timing the exact-arithmetic kernel beside the fast one")
     return ap.parse_args()
 
 
@@ -288,12 +290,12 @@ def run_b200(a):
     assert sptr != 0
     lp = (lost.data_ptr(), lturn.data_ptr(), lelem.data_ptr(), lcoord.data_ptr())
 
-    def step(turn0, with_alive):
+    def step(turn0, with_alive, arith=None):
         if with_alive:
             alive.zero_()
         eng.track_device(lid, rd.data_ptr(), N, T, turn0, losses=lp,
-                         alive_ptr=alive.data_ptr() if with_alive else None, mode=mode,
-                         stream=sptr)
+                         alive_ptr=alive.data_ptr() if with_alive else None,
+                         mode=arith or mode, stream=sptr)
 
     turn = 0
     for _ in range(a.warmup):
@@ -334,6 +336,30 @@ def run_b200(a):
     # roofline of the tracking kernel: algorithmic flops of the particle-turns
     # actually tracked (survivors per turn) over its event-timed duration
     achieved = fpt * survivors / sum(times) / 1e12
+
+    # the exact-arithmetic kernel on the same resident bunch (the reference's
+    # operation order: within the stated one-turn tolerance on every ring)
+    exact_line = None
+    if world == 1 and mode == "fast" and not a.no_exact_line:
+        xt = []
+        step(turn, False, "exact")              # warm-up
+        turn += T
+        for _ in range(2):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(turn, False, "exact")
+            e1.record(stream)
+            e1.synchronize()
+            xt.append(e0.elapsed_time(e1) * 1e-3)
+            turn += T
+        eng.sync(sptr)
+        exact_line = {"value": N * T * len(xt) / sum(xt), "unit": UNIT,
+                      "ms_per_step": 1e3 * sum(xt) / len(xt), "steps": len(xt),
+                      "one_turn_deviation_from_oracle":
+                          "exact: <= 1e-13 on every ring; the headline's fast arithmetic: "
+                          "<= 2e-13 on this ring (tests/test_gpu_parity.py)"}
 
     # end to end through the drop-in entry point on pinned host buffers
     e2e = None
@@ -404,6 +430,7 @@ def run_b200(a):
                          "flops_per_particle_turn": fpt, "survivor_particle_turns": survivors},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps, "clocks": clk,
             "serving": serve, "differentiation": dif, "batching": bat, "acceptance": acc,
+            "exact_arithmetic": exact_line,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
