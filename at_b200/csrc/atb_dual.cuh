@@ -118,6 +118,57 @@ struct Dual {
     }
 };
 
+/* acc + a*b and acc - a*b: the value rounded as the plain expression (the
+ * product, then the sum), each derivative slot in two FMAs instead of a
+ * product, an FMA and an add.  The double forms are the plain expressions, so
+ * the tracking kernels compute what they computed before. */
+__device__ __forceinline__ double madd(double acc, double a, double b) { return acc + a * b; }
+__device__ __forceinline__ double msub(double acc, double a, double b) { return acc - a * b; }
+
+template <int K>
+__device__ __forceinline__ Dual<K> madd(const Dual<K>& acc, const Dual<K>& a, const Dual<K>& b) {
+    Dual<K> r;
+    r.v = acc.v + a.v * b.v;
+#pragma unroll
+    for (int i = 0; i < K; ++i) r.d[i] = fma(a.d[i], b.v, fma(a.v, b.d[i], acc.d[i]));
+    return r;
+}
+template <int K>
+__device__ __forceinline__ Dual<K> madd(const Dual<K>& acc, double a, const Dual<K>& b) {
+    Dual<K> r;
+    r.v = acc.v + a * b.v;
+#pragma unroll
+    for (int i = 0; i < K; ++i) r.d[i] = fma(a, b.d[i], acc.d[i]);
+    return r;
+}
+template <int K>
+__device__ __forceinline__ Dual<K> msub(const Dual<K>& acc, double a, const Dual<K>& b) {
+    Dual<K> r;
+    r.v = acc.v - a * b.v;
+#pragma unroll
+    for (int i = 0; i < K; ++i) r.d[i] = fma(-a, b.d[i], acc.d[i]);
+    return r;
+}
+
+/* One complex Horner step on dual numbers, (re, im) <- (re, im)(x + i y) +
+ * (b + i a), values in the reference's order (re x - im y + b,
+ * im x + re y + a) and each derivative slot of a component in four fused
+ * operations instead of five. */
+template <int K>
+__device__ __forceinline__ void horner_step_dual(Dual<K>& re, Dual<K>& im, const Dual<K>& x,
+                                                 const Dual<K>& y, double b, double a) {
+    Dual<K> nr, ni;
+    nr.v = re.v * x.v - im.v * y.v + b;
+    ni.v = im.v * x.v + re.v * y.v + a;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        nr.d[i] = fma(re.d[i], x.v, fma(re.v, x.d[i], fma(-im.d[i], y.v, -(im.v * y.d[i]))));
+        ni.d[i] = fma(im.d[i], x.v, fma(im.v, x.d[i], fma(re.d[i], y.v, re.v * y.d[i])));
+    }
+    re = nr;
+    im = ni;
+}
+
 /* sin and cos are called separately (not sincos) so the value is exactly
  * the one the double kernels compute */
 template <int K>

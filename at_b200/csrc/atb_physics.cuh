@@ -147,8 +147,8 @@ __device__ __forceinline__ void drift6(P6T<T>& r, double L) {
     } else {
         T pn = 1 / (1 + r.dp);
         T nl = L * pn;
-        r.x += nl * r.px;
-        r.y += nl * r.py;
+        r.x = madd(r.x, nl, r.px);
+        r.y = madd(r.y, nl, r.py);
         r.ct += nl * pn * (r.px * r.px + r.py * r.py) / 2;
     }
 }
@@ -156,8 +156,8 @@ __device__ __forceinline__ void drift6(P6T<T>& r, double L) {
 /* driftkick.c:37-48 fastdrift.  FAST: c2 = NormL/(2(1+delta)) precomputed. */
 template <bool FAST, class T>
 __device__ __forceinline__ void fastdrift(P6T<T>& r, const T& nl, const T& c2) {
-    r.x += nl * r.px;
-    r.y += nl * r.py;
+    r.x = madd(r.x, nl, r.px);
+    r.y = madd(r.y, nl, r.py);
     if constexpr (FAST) r.ct += c2 * (r.px * r.px + r.py * r.py);
     else r.ct += nl * (r.px * r.px + r.py * r.py) / (2 * (1 + r.dp));
 }
@@ -287,11 +287,8 @@ struct Poly<-1> {
         if constexpr (is_dual<T>::value) {
             re = (sk == mo) ? kv : b[mo];
             im = a[mo];
-            for (int i = mo - 1; i >= 0; --i) {
-                T ret = re * x - im * y + ((i == sk) ? kv : b[i]);
-                im = im * x + re * y + a[i];
-                re = ret;
-            }
+            for (int i = mo - 1; i >= 0; --i)
+                horner_step_dual(re, im, x, y, (i == sk) ? kv : b[i], a[i]);
             seed_coef(val(x), val(y), sk, re, im);
         } else {
             horner_dyn(a, b, mo, x, y, re, im);
@@ -304,8 +301,8 @@ template <class PL, class T>
 __device__ __forceinline__ void strthinkick(P6T<T>& r, const PL& pl, double L) {
     T re, im;
     pl.field(r.x, r.y, re, im);
-    r.px -= L * re;
-    r.py += L * im;
+    r.px = msub(r.px, L, re);
+    r.py = madd(r.py, L, im);
 }
 
 /* driftkick.c:51-89 bndthinkick; lirho = L*irho folded on the host */
@@ -315,8 +312,8 @@ __device__ __forceinline__ void bndthinkick(P6T<T>& r, const PL& pl, double L, d
     T re, im;
     pl.field(r.x, r.y, re, im);
     r.px -= L * (re - (r.dp - r.x * irho) * irho);
-    r.py += L * im;
-    r.ct += lirho * r.x;
+    r.py = madd(r.py, L, im);
+    r.ct = madd(r.ct, lirho, r.x);
 }
 
 /* Radiating kicks and drifts in the reference's expression order
@@ -338,8 +335,8 @@ __device__ __forceinline__ void str_kick_rad(P6T<T>& r, const PL& pl, double L, 
     p_norm = 1.0 / (1.0 + r.dp);
     r.px = xpr / p_norm;
     r.py = ypr / p_norm;
-    r.px -= L * re;
-    r.py += L * im;
+    r.px = msub(r.px, L, re);
+    r.py = madd(r.py, L, im);
 }
 
 /* diff_bnd_kick.c:101-174 with its B2perp (:85-99), bdiff == NULL */
@@ -364,8 +361,8 @@ __device__ __forceinline__ void bnd_kick_rad(P6T<T>& r, const PL& pl, double L, 
     r.px = xpr / p_norm;
     r.py = ypr / p_norm;
     r.px -= L * (re - (dp_0 - r.x * irho) * irho);
-    r.py += L * im;
-    r.ct += lirho * r.x;
+    r.py = madd(r.py, L, im);
+    r.ct = madd(r.ct, lirho, r.x);
 }
 
 /* diff_drift.c:30-43 (bdiff == NULL) */
@@ -373,8 +370,8 @@ template <class T>
 __device__ __forceinline__ void diff_drift(P6T<T>& r, double L) {
     T p_norm = 1.0 / (1.0 + r.dp);
     T NormL = L * p_norm;
-    r.x += NormL * r.px;
-    r.y += NormL * r.py;
+    r.x = madd(r.x, NormL, r.px);
+    r.y = madd(r.y, NormL, r.py);
     r.ct += NormL * p_norm * (r.px * r.px + r.py * r.py) / 2.0;
 }
 
