@@ -172,3 +172,13 @@ def test_noalloc_refuses_a_table_for_another_integrator():
                              None, None, None, None, _lib.MODE_FAST, None)
     assert rc == _lib.ATB_ERR_ARG
     assert b"another integrator" in L.atb_last_error()
+
+
+@pytest.mark.parametrize("bad", [0, 7, -3])
+def test_gpupass_rejects_unknown_integrators_before_any_device_work(bad):
+    """The argument check runs before the engine or a device is touched, with
+    the reference backend's error type and message."""
+    from at_b200 import gpupass
+    r = np.asfortranarray(np.zeros((6, 4)))
+    with pytest.raises(RuntimeError, match="SymplecticIntegrator, type %d not supported" % bad):
+        gpupass(list(rings.fodo_ring()), r, 1, energy=3e9, integrator=bad)
