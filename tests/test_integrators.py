@@ -63,9 +63,12 @@ def test_oracle_table_is_the_reference_backends(golden):
         assert oracle.integrator_table(k) == golden[k], k
 
 
-def _quad_sext():
-    return [E.Quadrupole("Q", 1.0, 3.0, NumIntSteps=1),
+def _quad_sext(rad=False):
+    line = [E.Quadrupole("Q", 1.0, 3.0, NumIntSteps=1),
             E.Sextupole("S", 0.5, 40.0, NumIntSteps=1)]
+    if rad:
+        line = list(rings.radiating(E.Lattice(line, energy=3e9, particle="electron")))
+    return line
 
 
 def _one_pass(line, k, nsteps):
@@ -76,11 +79,13 @@ def _one_pass(line, k, nsteps):
     return r[:, 0].copy()
 
 
+@pytest.mark.parametrize("rad", [False, True])
 @pytest.mark.parametrize("k", sorted(ORDERS))
-def test_oracle_orders_of_accuracy(k):
+def test_oracle_orders_of_accuracy(k, rad):
     """Halving the step divides the error of integrator k by about 2^order
-    (reference: Yoshida's method with 512 steps)."""
-    line = _quad_sext()
+    (reference: Yoshida's method with 512 steps), in plain and radiating
+    magnets."""
+    line = _quad_sext(rad)
     ref = _one_pass(line, 6, 512)
     n0 = {1: 64, 2: 16, 3: 8, 4: 8, 5: 8, 6: 4}[k]
     e1 = np.abs(_one_pass(line, k, n0) - ref).max()
