@@ -2,9 +2,18 @@
 shapes are timed with one particle per thread, then the particle counts at
 the winning shape; the winner is applied and cached with its particle count,
 and a cache entry without one is re-tuned."""
-import json
+import pytest
 
 from at_b200 import autotune
+
+
+@pytest.fixture
+def cache(monkeypatch):
+    """An in-memory tuning cache (the tests write no file)."""
+    store = {}
+    monkeypatch.setattr(autotune, "_load_cache", lambda: dict(store))
+    monkeypatch.setattr(autotune, "_store_cache", lambda c: store.update(c))
+    return store
 
 
 class FakeEngine:
@@ -23,8 +32,7 @@ def _sample(eng, cost):
     return run
 
 
-def test_two_phase_search_and_cache(tmp_path, monkeypatch):
-    monkeypatch.setenv("AT_B200_TUNE_CACHE", str(tmp_path / "t.json"))
+def test_two_phase_search_and_cache(cache):
     eng = FakeEngine()
 
     def cost(t, c, k):              # best block shape 256 x 4096; two per thread better
@@ -40,7 +48,6 @@ def test_two_phase_search_and_cache(tmp_path, monkeypatch):
                                                   for cc in autotune.SEG_CAPS}
     assert {s for s in shapes if s[2] == 2} == {(256, 4096, 2)}
     assert len(timings) == len(autotune.THREADS) * len(autotune.SEG_CAPS) + 1
-    cache = json.loads((tmp_path / "t.json").read_text())
     assert cache["dev|x"]["ppt"] == 2 and cache["dev|x"]["threads"] == 256
 
     eng2 = FakeEngine()
@@ -49,17 +56,14 @@ def test_two_phase_search_and_cache(tmp_path, monkeypatch):
     assert eng2.calls == [(256, 4096, 2)]
 
 
-def test_cache_entry_without_particle_count_is_retuned(tmp_path, monkeypatch):
-    p = tmp_path / "t.json"
-    monkeypatch.setenv("AT_B200_TUNE_CACHE", str(p))
-    p.write_text(json.dumps({"dev|y": {"threads": 128, "seg_cap": 3072, "seconds": 1.0}}))
+def test_cache_entry_without_particle_count_is_retuned(cache):
+    cache["dev|y"] = {"threads": 128, "seg_cap": 3072, "seconds": 1.0}
     eng = FakeEngine()
     t, c, k, info = autotune.tune(eng, _sample(eng, lambda t, c, k: t + c + k), key="dev|y")
     assert info != {"cached": True} and (t, c, k) == (128, 3072, 1)
 
 
-def test_explicit_candidates_and_failures(tmp_path, monkeypatch):
-    monkeypatch.setenv("AT_B200_TUNE_CACHE", str(tmp_path / "t.json"))
+def test_explicit_candidates_and_failures(cache):
     eng = FakeEngine()
 
     def cost(t, c, k):

@@ -23,7 +23,7 @@ def _free_port():
     return p
 
 
-def _worker(rank, world, port, out_path):
+def _worker(rank, world, port, results):
     import torch.distributed as dist
 
     from at_b200 import rings
@@ -41,7 +41,7 @@ def _worker(rank, world, port, out_path):
         full = shard.gather_shards(mine)
         t = shard.max_over_ranks(float(rank + 1))
         if rank == 0:
-            np.savez(out_path, full=full, t=t)
+            results.put((np.ascontiguousarray(full), float(t)))
     finally:
         dist.destroy_process_group()
 
@@ -54,20 +54,21 @@ def test_shard_bounds_match_array_split():
             assert list(np.diff(b)) == sizes
 
 
-def test_two_rank_gloo_shards_equal_single_process(tmp_path):
+def test_two_rank_gloo_shards_equal_single_process():
     from at_b200 import rings
     from oracle import oracle
 
-    out = str(tmp_path / "gathered.npz")
     port = _free_port()
     ctx = mp.get_context("spawn")
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+    results = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, results)) for r in range(2)]
     for p in procs:
         p.start()
+    full, t = results.get(timeout=300)        # rank 0's gathered state
     for p in procs:
         p.join(timeout=300)
         assert p.exitcode == 0
-    g = np.load(out)
+    g = {"full": full, "t": t}
     ring = rings.fodo_ring()
     ref = np.asfortranarray(rings.gaussian(301, seed=5) * 3.0)
     oracle.track(ring, ref, 40, energy=ring.energy, rest_energy=ring.particle.rest_energy)
