@@ -74,6 +74,11 @@ class Engine:
     def set_launch(self, threads: int = 0, seg_cap_words: int = 0, resident_max_words: int = 0,
                    rout_budget_bytes: int = 0, particles_per_thread: int = 0,
                    refill_factor: int = 0):
+        """Launch shape of the tracking kernel (0 keeps a setting): threads
+        per block, shared-memory segment and resident-table sizes in 64-bit
+        words, the refpts snapshot budget, particles per thread (1 or 2) and
+        the refill factor of prepared batches (1-64).  Refused while prepared
+        batches exist."""
         check(lib().atb_set_launch(self.h, int(threads), int(seg_cap_words),
                                    int(resident_max_words), int(rout_budget_bytes)))
         if particles_per_thread:
