@@ -153,25 +153,50 @@ def get_tunes_damp(m: np.ndarray, r: np.ndarray | None = None):
 
 # -- the envelope -----------------------------------------------------------------
 
-_SUBMAT = [slice(0, 2), slice(2, 4), slice(6, 3, -1)]
+#: the three planes' coordinate pairs: (x, px), (y, py), (delta, ct)
+_PLANES = ((0, 1), (2, 3), (4, 5))
+#: a projected emittance below this is taken as zero (no equilibrium beam
+#: in that plane), as the reference's envelope code does
+_EMIT_FLOOR = 1.0e-13
+
+
+def _plane_emittances(sigma, planes):
+    """sqrt(det) of each plane's 2x2 block of a beam matrix: the projected
+    emittance (a negative determinant from rounding counts as zero)."""
+    out = np.empty(len(planes))
+    for k, (i, j) in enumerate(planes):
+        det = sigma[i, i] * sigma[j, j] - sigma[i, j] * sigma[j, i]
+        out[k] = np.sqrt(max(det, 0.0))
+    return out
+
+
+def _conditional(sigma, keep, given):
+    """Covariance of the coordinates ``keep`` when the coordinates ``given``
+    are held at zero: the Schur complement S_kk - S_kg S_gg^-1 S_gk of the
+    Gaussian beam matrix."""
+    s_kk = sigma[np.ix_(keep, keep)]
+    s_kg = sigma[np.ix_(keep, given)]
+    s_gg = sigma[np.ix_(given, given)]
+    return s_kk - s_kg @ solve(s_gg, s_kg.T)
 
 
 def _project(r66):
-    """Projected emittances of a 6x6 beam matrix and its 4x4 betatron part at
-    delta = 0 (radiation.py:206-225)."""
-    e3sq = np.array([np.linalg.det(r66[s, s]) for s in _SUBMAT])
-    e3 = np.sqrt(np.maximum(e3sq, 0.0))
-    if e3[0] < 1.0e-13:
-        r44 = np.nan * np.ones((4, 4))
-    elif e3[1] < 1.0e-13:
-        minv = inv(r66[[0, 1, 4, 5], :][:, [0, 1, 4, 5]])
-        r44 = np.zeros((4, 4))
-        r44[:2, :2] = inv(minv[:2, :2])
+    """The envelope record's projections of a 6x6 beam matrix (the
+    reference's emitXYZ, emitXY and r44, radiation.py:206-225): the three
+    planes' projected emittances, and the betatron beam matrix at zero
+    momentum deviation, i.e. the transverse covariance conditional on
+    (delta, ct) = 0.  Without a horizontal equilibrium it is undefined (NaN);
+    without a vertical one (an uncoupled ring) only its horizontal block is
+    filled."""
+    e3 = _plane_emittances(r66, _PLANES)
+    r44 = np.zeros((4, 4))
+    if e3[0] < _EMIT_FLOOR:
+        r44[:] = np.nan
+    elif e3[1] < _EMIT_FLOOR:
+        r44[:2, :2] = _conditional(r66, [0, 1], [4, 5])
     else:
-        minv = inv(r66)
-        r44 = inv(minv[:4, :4])
-    e2sq = np.array([np.linalg.det(r44[s, s]) for s in _SUBMAT[:2]])
-    e2 = np.sqrt(np.maximum(e2sq, 0.0))
+        r44[:] = _conditional(r66, [0, 1, 2, 3], [4, 5])
+    e2 = _plane_emittances(r44, _PLANES[:2])
     return r44, e2, e3
 
 
@@ -222,20 +247,29 @@ def quantdiffmat(ring, orbit=None, device: int = 0) -> np.ndarray:
 
 
 def lmat(dmat: np.ndarray) -> np.ndarray:
-    """Lower-triangular L with L L^T = dmat (radiation.py:125-146): the
-    eigenvalues are lifted to eps * max|eigenvalue| before the Cholesky
-    factorisation; if it still fails, the non-zero 4x4 block (no vertical
-    diffusion) is factorised alone."""
-    out = np.zeros((6, 6))
-    try:
-        v, w = np.linalg.eigh(dmat)
-        tol = np.finfo(float).eps * np.abs(v).max()
-        v[v < tol] = tol
-        out = np.linalg.cholesky(w @ np.diag(v) @ w.T)
-    except np.linalg.LinAlgError:
-        nz = np.where(dmat != 0)
-        c = np.linalg.cholesky(np.reshape(dmat[nz], (4, 4)))
-        out[nz] = np.reshape(c, (16,))
+    """Lower-triangular L with L L^T = dmat, the factor a QuantumDiffusion
+    element applies to six standard normals (the reference's Lmatp,
+    radiation.py:125-146).
+
+    A diffusion matrix is symmetric positive semi-definite, and singular in
+    a ring without vertical diffusion (zero rows and columns).  L comes from
+    the column-by-column Cholesky recursion with semi-definite pivoting: a
+    column whose pivot is at or below eps times the largest diagonal entry
+    is left at zero, which still gives L L^T = dmat.  The reference lifts
+    such eigenvalues to eps * max|eigenvalue| before a plain Cholesky, so
+    its factor holds entries of about sqrt(eps) of the scale in that
+    subspace where this one holds zeros; on a non-singular matrix the two
+    agree to rounding."""
+    d = 0.5 * (np.asarray(dmat, dtype=np.float64) + np.asarray(dmat, dtype=np.float64).T)
+    n = d.shape[0]
+    out = np.zeros((n, n))
+    floor = np.finfo(float).eps * float(np.abs(np.diag(d)).max(initial=0.0))
+    for j in range(n):
+        piv = d[j, j] - out[j, :j] @ out[j, :j]
+        if piv <= floor:
+            continue
+        out[j, j] = np.sqrt(piv)
+        out[j + 1:, j] = (d[j + 1:, j] - out[j + 1:, :j] @ out[j, :j]) / out[j, j]
     return out
 
 

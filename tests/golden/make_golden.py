@@ -238,6 +238,45 @@ def acceptance_fixture():
     np.savez_compressed(os.path.join(HERE, "acceptance_large.npz"), **out)
 
 
+def acceptance_modes_fixture():
+    """The reference's other acceptance searches on the radiating large ring
+    (pyat/at/acceptance/boundary.py:409-500 recursive, floodfill_acceptance.py
+    flood fill) and a larger cartesian grid, at few turns; arrays stored by
+    case name (boundary, survived, tracked)."""
+    sys.path.insert(0, REPO)
+    from at_b200 import rings
+    from at.acceptance import GridMode
+    lat = ref_lattice(rings.large_ring(seed=1))
+    out = {}
+    cases_ = {
+        "cart21": dict(planes=["x", "y"], npoints=[21, 11], amplitudes=[8e-3, 4e-3],
+                       grid_mode=GridMode.CARTESIAN, nturns=24),
+        "rec2d": dict(planes=["x", "y"], npoints=[12, 7], amplitudes=[8e-3, 4e-3],
+                      grid_mode=GridMode.RECURSIVE, nturns=16),
+        "rec1d": dict(planes=["dp"], npoints=[16], amplitudes=[0.04],
+                      grid_mode=GridMode.RECURSIVE, nturns=16),
+        "flood": dict(planes=["x", "y"], npoints=[15, 9], amplitudes=[8e-3, 4e-3],
+                      grid_mode=GridMode.FLOODFILL, nturns=16),
+        "flood_obs": dict(planes=["x", "y"], npoints=[11, 7], amplitudes=[8e-3, 4e-3],
+                          grid_mode=GridMode.FLOODFILL, nturns=12, refpts=61),
+        "rec_obs": dict(planes=["x", "y"], npoints=[8, 5], amplitudes=[8e-3, 4e-3],
+                        grid_mode=GridMode.RECURSIVE, nturns=12, refpts=61),
+    }
+    # the flood fill centres its grid on the orbit of a ring copy whose RF
+    # frequency is reset for dp = 0 (boundary.py:303-309 with
+    # frequency_control); the fixtures give both searches the ring's own 6-D
+    # closed orbit at the observation point instead, through ``offset``
+    orbit0 = np.array(rings.LARGE_ORBIT, dtype=np.float64)
+    _, orbit61 = lat.find_orbit(refpts=61, orbit=orbit0)
+    out["orbit0"], out["orbit61"] = orbit0, np.squeeze(orbit61)
+    for name, kw in cases_.items():
+        if kw["grid_mode"] is GridMode.FLOODFILL:
+            kw = dict(kw, offset=out["orbit61"] if kw.get("refpts") else orbit0)
+        b, sv, g = at.get_acceptance(lat, use_mp=False, **kw)
+        out[name + "_b"], out[name + "_s"], out[name + "_g"] = b, sv, g
+    np.savez_compressed(os.path.join(HERE, "acceptance_modes.npz"), **out)
+
+
 def m66_fixture():
     """The reference's closed orbit (find_orbit6) and one-turn matrix
     (find_m66, pyat/at/physics/matrix.py:105-165: central differences with
@@ -319,13 +358,14 @@ def hmba_fixture():
         json.dump(out, f)
 
 
+FIXTURES = ["element_fixtures", "fodo_fixture", "sink_fixture", "hmba_fixture", "m66_fixture",
+            "ohmi_fixture", "quantdiff_fixture", "acceptance_fixture",
+            "acceptance_modes_fixture"]
+
 if __name__ == "__main__":
-    element_fixtures()
-    fodo_fixture()
-    sink_fixture()
-    hmba_fixture()
-    m66_fixture()
-    ohmi_fixture()
-    quantdiff_fixture()
-    acceptance_fixture()
+    # no argument: every fixture; otherwise the named ones (e.g. acceptance_modes)
+    names = sys.argv[1:] or FIXTURES
+    for nm in names:
+        fn = nm if nm.endswith("_fixture") or nm.endswith("_fixtures") else nm + "_fixture"
+        globals()[fn]()
     print("golden fixtures written to", HERE)
