@@ -26,7 +26,7 @@ class BatchTracker:
     returns the final coordinates and loss maps per job.
     """
 
-    def __init__(self, lattices, particles, nturns, turn0=0, mode="fast", device: int = 0,
+    def __init__(self, lattices, particles, nturns, turn0=0, mode="exact", device: int = 0,
                  tune: bool = True, graph: bool = True, tune_turns: int = 2):
         import torch
 

@@ -77,7 +77,11 @@ __global__ void atb_noalloc_tiles(AtbTile* tiles, int ntiles, int64_t np, int th
 }
 
 /* Per-device set-up (first call on each device): the device address of the
- * scratch array and the kernels' shared-memory limit. */
+ * scratch array and the kernels' shared-memory limit.  The limit is raised to
+ * the device's opt-in maximum (less 1 KiB for the kernels' static shared
+ * memory), the value atb_create sets: it is a process-wide property of the
+ * kernel, so setting anything smaller here would shrink what handles set up
+ * earlier rely on. */
 int na_setup(int device, unsigned char** out) {
     std::lock_guard<std::mutex> g(g_na_lock);
     if (g_na_ptr[device]) {
@@ -92,13 +96,14 @@ int na_setup(int device, unsigned char** out) {
     int optin = 0;
     e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (e != cudaSuccess) return na_fail(ATB_ERR_CUDA, cudaGetErrorString(e));
-    int want = std::max(2 * NA_SEG_CAP_WORDS, NA_RESIDENT_MAX_WORDS) * 8;
-    if (want > optin - 1024) return na_fail(ATB_ERR_ARG, "device shared memory too small");
+    const int want = std::max(2 * NA_SEG_CAP_WORDS, NA_RESIDENT_MAX_WORDS) * 8;
+    const int limit = optin - 1024;
+    if (want > limit) return na_fail(ATB_ERR_ARG, "device shared memory too small");
     e = cudaFuncSetAttribute(atb_track_kernel_exact, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             want);
+                             limit);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(atb_track_kernel_fast,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, want);
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
     if (e != cudaSuccess) return na_fail(ATB_ERR_CUDA, cudaGetErrorString(e));
     g_na_ptr[device] = static_cast<unsigned char*>(p);
     *out = g_na_ptr[device];
@@ -109,7 +114,8 @@ int na_setup(int device, unsigned char** out) {
 
 /* Flags a table element compiled for another integrator of the GPU call:
    this entry point runs the default tracking kernels, which have only the
-   Forest-Ruth steps; the call then fails instead of tracking it. */
+   Forest-Ruth steps.  The host reads the flag before it launches the
+   tracking, so such a call fails with the particles untouched. */
 __global__ void atb_noalloc_scan(const double* __restrict__ table,
                                  const uint32_t* __restrict__ elem_off, int nelem,
                                  int* __restrict__ status) {
@@ -135,6 +141,24 @@ extern "C" int atb_track_noalloc(int32_t device, const double* table, int64_t nw
         return na_fail(ATB_ERR_ARG, "loss map buffers missing");
     if (nelem > 0 && (elem_off_host[0] != 0 || (int64_t)elem_off_host[nelem] != nwords))
         return na_fail(ATB_ERR_ARG, "element offsets do not span the table");
+    /* the table is staged by 16-byte bulk copies and the particles and loss
+       coordinates are moved in 16-byte vectors: the caller's buffers (which
+       may come from its own sub-allocator) must allow that */
+    if ((nwords & 1) != 0)
+        return na_fail(ATB_ERR_ARG, "atb_track_noalloc: the table must hold an even number of "
+                                    "words (whole 16-byte records)");
+    if ((reinterpret_cast<uintptr_t>(table) | reinterpret_cast<uintptr_t>(r)) & 15u)
+        return na_fail(ATB_ERR_ARG, "atb_track_noalloc: table and r must be 16-byte aligned");
+    if (losses && ((reinterpret_cast<uintptr_t>(lcoord) & 15u) ||
+                   ((reinterpret_cast<uintptr_t>(lturn) | reinterpret_cast<uintptr_t>(lelem)) & 3u)))
+        return na_fail(ATB_ERR_ARG, "atb_track_noalloc: lcoord must be 16-byte and lturn/lelem "
+                                    "4-byte aligned");
+    if (nelem > 0 && (reinterpret_cast<uintptr_t>(elem_off) & 3u))
+        return na_fail(ATB_ERR_ARG, "atb_track_noalloc: elem_off must be 4-byte aligned");
+    for (int32_t i = 0; i < nelem; ++i)
+        if ((elem_off_host[i] & 1u) || elem_off_host[i + 1] < elem_off_host[i])
+            return na_fail(ATB_ERR_ARG, "atb_track_noalloc: element records must start on even "
+                                        "words (16-byte boundaries), in increasing order");
     const int64_t ntiles64 = (np + NA_THREADS - 1) / NA_THREADS;
     if (ntiles64 > ATB_NOALLOC_MAX_TILES)
         return na_fail(ATB_ERR_ARG, "atb_track_noalloc: " + std::to_string(np) +
@@ -163,7 +187,7 @@ extern "C" int atb_track_noalloc(int32_t device, const double* table, int64_t nw
         segs[0].first_elem = 0;
         segs[0].nelem = nelem;
         segs[0].word0 = 0;
-        segs[0].nwords = (int32_t)(nwords + (nwords & 1));
+        segs[0].nwords = (int32_t)nwords;
         segs[0].pad = 0;
         nseg = 1;
     } else {
@@ -179,7 +203,7 @@ extern "C" int atb_track_noalloc(int32_t device, const double* table, int64_t nw
             segs[nseg].first_elem = i;
             segs[nseg].nelem = j - i;
             segs[nseg].word0 = elem_off_host[i];
-            segs[nseg].nwords = nw + (nw & 1);
+            segs[nseg].nwords = nw;
             segs[nseg].pad = 0;
             ++nseg;
             i = j;
@@ -220,9 +244,18 @@ extern "C" int atb_track_noalloc(int32_t device, const double* table, int64_t nw
     const int ntiles = (int)ntiles64;
     AtbTile* tiles = reinterpret_cast<AtbTile*>(base + NA_TILES);
     atb_noalloc_tiles<<<(ntiles + 255) / 256, 256, 0, st>>>(tiles, ntiles, np, NA_THREADS);
-    if (nelem > 0)
-        atb_noalloc_scan<<<(nelem + 255) / 256, 256, 0, st>>>(table, elem_off, nelem,
-                                                             reinterpret_cast<int*>(base + NA_STATUS));
+    int* status = reinterpret_cast<int*>(base + NA_STATUS);
+    if (nelem > 0) {
+        /* refuse a table for another integrator before anything is tracked */
+        atb_noalloc_scan<<<(nelem + 255) / 256, 256, 0, st>>>(table, elem_off, nelem, status);
+        int s0 = 0;
+        e = cudaMemcpyAsync(&s0, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return na_fail(ATB_ERR_CUDA, cudaGetErrorString(e));
+        if (s0 & ATB_STATUS_INTEGRATOR)
+            return na_fail(ATB_ERR_ARG, "atb_track_noalloc: the table uses another integrator "
+                                        "than the default (4); use atb_track");
+    }
 
     const int smem = resident ? segs[0].nwords * 8 : 2 * NA_SEG_CAP_WORDS * 8;
     const void* fn = mode == ATB_MODE_EXACT ? (const void*)atb_track_kernel_exact
@@ -234,7 +267,6 @@ extern "C" int atb_track_noalloc(int32_t device, const double* table, int64_t nw
     const int grid = std::min(ntiles, per_sm * sms);
     const AtbJob* dj = reinterpret_cast<const AtbJob*>(base + NA_JOB);
     int* counter = reinterpret_cast<int*>(base + NA_COUNTER);
-    int* status = reinterpret_cast<int*>(base + NA_STATUS);
     if (mode == ATB_MODE_EXACT)
         atb_track_kernel_exact<<<grid, NA_THREADS, smem, st>>>(dj, tiles, ntiles, counter,
                                                                nullptr, status,
@@ -252,8 +284,5 @@ extern "C" int atb_track_noalloc(int32_t device, const double* table, int64_t nw
     if (e != cudaSuccess) return na_fail(ATB_ERR_CUDA, cudaGetErrorString(e));
     if (s & ATB_STATUS_WAIT_TIMEOUT)
         return na_fail(ATB_ERR_TIMEOUT, "a bounded shared-memory staging wait timed out");
-    if (s & ATB_STATUS_INTEGRATOR)
-        return na_fail(ATB_ERR_ARG, "atb_track_noalloc: the table uses another integrator than "
-                                    "the default (4); use atb_track");
     return ATB_OK;
 }

@@ -28,10 +28,6 @@ from . import table as T
 from .lattice import CompiledLattice
 
 
-def _misalign(flags_blocks) -> int:
-    return flags_blocks
-
-
 def element_flops(info, words, off) -> tuple[int, int]:
     """(flops, transcendental calls) per particle for one compiled element."""
     import numpy as np

@@ -57,7 +57,7 @@ class Request:
 
 class TrackingServer:
     def __init__(self, lattices: dict, hbm_budget_bytes: float = 150e9, device: int = 0,
-                 mode="fast", round_flops: float = 2e12, max_chunk: int = 512):
+                 mode="exact", round_flops: float = 2e12, max_chunk: int = 512):
         import torch
 
         self.torch = torch
@@ -172,7 +172,7 @@ class TrackingServer:
         self.lids = {}
 
 
-def serve_sequential(lattices: dict, requests: list[Request], mode="fast", device: int = 0):
+def serve_sequential(lattices: dict, requests: list[Request], mode="exact", device: int = 0):
     """The plain drop-in as a server: one blocking ``gpupass`` call per request,
     in arrival order (a request waits for all earlier ones)."""
     pending = sorted(requests, key=lambda r: r.arrival)

@@ -177,7 +177,11 @@ def gpupass(line, r_in, nturns, refpts=_defref, *, turn=0, energy=None, particle
     order, 4 Forest-Ruth 4th order (the default, the CPU engine's), 5
     McLachlan-Atela 4th order, 6 Yoshida 6th order; changing it recompiles the
     lattice even with ``reuse``.
-    ``mode`` selects "fast" (default) or "exact" arithmetic; ``stats=True``
+    ``mode`` selects "exact" (default: the reference's operation order,
+    bit-identical to the reference's C build on the +,-,*,/ path) or "fast"
+    arithmetic (FMA contraction and reciprocal reuse: about 2.5x the
+    throughput, and up to 2e-13 of each coordinate's scale from the
+    reference after one turn of a 2,000-element radiating ring); ``stats=True``
     adds per-turn survivor counts and coordinate sums as a third result.
     ``omp_num_threads``, ``bunch_spos``, ``bunch_currents``,
     ``harmonic_number`` and ``fillpattern`` are accepted for compatibility;

@@ -40,8 +40,9 @@ extern "C" {
 #define ATB_ERR_NOMEM (-4)    /* device memory budget exceeded             */
 #define ATB_ERR_NOLAT (-5)    /* unknown lattice id                        */
 
-#define ATB_MODE_EXACT 0      /* reference operation order, no FMA         */
-#define ATB_MODE_FAST 1       /* FMA + reciprocal reuse (default)          */
+#define ATB_MODE_EXACT 0      /* reference operation order, no FMA (the
+                                 Python layer's default)                  */
+#define ATB_MODE_FAST 1       /* FMA + reciprocal reuse                    */
 
 #define ATB_FLAG_ELEMENT 1    /* single-element pass: no loss marking      */
 
@@ -211,6 +212,12 @@ int atb_fp64_peak(int device, double* tflops, double* seconds);
  * held by every GPU that loads it until the process exits.  Limits: at most
  * ATB_NOALLOC_MAX_PARTICLES particles and ATB_NOALLOC_MAX_SEGS segments of 48 KB
  * (a lattice table of up to about 48 MB); larger requests return ATB_ERR_ARG.
+ * Alignment (checked, ATB_ERR_ARG otherwise; buffers from cudaMalloc always
+ * satisfy it, a caller's own sub-allocator must): `table`, `r` and `lcoord`
+ * 16-byte aligned, `elem_off`, `lturn` and `lelem` 4-byte aligned, `nwords`
+ * and every element offset even (records on 16-byte boundaries, as the
+ * lattice compiler writes them).  A table compiled for another integrator
+ * than the default is refused (ATB_ERR_ARG) before anything is tracked.
  * The first call on a device looks up the array's device address and sets the
  * kernels' shared-memory limit, so make it before any stream capture.  All
  * calls share the array: calls that overlap on the GPU (two host threads, or

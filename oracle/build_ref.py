@@ -1,7 +1,8 @@
 """Build recipe for the reference's own C tracking engine (test infrastructure).
 
-This script compiles the reference's C sources *where they lie* (default
-``/root/reference``; override with ``AT_REFERENCE``) with plain ``gcc``, using
+This script compiles the reference's C sources *where they lie* (the
+``AT_REFERENCE`` directory, else a ``reference`` checkout beside this
+repository) with plain ``gcc``, using
 the flags of the reference's ``setup.py`` (``-std=c99 -O2 -fopenmp -DPYAT``; the
 ISO C mode turns FMA contraction off, so this is the reference arithmetic).
 Outputs go only to ``oracle/_ref/`` (git-ignored):
@@ -72,7 +73,10 @@ class Element:
 
 
 def _ref_root() -> str:
-    return os.environ.get("AT_REFERENCE", "/root/reference")
+    """The reference checkout: ``AT_REFERENCE``, else the directory
+    ``reference`` beside the repository root."""
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    return os.environ.get("AT_REFERENCE", os.path.join(os.path.dirname(repo), "reference"))
 
 
 def _cflags(ref: str, openmp: bool = True) -> list[str]:

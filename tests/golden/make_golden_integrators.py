@@ -47,4 +47,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle.build_ref import _ref_root
+    main(sys.argv[1] if len(sys.argv) > 1 else _ref_root())

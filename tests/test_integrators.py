@@ -167,7 +167,8 @@ def test_gpupass_integrator_argument():
 def test_noalloc_refuses_a_table_for_another_integrator():
     """atb_track_noalloc runs the default kernels, which have only the
     Forest-Ruth steps: a raw table compiled for another integrator fails the
-    call (its header scan sets the status word) instead of tracking."""
+    call (its header scan sets the status word, read before the tracking
+    launch) and the particles stay as they were."""
     import ctypes as C
     import torch
     from at_b200 import _lib
@@ -177,12 +178,16 @@ def test_noalloc_refuses_a_table_for_another_integrator():
     off = torch.from_numpy(np.ascontiguousarray(cl.offsets).view(np.int32)).to(dev)
     off_host = np.ascontiguousarray(cl.offsets, dtype=np.uint32)
     rd = torch.from_numpy(np.ascontiguousarray(rings.gaussian(64, seed=3).T)).to(dev)
+    before = rd.clone()
     L = _lib.lib()
     rc = L.atb_track_noalloc(0, words.data_ptr(), int(cl.words.size), off_host.ctypes.data,
                              off.data_ptr(), int(cl.nelem), rd.data_ptr(), 64, 1, 0, 0,
                              None, None, None, None, _lib.MODE_FAST, None)
     assert rc == _lib.ATB_ERR_ARG
     assert b"another integrator" in L.atb_last_error()
+    torch.cuda.synchronize()
+    # refused before tracking: the particles are untouched
+    assert torch.equal(rd, before)
 
 
 @pytest.mark.parametrize("bad", [0, 7, -3])

@@ -103,3 +103,55 @@ def test_noalloc_rejects_oversize_requests():
                              None, None, None, None, _lib.MODE_FAST, None)
     assert rc == _lib.ATB_ERR_ARG
     assert b"exceed the maximum" in L.atb_last_error()
+
+
+def test_noalloc_rejects_misaligned_buffers_before_device_work():
+    """A caller's own sub-allocator may hand out buffers that are only
+    8-byte aligned; the entry point refuses them (the kernels move particles
+    in 16-byte vectors) instead of launching."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    ring = rings.fodo_ring()
+    cl = compile_lattice(ring, ring.energy, ring.particle.rest_energy)
+    words, off = _dev_lattice(torch, cl, dev)
+    buf = torch.zeros(6 * 9, dtype=torch.float64, device=dev)
+    off_host = np.ascontiguousarray(cl.offsets, dtype=np.uint32)
+    L = _lib.lib()
+    rc = L.atb_track_noalloc(0, words.data_ptr(), int(cl.words.size), off_host.ctypes.data,
+                             off.data_ptr(), int(cl.nelem), buf.data_ptr() + 8, 8, 1, 0, 0,
+                             None, None, None, None, _lib.MODE_EXACT, None)
+    assert rc == _lib.ATB_ERR_ARG
+    assert b"16-byte aligned" in L.atb_last_error()
+    assert not buf.any()
+
+
+def test_handle_path_after_noalloc_keeps_its_shared_memory_limit():
+    """The no-alloc set-up must not lower the kernels' shared-memory limit
+    that a handle relies on: after a no-alloc call, a handle keeps a 136 KB
+    table resident in shared memory (more than the no-alloc path itself
+    uses) and tracks it exactly as through the segmented pipeline."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    ring = rings.fodo_ring()
+    cl = compile_lattice(ring, ring.energy, ring.particle.rest_energy)
+    words, off = _dev_lattice(torch, cl, dev)
+    rd = torch.from_numpy(np.ascontiguousarray(rings.gaussian(512, seed=5).T)).to(dev)
+    _noalloc(torch, cl, words, off, rd, 2, 0, _losses(torch, 512, dev), _lib.MODE_EXACT)
+    torch.cuda.synchronize()
+
+    big = type(ring)(list(ring) * 4, energy=ring.energy, particle=ring.particle)
+    cbig = compile_lattice(big, big.energy, big.particle.rest_energy)
+    assert 14336 < cbig.words.size <= 20000
+    eng = Engine.get(0)
+    lid = eng.upload(cbig)
+    r0 = rings.gaussian(2048, seed=6)
+    try:
+        ra = r0.copy(order="F")
+        eng.track(lid, ra, 3, mode="exact")                   # segmented (default limits)
+        eng.set_launch(resident_max_words=20000)
+        rb = r0.copy(order="F")
+        eng.track(lid, rb, 3, mode="exact")                   # resident 136 KB table
+    finally:
+        eng.set_launch(resident_max_words=14336)
+        eng.free(lid)
+    np.testing.assert_array_equal(rb, ra)
