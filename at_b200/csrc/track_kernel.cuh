@@ -1084,7 +1084,18 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
     }
 }
 
-extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
+/* Launch bounds of the one-particle-per-thread entry: by default any block
+   size up to ATB_MAX_THREADS (which caps registers at 128 per thread); a
+   build may trade registers for resident warps with ATB_TRACK_LB (threads)
+   and ATB_TRACK_MINB (blocks per SM). */
+#ifndef ATB_TRACK_LB
+#define ATB_TRACK_LB ATB_MAX_THREADS
+#endif
+#ifndef ATB_TRACK_MINB
+#define ATB_TRACK_MINB 1
+#endif
+
+extern "C" __global__ void __launch_bounds__(ATB_TRACK_LB, ATB_TRACK_MINB)
 ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
                                        const AtbTile* __restrict__ tiles, int ntiles,
                                        int* __restrict__ tile_counter,

@@ -23,8 +23,19 @@ Outputs go only to ``oracle/_ref/`` (git-ignored):
     generate the committed golden fixtures and by CPU tests that cross-check the
     oracle against the reference when the reference tree is present.
 
-The reference's own build system is not run.  The existing atgpu backend is not
-built: it needs generated code (``atgpu/genheader.py``) and a CUDA driver.
+``oracle/_ref/pyat_full/at/tracking/gpu<EXT>`` (only with ``--atgpu``)
+    The reference's own GPU backend (``atgpu``, its CUDA flavour), built as
+    the reference's ``setup.py`` builds it with ``CUDA`` set: ``genheader.py``
+    run on a copy of ``atgpu/`` under ``oracle/_ref/atgpu_build/`` to generate
+    the kernel header, then the ``*Pass.cpp`` and runtime sources compiled with
+    ``-DPYAT -DCUDA`` and linked against ``libcuda`` (the toolkit's link stub
+    here; the driver's library where it runs) and ``libnvrtc``.  It compiles
+    its generated tracking kernel with NVRTC at run time, so it only loads on a
+    machine with a CUDA driver; the full pyat copy does not import it by itself
+    (its ``cconfig`` is built without CUDA), callers import
+    ``at.tracking.gpu`` explicitly.
+
+The reference's own build system is not run.
 """
 from __future__ import annotations
 
@@ -178,17 +189,59 @@ def build_full(ref: str, out_root: str = join(REF_OUT, "pyat_full")) -> str:
     return out_root
 
 
+ATGPU_SOURCES = ("AbstractGPU.cpp", "AbstractInterface.cpp", "PyInterface.cpp", "Lattice.cpp",
+                 "PassMethodFactory.cpp", "SymplecticIntegrator.cpp", "CudaGPU.cpp")
+
+
+def build_atgpu(ref: str, out_root: str = join(REF_OUT, "pyat_full")) -> str:
+    """The reference's CUDA backend as ``at/tracking/gpu<EXT>`` of the full
+    pyat copy (the extension ``at.tracking.gpu`` of the reference's
+    setup.py:237-253 with CUDA set)."""
+    import numpy
+
+    cuda = os.environ.get("CUDA_PATH", "/usr/local/cuda")
+    work = join(REF_OUT, "atgpu_build")
+    src = join(work, "atgpu")
+    if os.path.isdir(src):
+        shutil.rmtree(src)
+    shutil.copytree(join(ref, "atgpu"), src)
+    # the sources include ../atintegrators/atconstants.h
+    link = join(work, "atintegrators")
+    if not os.path.lexists(link):
+        os.symlink(join(ref, "atintegrators"), link)
+    # genheader.py reads atgpu/Element.h and writes atgpu/element.gpuh relative
+    # to the working directory, as the reference's setup.py runs it
+    subprocess.run([sys.executable, join("atgpu", "genheader.py")], cwd=work, check=True)
+    sources = sorted(glob.glob(join(src, "*Pass.cpp"))) + [join(src, f) for f in ATGPU_SOURCES]
+    out = join(out_root, "at", "tracking", "gpu" + EXT)
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    cmd = ["g++", "-O2", "-fPIC", "-shared", "-DPYAT", "-DCUDA", "-Wno-unused-function",
+           "-Wno-unknown-pragmas", "-I" + sysconfig.get_paths()["include"],
+           "-I" + numpy.get_include(), "-I" + join(cuda, "include"), "-I" + src, *sources,
+           "-o", out, "-L" + join(cuda, "lib64"), "-L" + join(cuda, "lib64", "stubs"),
+           "-Wl,-rpath," + join(cuda, "lib64"), "-lcuda", "-lnvrtc"]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    shutil.rmtree(work)          # build scratch (holds a link into the reference tree)
+    if p.returncode != 0:
+        raise RuntimeError("atgpu build failed:\n" + p.stderr[-4000:])
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--full", action="store_true", help="also build the full pyat copy")
+    ap.add_argument("--atgpu", action="store_true",
+                    help="also build the reference's CUDA backend into the full pyat copy")
     args = ap.parse_args(argv)
     ref = _ref_root()
     if not os.path.isdir(join(ref, "atintegrators")):
         print("reference tree not found at %s: nothing to build" % ref)
         return 0
     build_minimal(ref)
-    if args.full:
+    if args.full or args.atgpu:
         build_full(ref)
+    if args.atgpu:
+        print("atgpu ->", build_atgpu(ref))
     print("reference build ->", REF_OUT)
     return 0
 

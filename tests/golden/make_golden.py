@@ -277,6 +277,32 @@ def acceptance_modes_fixture():
     np.savez_compressed(os.path.join(HERE, "acceptance_modes.npz"), **out)
 
 
+def longrun_fixture():
+    """The two tracking workloads at their stated sizes, run by the reference's
+    own engine (OpenMP over every core of this machine): the FODO ring with
+    10,000 particles (Gaussian from seed 0) for 1000 turns, and the radiating
+    large ring with 2048 particles around its closed orbit (seed 21) for 1000
+    turns, losses on.  The inputs are regenerated from their seeds by the
+    tests (a digest of each input is stored to catch a generator change)."""
+    import hashlib
+    sys.path.insert(0, REPO)
+    from at_b200 import rings
+    nthreads = os.cpu_count() or 1
+    for tag, ring, r0, nturns in (
+            ("fodo", rings.fodo_ring(), rings.gaussian(10000, seed=0), 1000),
+            ("large", rings.large_ring(), rings.large_ring_bunch(2048, seed=21), 1000)):
+        lat = ref_lattice(ring)
+        r = r0.copy(order="F")
+        _, ld = atpass(list(lat), r, nturns, energy=float(ring.energy),
+                       particle=at.Particle("electron"), losses=True,
+                       omp_num_threads=nthreads)
+        np.savez_compressed(os.path.join(HERE, "longrun_%s.npz" % tag),
+                            rin_sha256=np.frombuffer(hashlib.sha256(
+                                np.ascontiguousarray(r0).tobytes()).digest(), dtype=np.uint8),
+                            nturns=nturns, rout_final=r, islost=ld["islost"], lturn=ld["turn"],
+                            lelem=ld["elem"], lcoord=ld["coord"])
+
+
 def m66_fixture():
     """The reference's closed orbit (find_orbit6) and one-turn matrix
     (find_m66, pyat/at/physics/matrix.py:105-165: central differences with
@@ -360,7 +386,7 @@ def hmba_fixture():
 
 FIXTURES = ["element_fixtures", "fodo_fixture", "sink_fixture", "hmba_fixture", "m66_fixture",
             "ohmi_fixture", "quantdiff_fixture", "acceptance_fixture",
-            "acceptance_modes_fixture"]
+            "acceptance_modes_fixture", "longrun_fixture"]
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones (e.g. acceptance_modes)
