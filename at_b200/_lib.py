@@ -65,6 +65,7 @@ _SIGS = {
                           _i32, _vp], C.c_int),
     "atb_track_batch": ([_vp, C.POINTER(AtbJobDesc), _i32, _i32, _vp], C.c_int),
     "atb_element_maps": ([_vp, _i32, _vp, _vp, _vp, C.c_double, _vp], C.c_int),
+    "atb_element_pass": ([_vp, _i32, _vp, _vp, _vp, _vp], C.c_int),
     "atb_tangent_device": ([_vp, _i32, _vp, _i64, _i32, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _vp,
                             _vp], C.c_int),
     "atb_sync": ([_vp, _vp], C.c_int),

@@ -879,6 +879,33 @@ int atb_element_maps(atb_handle* h, int32_t id, const double* orbits, double* m6
     return ATB_OK;
 }
 
+int atb_element_pass(atb_handle* h, int32_t id, const double* r_in, double* r_out, double* m66,
+                     void* stream) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Lattice* L = get_lat(h, id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    if (L->nelem == 0) return ATB_OK;
+    if (!r_in || !r_out) return fail(ATB_ERR_ARG, "NULL buffer");
+    for (int e = 0; e < L->nelem; ++e)
+        if ((L->hdr[e] >> ATB_H_FL_SHIFT) & ATB_F_INTEG)
+            return fail(ATB_ERR_ARG, "element passes need a lattice compiled for the default "
+                                     "integrator (4)");
+    DeviceGuard g(h->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    AtbElemMaps A;
+    std::memset(&A, 0, sizeof(A));
+    A.table = L->words.as<double>();
+    A.elem_off = L->doff.as<uint32_t>();
+    A.nelem = L->nelem;
+    A.orbits = r_in;
+    A.m66 = m66;
+    A.exits = r_out;
+    const int blocks = (L->nelem + ATB_TANGENT_THREADS - 1) / ATB_TANGENT_THREADS;
+    atb_element_maps_kernel<<<blocks, ATB_TANGENT_THREADS, 0, st>>>(A);
+    ATB_CUDA(cudaGetLastError());
+    return ATB_OK;
+}
+
 int atb_tangent_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t nturns,
                        int32_t turn0, const int32_t* param_elem, const int32_t* param_order,
                        const double* param_value, int32_t nparam, double* jac, double* grad,

@@ -265,8 +265,9 @@ atb_element_maps_kernel(const AtbElemMaps A) {
     e.opt = hp[1];
     const double* o = A.orbits + 6 * (long long)i;
 
-    /* transfer matrix: the element on dual numbers seeded with the identity */
-    {
+    /* transfer matrix: the element on dual numbers seeded with the identity
+       (their values are the exact-arithmetic exit coordinates) */
+    if (A.m66 || A.exits) {
         P6T<TD> r;
         r.x = TD(o[0]); r.px = TD(o[1]); r.y = TD(o[2]);
         r.py = TD(o[3]); r.dp = TD(o[4]); r.ct = TD(o[5]);
@@ -274,13 +275,21 @@ atb_element_maps_kernel(const AtbElemMaps A) {
         r.py.d[3] = 1.0; r.dp.d[4] = 1.0; r.ct.d[5] = 1.0;
         track_element(r, e, 0);
         TD* rows[6] = ATB_ROWS(r);
-        double* m = A.m66 + 36 * (long long)i;
+        if (A.m66) {
+            double* m = A.m66 + 36 * (long long)i;
 #pragma unroll
-        for (int a = 0; a < 6; ++a) {
+            for (int a = 0; a < 6; ++a) {
 #pragma unroll
-            for (int b = 0; b < 6; ++b) m[6 * a + b] = rows[a]->d[b];
+                for (int b = 0; b < 6; ++b) m[6 * a + b] = rows[a]->d[b];
+            }
+        }
+        if (A.exits) {
+            double* x = A.exits + 6 * (long long)i;
+#pragma unroll
+            for (int a = 0; a < 6; ++a) x[a] = rows[a]->v;
         }
     }
+    if (!A.b66) return;
     /* diffusion matrix */
     double B[36];
     for (int k = 0; k < 36; ++k) B[k] = 0.0;

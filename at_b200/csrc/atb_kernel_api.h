@@ -115,6 +115,7 @@ typedef struct AtbElemMaps {
     double* m66;                /* (nelem, 6, 6) row-major: d out_i / d in_j */
     double* b66;                /* (nelem, 6, 6) row-major diffusion matrix */
     double diff_const;          /* DIF_CONST * gamma^5                      */
+    double* exits;              /* (nelem, 6) exit coordinates, or NULL     */
 } AtbElemMaps;
 
 #endif /* ATB_KERNEL_API_H */

@@ -173,6 +173,13 @@ class Engine:
         check(lib().atb_element_maps(self.h, int(lid), orbits_ptr, m_ptr, b_ptr,
                                      float(diff_const), stream))
 
+    def element_pass(self, lid: int, rin_ptr: int, rout_ptr: int, m_ptr: int | None = None,
+                     stream: int | None = None):
+        """Enqueue every element alone on its own particle: element i tracks
+        row i of the (nelem, 6) device array at ``rin_ptr`` into ``rout_ptr``
+        (and its transfer matrix into ``m_ptr`` when given)."""
+        check(lib().atb_element_pass(self.h, int(lid), rin_ptr, rout_ptr, m_ptr, stream))
+
     def track_batch(self, jobs: list[dict], mode=None, stream: int | None = None):
         """One persistent launch over many jobs (dicts with lattice_id, r, np,
         nturns, optional turn0 and losses=(islost, lturn, lelem, lcoord)

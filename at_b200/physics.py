@@ -67,7 +67,7 @@ def energy_loss(ring, elem_track) -> float:
     return -delta * float(ring.energy)
 
 
-def _ct_guess(ring, elem_track) -> float:
+def _ct_guess(ring, elem_track, u0: float | None = None) -> float:
     """Initial ct of the orbit search: minus the synchronous time shift
     ts = c/(2 pi f) asin(U0 / V) - TimeLag of cavities sharing one frequency
     (pyat/at/physics/energy_loss.py:156-205 and orbit.py:323-330); 0 when
@@ -75,9 +75,10 @@ def _ct_guess(ring, elem_track) -> float:
     from .lattice import C0
 
     cavs = [e for e in ring if getattr(e, "PassMethod", None) == "RFCavityPass"]
-    if not cavs or elem_track is None:
+    if not cavs or (elem_track is None and u0 is None):
         return 0.0
-    u0 = energy_loss(ring, elem_track)
+    if u0 is None:
+        u0 = energy_loss(ring, elem_track)
     freqs = {float(c.Frequency) for c in cavs}
     lags = {float(getattr(c, "TimeLag", 0.0)) for c in cavs}
     if len(freqs) != 1 or len(lags) != 1:

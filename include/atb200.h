@@ -174,6 +174,18 @@ int atb_tangent_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np,
 int atb_element_maps(atb_handle* h, int32_t lattice_id, const double* orbits, double* m66,
                      double* b66, double diff_const, void* stream);
 
+/* Every element alone on its own particle (device pointers, enqueued on
+ * `stream`): element i tracks r_in[6 i .. 6 i + 5] once, in the exact
+ * arithmetic at turn 0, and writes its exit coordinates to r_out (nelem, 6)
+ * and, when m66 is not NULL, its transfer matrix (nelem, 6, 6, row-major,
+ * exact derivatives), all elements in one launch (the lattice compiled for
+ * the default integrator, ATB_ERR_ARG otherwise).  Replaces a loop of
+ * at_elempass calls, one per element (pyat/at.c:683-753), such as the
+ * radiation energy loss of pyat/at/physics/energy_loss.py:80-89 (method
+ * TRACKING: each radiating element entered at zero). */
+int atb_element_pass(atb_handle* h, int32_t lattice_id, const double* r_in, double* r_out,
+                     double* m66, void* stream);
+
 /* Many lattice variants and particle sets in one persistent launch (device
  * pointers); the tiles of the longest jobs are scheduled first. */
 int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int32_t mode,

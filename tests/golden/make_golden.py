@@ -303,6 +303,55 @@ def longrun_fixture():
                             lelem=ld["elem"], lcoord=ld["coord"])
 
 
+def optics_fixture():
+    """The reference's linopt6 (pyat/at/physics/linear.py:846-971) with
+    chromaticity at a few observation points of the radiating large ring and
+    of its own hmba.mat in 6-D, and its find_orbit6 of four error-seeded
+    large-ring variants (seeds 2-5)."""
+    import warnings
+    sys.path.insert(0, REPO)
+    from at_b200 import rings
+    out = {}
+    lat = ref_lattice(rings.large_ring(seed=1))
+    # pyat switches radiation on and off by element class (Lattice._set_6d):
+    # give the generic elements the classes a user's lattice would have
+    for i, e in enumerate(lat):
+        cls = (at.Dipole if e.PassMethod.startswith("BndMPole") else
+               at.Multipole if e.PassMethod.startswith("StrMPole") else None)
+        if cls is not None:
+            new = cls.__new__(cls)
+            for k, v in vars(e).items():
+                object.__setattr__(new, k, v)
+            lat[i] = new
+    refs = np.array([0, 1, 61, 500, 977, 1500, len(lat) - 1], dtype=np.uint32)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        e0, bd, el = at.linopt6(lat, refpts=refs, get_chrom=True)
+    out["large_refpts"] = refs
+    for k in ("alpha", "beta", "mu", "R", "A", "dispersion", "closed_orbit", "M", "s_pos"):
+        out["large_e0_" + k] = e0[k]
+        out["large_el_" + k] = el[k]
+    for k in ("tune", "chromaticity", "damping_time"):
+        out["large_bd_" + k] = bd[k]
+    for seed in (2, 3, 4, 5):
+        v = ref_lattice(rings.large_ring_variant(seed))
+        o, _ = at.find_orbit6(v)
+        out["variant%d_orbit" % seed] = o
+    hmba = at.load_mat(os.path.join(REPO, "oracle", "_ref", "pyat_full", "machine_data",
+                                    "hmba.mat"), use="RING").enable_6d(copy=True)
+    hrefs = np.array([0, 5, 40, len(hmba) - 1], dtype=np.uint32)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        e0, bd, el = at.linopt6(hmba, refpts=hrefs, get_chrom=True)
+    out["hmba_refpts"] = hrefs
+    for k in ("alpha", "beta", "mu", "dispersion", "closed_orbit", "M", "s_pos"):
+        out["hmba_el_" + k] = el[k]
+        out["hmba_e0_" + k] = e0[k]
+    for k in ("tune", "chromaticity", "damping_time"):
+        out["hmba_bd_" + k] = bd[k]
+    np.savez_compressed(os.path.join(HERE, "optics.npz"), **out)
+
+
 def m66_fixture():
     """The reference's closed orbit (find_orbit6) and one-turn matrix
     (find_m66, pyat/at/physics/matrix.py:105-165: central differences with
@@ -386,7 +435,7 @@ def hmba_fixture():
 
 FIXTURES = ["element_fixtures", "fodo_fixture", "sink_fixture", "hmba_fixture", "m66_fixture",
             "ohmi_fixture", "quantdiff_fixture", "acceptance_fixture",
-            "acceptance_modes_fixture", "longrun_fixture"]
+            "acceptance_modes_fixture", "longrun_fixture", "optics_fixture"]
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones (e.g. acceptance_modes)
