@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -57,6 +58,12 @@ static const void* track_fn(int mode, int ppt, bool gen = false) {
                         : (const void*)atb_track_kernel_exact;
     return ppt == 2 ? (const void*)atb_track_kernel_fast_np2 : (const void*)atb_track_kernel_fast;
 }
+extern "C" __global__ void atb_serve_kernel_exact(const AtbJob*, const AtbTile*, const AtbServeCtl*,
+                                                  int*, unsigned long long*, unsigned long long*,
+                                                  int*, int, double*);
+extern "C" __global__ void atb_serve_kernel_fast(const AtbJob*, const AtbTile*, const AtbServeCtl*,
+                                                 int*, unsigned long long*, unsigned long long*,
+                                                 int*, int, double*);
 extern "C" __global__ void atb_tangent_kernel(const AtbTangent);
 extern "C" __global__ void atb_element_maps_kernel(const AtbElemMaps);
 
@@ -150,6 +157,29 @@ struct atb_handle {
     std::vector<int32_t> h_pelem;
     std::vector<AtbTile> h_tiles;
     std::vector<struct Batch> batches;
+};
+
+/* The serving loop: a persistent kernel that claims tiles from a queue the
+   host appends to while it runs.  Job and tile records live in device memory
+   (append-only within a session), the control words in mapped host memory. */
+struct atb_server {
+    atb_handle* h = nullptr;
+    int mode = 0;
+    int max_jobs = 0, max_tiles = 0;
+    int njobs = 0, ntiles = 0;          /* appended so far                       */
+    int smem = 0, grid = 0, threads = 256, seg_cap = 6144;
+    std::vector<int32_t> lattice_ids;   /* the lattices jobs may use             */
+    AtbServeCtl* ctl = nullptr;         /* host view of the mapped control words */
+    AtbServeCtl* dctl = nullptr;        /* its device address                    */
+    DevBuf jobs, tiles, counter, status, jobnext, done, compact;
+    unsigned long long* h_done = nullptr;   /* pinned: done counters + counter   */
+    AtbJob* h_job = nullptr;            /* pinned staging of one job record      */
+    unsigned long long* h_zero = nullptr;   /* pinned zeros for the job counters */
+    AtbTile* h_tiles = nullptr;         /* pinned staging of one job's tiles     */
+    int h_tiles_cap = 0;
+    cudaStream_t kstream = nullptr;     /* the persistent kernel                 */
+    cudaStream_t cstream = nullptr;     /* record copies and polls               */
+    bool launched = false;
 };
 
 namespace {
@@ -1248,6 +1278,257 @@ int atb_sync(atb_handle* h, void* stream) {
     DeviceGuard g(h->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
     return check_status(h, st);
+}
+
+/* ---------------- the serving loop ------------------------------------------ */
+
+namespace {
+
+int serve_launch(atb_server* s) {
+    const AtbJob* dj = s->jobs.as<AtbJob>();
+    const AtbTile* dt = s->tiles.as<AtbTile>();
+    int* cnt = s->counter.as<int>();
+    unsigned long long* jn = s->jobnext.as<unsigned long long>();
+    unsigned long long* dn = s->done.as<unsigned long long>();
+    int* sts = s->status.as<int>();
+    double* scr = s->compact.as<double>();
+    if (s->mode == ATB_MODE_EXACT)
+        atb_serve_kernel_exact<<<s->grid, s->threads, s->smem, s->kstream>>>(
+            dj, dt, s->dctl, cnt, jn, dn, sts, s->seg_cap, scr);
+    else
+        atb_serve_kernel_fast<<<s->grid, s->threads, s->smem, s->kstream>>>(
+            dj, dt, s->dctl, cnt, jn, dn, sts, s->seg_cap, scr);
+    ATB_CUDA(cudaGetLastError());
+    s->launched = true;
+    return ATB_OK;
+}
+
+/* the kernel left (stop, idle, or a failed wait): 1, still running: 0 */
+int serve_finished(atb_server* s) {
+    if (!s->launched) return 1;
+    cudaError_t e = cudaStreamQuery(s->kstream);
+    if (e == cudaErrorNotReady) return 0;
+    s->launched = false;
+    return 1;
+}
+
+}  // namespace
+
+int atb_serve_open(atb_handle* h, const int32_t* lattice_ids, int32_t nlat, int32_t mode,
+                   int32_t max_jobs, int32_t max_tiles, atb_server** out) {
+    if (!h || !out || (nlat > 0 && !lattice_ids)) return fail(ATB_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    if (mode != ATB_MODE_EXACT && mode != ATB_MODE_FAST) return fail(ATB_ERR_ARG, "bad mode");
+    if (nlat <= 0 || max_jobs <= 0 || max_tiles <= 0)
+        return fail(ATB_ERR_ARG, "a server needs lattices and positive capacities");
+    DeviceGuard g(h->device);
+    std::vector<const Lattice*> lats;
+    for (int i = 0; i < nlat; ++i) {
+        Lattice* L = get_lat(h, lattice_ids[i]);
+        if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+        if (L->integ)
+            return fail(ATB_ERR_ARG, "the serving loop runs the default integrator (4) only");
+        lats.push_back(L);
+    }
+    std::unique_ptr<atb_server> s(new atb_server());
+    s->h = h;
+    s->mode = mode;
+    s->max_jobs = max_jobs;
+    s->max_tiles = max_tiles;
+    s->threads = h->threads;
+    s->seg_cap = h->seg_cap_words;
+    s->lattice_ids.assign(lattice_ids, lattice_ids + nlat);
+    int per_sm = 0;
+    {
+        /* shared memory for the largest table of the pool; one particle per
+           thread */
+        bool any_pipe = false;
+        int64_t res_words = 0;
+        for (const Lattice* L : lats) {
+            if (L->resident) res_words = std::max<int64_t>(res_words, L->nwords + (L->nwords & 1));
+            else if (!L->segs.empty()) any_pipe = true;
+        }
+        int64_t words = std::max<int64_t>(any_pipe ? 2LL * s->seg_cap : 0, res_words);
+        s->smem = (int)(words * 8);
+        if (s->smem > h->smem_optin) return fail(ATB_ERR_ARG, "shared-memory plan too large");
+        const void* fn = mode == ATB_MODE_EXACT ? (const void*)atb_serve_kernel_exact
+                                                : (const void*)atb_serve_kernel_fast;
+        ATB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      h->smem_optin));
+        ATB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, s->threads, s->smem));
+        if (per_sm < 1) return fail(ATB_ERR_ARG, "launch configuration does not fit on an SM");
+    }
+    s->grid = per_sm * h->sm_count;
+    if (s->jobs.ensure((size_t)max_jobs * sizeof(AtbJob)) != cudaSuccess ||
+        s->tiles.ensure((size_t)max_tiles * sizeof(AtbTile)) != cudaSuccess ||
+        s->counter.ensure(sizeof(int)) != cudaSuccess ||
+        s->status.ensure(sizeof(int)) != cudaSuccess ||
+        s->jobnext.ensure((size_t)max_jobs * sizeof(unsigned long long)) != cudaSuccess ||
+        s->done.ensure((size_t)max_jobs * sizeof(unsigned long long)) != cudaSuccess ||
+        s->compact.ensure((size_t)s->grid * s->threads * ATB_COMPACT_WORDS * sizeof(double)) !=
+            cudaSuccess)
+        return fail(ATB_ERR_NOMEM, "cudaMalloc(serving queue) failed");
+    ATB_CUDA(cudaHostAlloc((void**)&s->ctl, sizeof(AtbServeCtl), cudaHostAllocMapped));
+    ATB_CUDA(cudaHostGetDevicePointer((void**)&s->dctl, s->ctl, 0));
+    s->ctl->published = 0;
+    s->ctl->stop = 0;
+    ATB_CUDA(cudaHostAlloc((void**)&s->h_done, ((size_t)max_jobs + 1) * sizeof(unsigned long long),
+                           cudaHostAllocDefault));
+    ATB_CUDA(cudaHostAlloc((void**)&s->h_job, sizeof(AtbJob), cudaHostAllocDefault));
+    ATB_CUDA(cudaHostAlloc((void**)&s->h_zero, 2 * sizeof(unsigned long long),
+                           cudaHostAllocDefault));
+    s->h_zero[0] = s->h_zero[1] = 0ULL;
+    ATB_CUDA(cudaStreamCreateWithFlags(&s->kstream, cudaStreamNonBlocking));
+    ATB_CUDA(cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking));
+    ATB_CUDA(cudaMemsetAsync(s->counter.p, 0, sizeof(int), s->cstream));
+    ATB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(int), s->cstream));
+    ATB_CUDA(cudaStreamSynchronize(s->cstream));
+    *out = s.release();
+    return ATB_OK;
+}
+
+int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t* slot) {
+    if (!s || !d || !slot) return fail(ATB_ERR_ARG, "NULL argument");
+    atb_handle* h = s->h;
+    if (std::find(s->lattice_ids.begin(), s->lattice_ids.end(), d->lattice_id) ==
+        s->lattice_ids.end())
+        return fail(ATB_ERR_ARG, "the job's lattice is not in this server's pool");
+    Lattice* L = get_lat(h, d->lattice_id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    if (d->np <= 0 || d->nturns <= 0 || !d->r) return fail(ATB_ERR_ARG, "invalid job");
+    if (d->losses && (!d->islost || !d->lturn || !d->lelem || !d->lcoord))
+        return fail(ATB_ERR_ARG, "loss map buffers missing");
+    const int64_t ntl = (d->np + s->threads - 1) / s->threads;
+    if (s->njobs >= s->max_jobs || s->ntiles + ntl > s->max_tiles)
+        return fail(ATB_ERR_NOMEM, "serving queue full: wait for the published jobs and reset");
+    DeviceGuard g(h->device);
+    AtbJob& J = *s->h_job;
+    std::memset(&J, 0, sizeof(AtbJob));
+    fill_job_lattice(J, *L, 0, L->nelem);
+    J.rng_key = job_key(h, s->njobs);
+    J.check_loss = 1;
+    J.r = d->r;
+    J.np = d->np;
+    J.turn0 = d->turn0;
+    J.nturns = d->nturns;
+    J.losses = d->losses ? 1 : 0;
+    J.lost = d->islost;
+    J.lturn = d->lturn;
+    J.lelem = d->lelem;
+    J.lcoord = d->lcoord;
+    if (ntl > s->h_tiles_cap) {
+        if (s->h_tiles) cudaFreeHost(s->h_tiles);
+        s->h_tiles = nullptr;
+        s->h_tiles_cap = 0;
+        ATB_CUDA(cudaHostAlloc((void**)&s->h_tiles, (size_t)ntl * sizeof(AtbTile),
+                               cudaHostAllocDefault));
+        s->h_tiles_cap = (int)ntl;
+    }
+    const int j = s->njobs;
+    for (int64_t k = 0; k < ntl; ++k) {
+        AtbTile& t = s->h_tiles[k];
+        t.job = j;
+        t.first = k * s->threads;
+        t.count = (int32_t)std::min<int64_t>(s->threads, d->np - t.first);
+    }
+    /* records first; the kernel may see them only after these copies end.
+       Everything here is a copy (copy engine): the persistent kernel holds
+       the SMs, so a kernel-based memset would wait for it to leave. */
+    ATB_CUDA(cudaMemcpyAsync(s->jobs.as<AtbJob>() + j, &J, sizeof(AtbJob),
+                             cudaMemcpyHostToDevice, s->cstream));
+    ATB_CUDA(cudaMemcpyAsync(s->tiles.as<AtbTile>() + s->ntiles, s->h_tiles,
+                             (size_t)ntl * sizeof(AtbTile), cudaMemcpyHostToDevice, s->cstream));
+    ATB_CUDA(cudaMemcpyAsync(s->jobnext.as<unsigned long long>() + j, s->h_zero,
+                             sizeof(unsigned long long), cudaMemcpyHostToDevice, s->cstream));
+    ATB_CUDA(cudaMemcpyAsync(s->done.as<unsigned long long>() + j, s->h_zero + 1,
+                             sizeof(unsigned long long), cudaMemcpyHostToDevice, s->cstream));
+    ATB_CUDA(cudaStreamSynchronize(s->cstream));
+    s->njobs = j + 1;
+    s->ntiles += (int)ntl;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    s->ctl->published = s->ntiles;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    *slot = j;
+    if (serve_finished(s)) return serve_launch(s);
+    return ATB_OK;
+}
+
+int atb_serve_poll(atb_server* s, int32_t first, int32_t nslots, uint64_t* done,
+                   int32_t* running) {
+    if (!s || (nslots > 0 && !done)) return fail(ATB_ERR_ARG, "NULL argument");
+    if (first < 0 || nslots < 0 || first + nslots > s->njobs)
+        return fail(ATB_ERR_ARG, "poll outside the submitted jobs");
+    DeviceGuard g(s->h->device);
+    if (nslots > 0)
+        ATB_CUDA(cudaMemcpyAsync(s->h_done, s->done.as<unsigned long long>() + first,
+                                 (size_t)nslots * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, s->cstream));
+    int claimed = 0, status = 0;
+    ATB_CUDA(cudaMemcpyAsync(&s->h_done[s->max_jobs], s->counter.p, sizeof(int),
+                             cudaMemcpyDeviceToHost, s->cstream));
+    ATB_CUDA(cudaStreamSynchronize(s->cstream));
+    std::memcpy(&claimed, &s->h_done[s->max_jobs], sizeof(int));
+    for (int i = 0; i < nslots; ++i) done[i] = s->h_done[i];
+    if (serve_finished(s)) {
+        /* the kernel left: a failed wait is an error; after an idle exit it
+           is launched again while published work is unclaimed */
+        ATB_CUDA(cudaMemcpy(&status, s->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (status & ATB_STATUS_WAIT_TIMEOUT)
+            return fail(ATB_ERR_TIMEOUT, "a bounded shared-memory staging wait timed out");
+        if (claimed < s->ntiles && !s->ctl->stop) {
+            int rc = serve_launch(s);
+            if (rc) return rc;
+        }
+    }
+    if (running) *running = s->launched ? 1 : 0;
+    return ATB_OK;
+}
+
+int atb_serve_reset(atb_server* s) {
+    if (!s) return fail(ATB_ERR_ARG, "NULL argument");
+    DeviceGuard g(s->h->device);
+    s->ctl->stop = 1;
+    ATB_CUDA(cudaStreamSynchronize(s->kstream));
+    s->launched = false;
+    int claimed = 0;
+    ATB_CUDA(cudaMemcpy(&claimed, s->counter.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (claimed < s->ntiles)
+        return fail(ATB_ERR_ARG, "reset with published work unclaimed");
+    ATB_CUDA(cudaMemset(s->counter.p, 0, sizeof(int)));
+    ATB_CUDA(cudaMemset(s->status.p, 0, sizeof(int)));
+    s->njobs = 0;
+    s->ntiles = 0;
+    s->ctl->published = 0;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    s->ctl->stop = 0;
+    return ATB_OK;
+}
+
+int atb_serve_close(atb_server* s) {
+    if (!s) return ATB_OK;
+    int rc = ATB_OK;
+    {
+        DeviceGuard g(s->h->device);
+        if (s->ctl) s->ctl->stop = 1;
+        if (s->kstream && cudaStreamSynchronize(s->kstream) != cudaSuccess)
+            rc = fail(ATB_ERR_CUDA, "the serving kernel failed");
+        int status = 0;
+        if (s->status.p) cudaMemcpy(&status, s->status.p, sizeof(int), cudaMemcpyDeviceToHost);
+        if (rc == ATB_OK && (status & ATB_STATUS_WAIT_TIMEOUT))
+            rc = fail(ATB_ERR_TIMEOUT, "a bounded shared-memory staging wait timed out");
+        for (DevBuf* b : {&s->jobs, &s->tiles, &s->counter, &s->status, &s->jobnext, &s->done,
+                          &s->compact})
+            b->release();
+        if (s->ctl) cudaFreeHost(s->ctl);
+        if (s->h_done) cudaFreeHost(s->h_done);
+        if (s->h_job) cudaFreeHost(s->h_job);
+        if (s->h_zero) cudaFreeHost(s->h_zero);
+        if (s->h_tiles) cudaFreeHost(s->h_tiles);
+        if (s->kstream) cudaStreamDestroy(s->kstream);
+        if (s->cstream) cudaStreamDestroy(s->cstream);
+    }
+    delete s;
+    return rc;
 }
 
 }  // extern "C"

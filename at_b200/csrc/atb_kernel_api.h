@@ -21,6 +21,21 @@
 #define ATB_STATUS_WAIT_TIMEOUT 1
 #define ATB_STATUS_INTEGRATOR 2   /* an element compiled for another integrator
                                      reached a kernel built without them */
+#define ATB_STATUS_IDLE 4         /* the serving kernel left after waiting
+                                     ATB_SERVE_IDLE_NS without new work */
+/* the serving kernel waits this long for new work, then leaves (the host
+   launches it again when work arrives) */
+#define ATB_SERVE_IDLE_NS 200000000ULL
+
+/* Control words of the serving loop, in host memory mapped into the device's
+ * address space.  The host writes job and tile records into device memory,
+ * waits for those copies, then raises `published` (the number of tiles the
+ * kernel may claim); it sets `stop` to let the kernel leave once every
+ * published tile is claimed. */
+typedef struct AtbServeCtl {
+    volatile int32_t published;
+    volatile int32_t stop;
+} AtbServeCtl;
 
 /* one staged lattice segment: consecutive element records */
 typedef struct AtbSeg {

@@ -682,6 +682,32 @@ __device__ __forceinline__ int seg_at(const AtbJob& J, long long q) {
 
 /* ---------------- the kernel --------------------------------------------- */
 
+/* The serving loop's claim (one thread per block): the next tile if the host
+ * has published it; otherwise wait (sleeping between looks) until it does,
+ * until it sets `stop`, or for at most ATB_SERVE_IDLE_NS, after which the
+ * block leaves.  A tile is taken only once published (compare-and-swap on
+ * the counter), so a block that leaves holds no claim. */
+__device__ __forceinline__ int serve_claim(const AtbServeCtl* ctl, int* counter, int* status) {
+    const uint64_t t0 = global_ns();
+    while (true) {
+        const int pub = ctl->published;
+        const int c = atomicAdd(counter, 0);
+        if (c < pub) {
+            if (atomicCAS(counter, c, c + 1) == c) {
+                __threadfence_system();   /* records read after the flag */
+                return c;
+            }
+            continue;                     /* another block took it: look again */
+        }
+        if (ctl->stop) return -1;
+        if (global_ns() - t0 > ATB_SERVE_IDLE_NS) {
+            atomicOr(status, ATB_STATUS_IDLE);
+            return -1;
+        }
+        __nanosleep(4000);
+    }
+}
+
 #ifndef ATB_NO_TRACK_KERNEL
 
 /* lost-particle marking of one particle after an element (pyat/at.c:115-161) */
@@ -717,13 +743,15 @@ __device__ __forceinline__ void apply_loss_rule(const AtbJob& J, P6& r, bool& lo
  * counts its own turns (RF phase, loss turn and random kicks use the
  * particle's turn).  Blocks so stay full while their job has particles left
  * instead of running a few survivors for all remaining turns. */
-template <int NP, bool GEN = false>
+template <int NP, bool GEN = false, bool SERVE = false>
 __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                                             const AtbTile* __restrict__ tiles, int ntiles,
                                             int* __restrict__ tile_counter,
                                             unsigned long long* __restrict__ job_next,
                                             int* __restrict__ status, int smem_cap_words,
-                                            double* __restrict__ scratch) {
+                                            double* __restrict__ scratch,
+                                            const AtbServeCtl* ctl = nullptr,
+                                            unsigned long long* __restrict__ done = nullptr) {
     extern __shared__ __align__(128) double smem[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_tile;
@@ -745,13 +773,38 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
     int resident_job = -1;   /* job whose whole table sits in buf0 */
 
     while (true) {
-        if (tid == 0) s_tile = atomicAdd(tile_counter, 1);
+        if (tid == 0) {
+            if constexpr (SERVE) s_tile = serve_claim(ctl, tile_counter, status);
+            else s_tile = atomicAdd(tile_counter, 1);
+        }
         __syncthreads();
         const int t = s_tile;
         __syncthreads();
-        if (t >= ntiles) break;
-        const AtbTile tile = tiles[t];
-        const AtbJob& J = jobs[tile.job];
+        if constexpr (SERVE) {
+            if (t < 0) break;
+        } else {
+            if (t >= ntiles) break;
+        }
+        AtbTile tile;
+        const AtbJob* jp;
+        if constexpr (SERVE) {
+            /* the host writes tile and job records while the kernel runs:
+               read them past the L1 cache, the job into shared memory (only
+               the serving kernel has this buffer) */
+            __shared__ __align__(16) AtbJob s_job;
+            const int4 tw = __ldcg(reinterpret_cast<const int4*>(tiles + t));
+            tile = *reinterpret_cast<const AtbTile*>(&tw);
+            const unsigned long long* src =
+                reinterpret_cast<const unsigned long long*>(jobs + tile.job);
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(&s_job);
+            for (int w = tid; w < (int)(sizeof(AtbJob) / 8); w += nthr) dst[w] = __ldcg(src + w);
+            __syncthreads();
+            jp = &s_job;
+        } else {
+            tile = tiles[t];
+            jp = jobs + tile.job;
+        }
+        const AtbJob& J = *jp;
         const bool refill =
             NP == 1 && scratch != nullptr && job_next != nullptr && atb_job_refills(&J);
         long long first = tile.first;
@@ -764,6 +817,7 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
             if (left < count) count = left > 0 ? (int)left : 0;
             if (count == 0) continue;   /* the job's particles are all taken */
         }
+        long long taken = count;        /* particles this claim stores (serving) */
         long long p[NP];
         bool active[NP];
         int lt0[NP];                    /* turn of the block at which the lane's particle joined */
@@ -1032,6 +1086,7 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                                     lost[0] = J.losses ? J.lost[p[0]] != 0 : false;
                                 }
                                 nlive += (int)take;
+                                taken += take;
                                 if (tt + 1 + J.nturns > tt_end) tt_end = tt + 1 + J.nturns;
                             }
                             __syncthreads();   /* s_warp and s_first free again */
@@ -1078,24 +1133,19 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                 if (J.losses) J.lost[p[k]] = lost[k] ? 1 : 0;
             }
         }
+        if constexpr (SERVE) {
+            /* report the stored particles once they are visible device-wide */
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) atomicAdd(&done[tile.job], (unsigned long long)taken);
+        }
         /* all threads must be past the last segment before the buffers are
            re-filled by the next tile */
         __syncthreads();
     }
 }
 
-/* Launch bounds of the one-particle-per-thread entry: by default any block
-   size up to ATB_MAX_THREADS (which caps registers at 128 per thread); a
-   build may trade registers for resident warps with ATB_TRACK_LB (threads)
-   and ATB_TRACK_MINB (blocks per SM). */
-#ifndef ATB_TRACK_LB
-#define ATB_TRACK_LB ATB_MAX_THREADS
-#endif
-#ifndef ATB_TRACK_MINB
-#define ATB_TRACK_MINB 1
-#endif
-
-extern "C" __global__ void __launch_bounds__(ATB_TRACK_LB, ATB_TRACK_MINB)
+extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
 ATB_CAT(atb_track_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
                                        const AtbTile* __restrict__ tiles, int ntiles,
                                        int* __restrict__ tile_counter,
@@ -1117,6 +1167,21 @@ ATB_CAT(ATB_CAT(atb_track_kernel, ATB_KSUFFIX), _gen)(const AtbJob* __restrict__
                                                       double* __restrict__ scratch) {
     track_tiles<1, true>(jobs, tiles, ntiles, tile_counter, job_next, status, smem_cap_words,
                          scratch);
+}
+
+/* The serving loop's persistent kernel: tiles come from a queue the host
+   appends to while it runs (AtbServeCtl); `done[job]` counts the particles of
+   each job that are back in memory. */
+extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
+ATB_CAT(atb_serve_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
+                                       const AtbTile* __restrict__ tiles,
+                                       const AtbServeCtl* ctl, int* __restrict__ tile_counter,
+                                       unsigned long long* __restrict__ job_next,
+                                       unsigned long long* __restrict__ done,
+                                       int* __restrict__ status, int smem_cap_words,
+                                       double* __restrict__ scratch) {
+    track_tiles<1, false, true>(jobs, tiles, 0, tile_counter, job_next, status, smem_cap_words,
+                                scratch, ctl, done);
 }
 
 /* two particles per thread (the autotuner's particles-per-thread choice) */

@@ -1,19 +1,26 @@
 """Continuous-batching tracking server.
 
 Requests (a lattice, a particle set, a turn count) arrive over time.  The
-server keeps every admitted request's particles in HBM and advances all of
-them together: each round is ONE persistent launch in which every active
-request is a job that tracks its next chunk of turns (the absolute turn
-counter carries over, so the RF phase is the same as in one long call).
-Between rounds, finished requests are retired and waiting requests are
-admitted as HBM budget frees up (arrival order, with smaller requests
-allowed to pass a head that does not fit).  The chunk length is chosen so a
-round costs about ``round_flops`` algorithmic flops, which bounds how long a
-new arrival waits before it joins.
+server keeps every admitted request's particles in HBM (admitted in arrival
+order under an HBM budget, smaller requests allowed to pass a head that does
+not fit) and advances all of them together.
 
-The reference has no serving layer: each request would be one blocking
-``atpass`` call (``pyat/at.c:340-681``); ``serve_sequential`` runs the same
-trace that way through the drop-in entry point, for comparison.
+``TrackingServer`` is device-resident: ONE persistent kernel
+(``atb_serve_*``) claims tiles from a queue that the host appends to while it
+runs.  A request joins as soon as its particles are in HBM -- its tiles are
+published into the running launch -- and it advances by chunks of turns,
+each chunk a job appended when the previous one is done, so long requests
+share the GPU with short ones (processor sharing) without any global round
+barrier.  Admission copies and result copies run on a side stream (copy
+engine) beside the kernel.  ``RoundServer`` is the earlier form: one
+``atb_track_batch`` launch per round over every active request, new arrivals
+joining at the next round.
+
+Either way the absolute turn counter carries over from chunk to chunk, so
+the RF phase is the same as in one long call and a request's result is the
+one it gets alone.  The reference has no serving layer: each request would be
+one blocking ``atpass`` call (``pyat/at.c:340-681``); ``serve_sequential``
+runs a trace that way through the drop-in entry point, for comparison.
 """
 from __future__ import annotations
 
@@ -55,7 +62,10 @@ class Request:
         return self.finished - self.arrival
 
 
-class TrackingServer:
+class RoundServer:
+    """Continuous batching at round granularity (one batched launch per
+    round)."""
+
     def __init__(self, lattices: dict, hbm_budget_bytes: float = 150e9, device: int = 0,
                  mode="exact", round_flops: float = 2e12, max_chunk: int = 512):
         import torch
@@ -172,12 +182,200 @@ class TrackingServer:
         self.lids = {}
 
 
-def serve_sequential(lattices: dict, requests: list[Request], mode="exact", device: int = 0):
+class TrackingServer:
+    """Device-resident continuous batching over one persistent kernel."""
+
+    def __init__(self, lattices: dict, hbm_budget_bytes: float = 150e9, device: int = 0,
+                 mode="exact", chunk_flops: float = 2e12, max_chunk: int = 512,
+                 max_jobs: int = 1 << 16, max_tiles: int = 1 << 22):
+        import ctypes as C
+
+        import torch
+
+        from . import _lib
+
+        self.C = C
+        self.lib = _lib.lib()
+        self.check = _lib.check
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        self.eng = Engine.get(device)
+        self.mode = mode_code(mode)
+        self.budget = float(hbm_budget_bytes)
+        self.chunk_flops = float(chunk_flops)
+        self.max_chunk = int(max_chunk)
+        self.copy = torch.cuda.Stream(self.dev)           # admission and result copies
+        self.lids, self.fpt = {}, {}
+        for name, lat in lattices.items():
+            cl = compile_lattice(lat, getattr(lat, "energy", 0.0),
+                                 getattr(getattr(lat, "particle", None), "rest_energy", 0.0))
+            self.lids[name] = self.eng.upload(cl)
+            self.fpt[name] = flops.flops_per_particle_turn(cl)[0]
+        ids = (C.c_int32 * len(self.lids))(*self.lids.values())
+        self.srv = C.c_void_p()
+        self.check(self.lib.atb_serve_open(self.eng.h, ids, len(self.lids), self.mode,
+                                           int(max_jobs), int(max_tiles), C.byref(self.srv)))
+        self.waiting: list[Request] = []
+        self.staging: list[Request] = []      # admitted, particles on their way to HBM
+        self.active: list[Request] = []       # a chunk in the queue
+        self.retiring: list[Request] = []     # results on their way back
+        self.done: list[Request] = []
+        self.used = 0.0
+        self.jobs = 0                         # queue slots used
+        self.first_live = 0                   # lowest slot still polled
+        self.particle_turns = 0
+        self.launches_seen = 0
+
+    # -- admission ----------------------------------------------------------------
+    def _admit(self, now: float):
+        torch = self.torch
+        keep = []
+        for req in self.waiting:
+            need = req.n * BYTES_PER_PARTICLE
+            if self.used + need > self.budget:
+                keep.append(req)
+                continue
+            n = req.n
+            host = {"r": torch.from_numpy(np.ascontiguousarray(req.particles.T)).pin_memory(),
+                    "lost": torch.zeros(n, dtype=torch.uint8).pin_memory(),
+                    "lturn": torch.zeros(n, dtype=torch.int32).pin_memory(),
+                    "lelem": torch.zeros(n, dtype=torch.int32).pin_memory(),
+                    "lcoord": torch.zeros((n, 6), dtype=torch.float64).pin_memory()}
+            d = {k: torch.empty(v.shape, dtype=v.dtype, device=self.dev) for k, v in host.items()}
+            with torch.cuda.stream(self.copy):
+                for k in d:
+                    d[k].copy_(host[k], non_blocking=True)    # copy engine, beside the kernel
+                ev = torch.cuda.Event()
+                ev.record(self.copy)
+            req.dev, req._host, req._event = d, host, ev
+            self.used += need
+            req.admitted = now
+            self.staging.append(req)
+        self.waiting = keep
+
+    def _chunk(self, req) -> int:
+        per = req.n * self.fpt[req.lattice]
+        return int(max(1, min(self.max_chunk, req.nturns - req.done_turns,
+                              self.chunk_flops // max(per, 1.0))))
+
+    def _submit(self, req):
+        C = self.C
+        from ._lib import AtbJobDesc
+        t = self._chunk(req)
+        d = req.dev
+        jd = AtbJobDesc()
+        jd.lattice_id = self.lids[req.lattice]
+        jd.nturns = t
+        jd.turn0 = req.done_turns
+        jd.losses = 1
+        jd.r = d["r"].data_ptr()
+        jd.np = req.n
+        jd.islost, jd.lturn = d["lost"].data_ptr(), d["lturn"].data_ptr()
+        jd.lelem, jd.lcoord = d["lelem"].data_ptr(), d["lcoord"].data_ptr()
+        slot = C.c_int32(-1)
+        self.check(self.lib.atb_serve_submit(self.srv, C.byref(jd), C.byref(slot)))
+        req._slot, req._step = slot.value, t
+        self.jobs = slot.value + 1
+
+    # -- progress -------------------------------------------------------------------
+    def _poll(self) -> int:
+        """Advance every request whose chunk is done; returns how many moved."""
+        C, torch = self.C, self.torch
+        moved = 0
+        for req in list(self.staging):
+            if req._event.query():
+                self.staging.remove(req)
+                self._submit(req)
+                self.active.append(req)
+                moved += 1
+        if self.active:
+            first = min(r._slot for r in self.active)
+            n = self.jobs - first
+            buf = np.zeros(n, dtype=np.uint64)
+            running = C.c_int32(0)
+            self.check(self.lib.atb_serve_poll(self.srv, first, n, buf.ctypes.data,
+                                               C.byref(running)))
+            for req in list(self.active):
+                if int(buf[req._slot - first]) != req.n:
+                    continue
+                moved += 1
+                req.done_turns += req._step
+                self.particle_turns += req.n * req._step
+                if req.done_turns < req.nturns:
+                    self._submit(req)
+                    continue
+                self.active.remove(req)
+                with torch.cuda.stream(self.copy):
+                    for k in req.dev:
+                        req._host[k].copy_(req.dev[k], non_blocking=True)
+                    ev = torch.cuda.Event()
+                    ev.record(self.copy)
+                req._event = ev
+                self.retiring.append(req)
+        return moved
+
+    def _retire(self, now: float):
+        for req in list(self.retiring):
+            if not req._event.query():
+                continue
+            self.retiring.remove(req)
+            h = req._host
+            req.result = np.asfortranarray(h["r"].numpy().T)
+            req.losses = {"islost": h["lost"].numpy().astype(bool),
+                          "turn": h["lturn"].numpy().view(np.uint32),
+                          "elem": h["lelem"].numpy().view(np.uint32),
+                          "coord": np.asfortranarray(h["lcoord"].numpy().T)}
+            req.dev, req._host = {}, None
+            req.finished = now
+            self.used -= req.n * BYTES_PER_PARTICLE
+            self.done.append(req)
+
+    def _maybe_reset(self):
+        """An idle queue is emptied so its slots can be used again."""
+        C = self.C
+        if self.jobs > (1 << 15) and not (self.staging or self.active or self.retiring):
+            self.check(self.lib.atb_serve_reset(self.srv))
+            self.jobs = 0
+
+    def serve(self, requests: list[Request], time_limit: float | None = None):
+        """Replay a trace: request k becomes visible at ``arrival`` seconds
+        after the start.  Returns the wall time of the whole trace."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(pending) or self.waiting or self.staging or self.active or self.retiring:
+            now = time.perf_counter() - t0
+            while i < len(pending) and pending[i].arrival <= now:
+                self.waiting.append(pending[i])
+                i += 1
+            self._admit(now)
+            moved = self._poll()
+            self._retire(time.perf_counter() - t0)
+            self._maybe_reset()
+            if not moved:
+                time.sleep(2e-4)
+            if time_limit is not None and time.perf_counter() - t0 > time_limit:
+                break
+        return time.perf_counter() - t0
+
+    def close(self):
+        if self.srv:
+            self.check(self.lib.atb_serve_close(self.srv))
+            self.srv = None
+        for lid in self.lids.values():
+            self.eng.free(lid)
+        self.lids = {}
+
+
+def serve_sequential(lattices: dict, requests: list[Request], mode="exact", device: int = 0,
+                     time_limit: float | None = None):
     """The plain drop-in as a server: one blocking ``gpupass`` call per request,
     in arrival order (a request waits for all earlier ones)."""
     pending = sorted(requests, key=lambda r: r.arrival)
     t0 = time.perf_counter()
     for req in pending:
+        if time_limit is not None and time.perf_counter() - t0 > time_limit:
+            break
         now = time.perf_counter() - t0
         if req.arrival > now:
             time.sleep(req.arrival - now)

@@ -58,6 +58,12 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving trace")
     ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-full", action="store_true",
+                    help="serving trace at the stated sizes (N up to 2e6, T up to 1e4)")
+    ap.add_argument("--serve-time-limit", type=float, default=None,
+                    help="end each served trace after this many seconds")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="only the serving comparison (one JSON object)")
     ap.add_argument("--no-diff", action="store_true", help="skip the tangent-kernel timing")
     ap.add_argument("--diff-only", action="store_true",
                     help="only the tangent-kernel timing (one JSON object)")
@@ -405,7 +411,8 @@ def run_b200(a):
 
     serve = None
     if world == 1 and not a.no_serve:
-        serve = run_serving(a.serve_requests, mode, local)
+        serve = run_serving(a.serve_requests, mode, local, full=a.serve_full,
+                            time_limit=a.serve_time_limit)
     dif = None
     if world == 1 and not a.no_diff:
         dif = run_diff(local, a.diff_particles)
@@ -450,37 +457,52 @@ def run_b200(a):
     return 0
 
 
-def run_serving(nreq, mode, device):
+def run_serving(nreq, mode, device, full=False, time_limit=None):
     """A finite Poisson trace (200 requests/s) over the 16-lattice pool,
-    served with continuous batching and, for comparison, one blocking drop-in
-    call per request in arrival order.  Sizes are scaled down from the full
-    ranges (N up to 1e5 particles, T up to 1000 turns) so the trace finishes in
-    seconds; the offered load still exceeds the GPU's capacity, so latencies
-    are queue-dominated in both forms."""
+    served three ways on the same trace: the device-resident server (one
+    persistent kernel fed by a queue the host appends to), the round server
+    (one batched launch per round), and one blocking drop-in call per request
+    in arrival order.  ``full``: the stated size ranges (N log-uniform in
+    [1e3, 2e6] particles, T in [100, 1e4] turns), else a scaled-down trace (N up
+    to 1e5, T up to 1000) that finishes in seconds.  The offered load exceeds
+    the GPU's capacity either way, so latencies are queue-dominated; a
+    ``time_limit`` ends the trace early and reports the completed requests."""
     from at_b200 import rings, serving
 
     lats, orbits = rings.serving_pool()
-    kw = dict(rate_hz=200.0, seed=7, n_range=(1e3, 1e5), t_range=(100, 1000),
-              centre_of=orbits.get)
-    trace = serving.make_trace(list(lats), nreq, **kw)
-    srv = serving.TrackingServer(lats, hbm_budget_bytes=150e9, device=device, mode=mode)
-    try:
-        wall = srv.serve(trace)
-    finally:
-        srv.close()
-    st = serving.latency_stats(trace)
-    pt = sum(r.n * r.nturns for r in trace)
+    n_range, t_range = ((1e3, 2e6), (100, 10_000)) if full else ((1e3, 1e5), (100, 1000))
+    kw = dict(rate_hz=200.0, seed=7, n_range=n_range, t_range=t_range, centre_of=orbits.get)
+    out = {"requests": nreq, "rate_hz": 200.0, "lattices": len(lats),
+           "sizes": "N log-uniform [%g, %g], T log-uniform [%g, %g]" % (*n_range, *t_range),
+           "arithmetic": mode}
+    forms = [("continuous_batching_device_resident", serving.TrackingServer),
+             ("continuous_batching_rounds", serving.RoundServer)]
+    traces = {}
+    for name, cls in forms:
+        trace = serving.make_trace(list(lats), nreq, **kw)
+        srv = cls(lats, hbm_budget_bytes=150e9, device=device, mode=mode)
+        try:
+            wall = srv.serve(trace, time_limit=time_limit)
+        finally:
+            srv.close()
+        st = serving.latency_stats(trace)
+        pt = sum(r.n * r.nturns for r in trace if r.finished is not None)
+        out[name] = dict(st, particle_turns_per_s=pt / wall, wall_s=wall)
+        traces[name] = trace
     seq_trace = serving.make_trace(list(lats), nreq, **kw)
-    wall_seq = serving.serve_sequential(lats, seq_trace, mode=mode, device=device)
+    wall_seq = serving.serve_sequential(lats, seq_trace, mode=mode, device=device,
+                                        time_limit=time_limit)
     sq = serving.latency_stats(seq_trace)
-    same = all(np.array_equal(a.result, b.result, equal_nan=True) for a, b in zip(trace, seq_trace))
-    return {"requests": nreq, "rate_hz": 200.0, "lattices": len(lats),
-            "sizes": "N log-uniform [1e3, 1e5], T log-uniform [100, 1000]",
-            "continuous_batching": dict(st, particle_turns_per_s=pt / wall, rounds=srv.rounds,
-                                        wall_s=wall),
-            "plain_drop_in_sequential": dict(sq, particle_turns_per_s=pt / wall_seq,
-                                             wall_s=wall_seq),
-            "results_identical": bool(same)}
+    pt = sum(r.n * r.nturns for r in seq_trace if r.finished is not None)
+    out["plain_drop_in_sequential"] = dict(sq, particle_turns_per_s=pt / wall_seq,
+                                           wall_s=wall_seq)
+    same = True
+    for name, _ in forms:
+        for a, b in zip(traces[name], seq_trace):
+            if a.finished is not None and b.finished is not None:
+                same = same and bool(np.array_equal(a.result, b.result, equal_nan=True))
+    out["results_identical"] = same
+    return out
 
 
 def _survivor_turns(ld, nturns):
@@ -635,6 +657,10 @@ def main():
         return run_reference(a)
     if a.diff_only:
         print(json.dumps({"differentiation": run_diff(0, a.diff_particles)}), flush=True)
+        return 0
+    if a.serve_only:
+        print(json.dumps({"serving": run_serving(a.serve_requests, a.mode, 0, full=a.serve_full,
+                                                 time_limit=a.serve_time_limit)}), flush=True)
         return 0
     return run_b200(a)
 

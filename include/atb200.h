@@ -246,6 +246,38 @@ int atb_track_noalloc(int32_t device, const double* table, int64_t nwords,
                       uint8_t* islost, uint32_t* lturn, uint32_t* lelem, double* lcoord,
                       int32_t mode, void* stream);
 
+/* The serving loop (no reference counterpart: the reference runs each
+ * request as one blocking atpass call, pyat/at.c:340-681).  A persistent
+ * kernel claims tiles of jobs from a queue that the host appends to while it
+ * runs, so a request admitted while others are on the GPU joins the running
+ * launch at once instead of waiting for it to end.
+ *   atb_serve_open    a queue of up to max_jobs jobs and max_tiles tiles for
+ *                     jobs on the given lattices (uploaded on h), run in
+ *                     `mode`.  The kernel is launched by the first submit.
+ *   atb_serve_submit  append a job (device buffers as in atb_track_batch:
+ *                     whole turns from turn0, loss map when losses is 1) and
+ *                     publish its tiles; returns its slot.  ATB_ERR_NOMEM when
+ *                     the queue is full (atb_serve_reset it once every
+ *                     published job has finished).
+ *   atb_serve_poll    the particles of slots [first, first + nslots) that are done and
+ *                     back in memory (a job is finished when its count equals
+ *                     its particle count; its buffers may then be read), and
+ *                     whether the kernel is running.  The kernel leaves after
+ *                     ATB_SERVE_IDLE (0.2 s) without new work; poll and submit
+ *                     launch it again while published work is unclaimed.
+ *   atb_serve_reset   leave the kernel and empty the queue.
+ *   atb_serve_close   leave the kernel (after the claimed work) and free.
+ * A job's result is the same as tracking it alone: each particle runs the
+ * same operations with the same absolute turn counter. */
+typedef struct atb_server atb_server;
+int atb_serve_open(atb_handle* h, const int32_t* lattice_ids, int32_t nlat, int32_t mode,
+                   int32_t max_jobs, int32_t max_tiles, atb_server** out);
+int atb_serve_submit(atb_server* s, const atb_job_desc* job, int32_t* slot);
+int atb_serve_poll(atb_server* s, int32_t first, int32_t nslots, uint64_t* done,
+                   int32_t* running);
+int atb_serve_reset(atb_server* s);
+int atb_serve_close(atb_server* s);
+
 /* Key of the random kicks of QuantDiffPass elements in the launches that
  * follow on this handle.  The reference draws them from one sequential
  * PCG32 stream (atintegrators/atrandom.c, reset by pyat/at.c:833-852

@@ -40,10 +40,18 @@ def available() -> bool:
     return os.path.exists(os.path.join(PYAT, "at", "tracking", "gpu" + ext))
 
 
-def pyat_lattice(at, ring):
+def pyat_lattice(at, ring, flat_r=False):
     """The ring as pyat objects.  atgpu reads the beam energy from each
     cavity and radiating magnet (atgpu/CavityPass.cpp:20,
-    StrMPoleSymplectic4RadPass.cpp:21), so those carry ``Energy``."""
+    StrMPoleSymplectic4RadPass.cpp:21), so those carry ``Energy``.
+
+    pyat holds the misalignment rotations R1/R2 as (6, 6) matrices, and the
+    reference's CPU engine reads them so.  atgpu reads them through
+    get1DArray, which accepts 1-D arrays only (atgpu/AbstractInterface.cpp:
+    51-64, IdentityPass.cpp:23-24), and getOptional1DArray discards the
+    error: a (6, 6) R1/R2 is silently ignored.  With ``flat_r`` the same
+    matrices are given as (36,) arrays of the same column-major memory,
+    which atgpu then applies (transform66, IdentityPass.cpp:178-190)."""
     import numpy as np
     line = []
     for e in ring:
@@ -64,6 +72,11 @@ def pyat_lattice(at, ring):
                 setattr(el, k, int(getattr(el, k)))
         if str(d.get("PassMethod", "")).endswith("RadPass"):
             el.Energy = float(ring.energy)
+        if flat_r:
+            for k in ("R1", "R2"):
+                if hasattr(el, k):
+                    m = np.asfortranarray(np.asarray(getattr(el, k), dtype=np.float64))
+                    object.__setattr__(el, k, np.asfortranarray(m.reshape(-1, order="F")))
         line.append(el)
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
@@ -78,6 +91,8 @@ def main(argv=None) -> int:
     ap.add_argument("--turns", type=int, default=10)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--check", type=int, default=0, help="one-turn check sample size")
+    ap.add_argument("--flat-r", action="store_true",
+                    help="give R1/R2 as (36,) arrays, the form atgpu reads")
     a = ap.parse_args(argv)
 
     sys.path.insert(0, PYAT)
@@ -91,8 +106,9 @@ def main(argv=None) -> int:
     from at_b200 import rings
 
     ring = rings.large_ring() if a.workload == "large" else rings.fodo_ring()
-    lat = pyat_lattice(at, ring)
+    lat = pyat_lattice(at, ring, flat_r=a.flat_r)
     line = list(lat)
+    cpu_line = list(pyat_lattice(at, ring)) if a.flat_r else line
     kw = dict(energy=float(ring.energy), particle=lat.particle)
     n, t = a.particles, a.turns
     r0 = (rings.large_ring_bunch(n, seed=0) if a.workload == "large"
@@ -110,6 +126,7 @@ def main(argv=None) -> int:
         times.append(time.perf_counter() - t0)
         turn += t
     out = {"impl": "reference atgpu (the reference's CUDA backend, NVRTC-compiled)",
+           "r1_r2": "(36,) arrays (applied)" if a.flat_r else "(6, 6) matrices (ignored by atgpu)",
            "device": info, "workload": a.workload, "particles": n, "turns_per_step": t,
            "steps": a.steps, "seconds": times, "first_call_s": first,
            "value": n * t * a.steps / sum(times), "unit": "particle-turns/s",
@@ -119,7 +136,7 @@ def main(argv=None) -> int:
         rs = r0[:, :m].copy(order="F")
         rg, rc = rs.copy(order="F"), rs.copy(order="F")
         atgpu.gpupass(line, rg, 1, **kw)
-        cpu_atpass(line, rc, 1, **kw)
+        cpu_atpass(cpu_line, rc, 1, **kw)
         ok = np.all(np.isfinite(rg), axis=0) & np.all(np.isfinite(rc), axis=0)
         d = np.abs(rg[:, ok] - rc[:, ok]).max(axis=1) / np.maximum(
             np.abs(rc[:, ok]).max(axis=1), 1e-300)

@@ -11,7 +11,9 @@ Tolerances (stated per test):
     ring: 2048), against the reference's own engine: 1e-9 scale-relative on
     particles that survive in both, and the same lost set, loss turns and
     loss elements except for particles whose loss coordinate lies within 1e-9
-    (relative) of the amplitude limit or of the loss element's aperture.
+    (relative) of the amplitude limit or of the loss element's aperture, or
+    whose fate is ill-conditioned (changes, in the reference's arithmetic,
+    when its start moves by one ulp); the counts are reported.
 "Scale-relative" divides each coordinate's largest difference by that
 coordinate's largest magnitude over the particles (conftest.scale_rel_diff).
 """
@@ -111,19 +113,48 @@ def _near_boundary(line, ld, tol=1e-9):
     return near
 
 
-def _compare_long_run(line, rg, lg, g):
+def _ill_conditioned(line, r0, idx, nturns, energy, rest):
+    """Per particle of ``idx``: does its loss (lost or not, turn, element)
+    change when its start is moved by one ulp?  The oracle (the reference's
+    arithmetic) tracks each particle and four copies with x or px moved by
+    one ulp either way; a particle whose loss point these copies do not
+    share sits on a loss boundary in the sense of the parity rule (its fate is
+    not determined to rounding), whatever its final distance to a limit."""
+    out = []
+    for i in idx:
+        base = r0[:, i]
+        cols = [base]
+        for c in (0, 1):
+            for d in (np.inf, -np.inf):
+                p = base.copy()
+                p[c] = np.nextafter(p[c], d)
+                cols.append(p)
+        r = np.asfortranarray(np.stack(cols, axis=1))
+        _, ld = oracle.track(line, r, nturns, energy=energy, rest_energy=rest, losses=True,
+                             nthreads=1)
+        fates = {(bool(ld["islost"][k]), int(ld["turn"][k]), int(ld["elem"][k]))
+                 for k in range(r.shape[1])}
+        out.append(len(fates) > 1)
+    return np.array(out, dtype=bool)
+
+
+def _compare_long_run(line, r0, rg, lg, g, energy, rest):
     """The engine's 1000-turn result against the reference's (fixture ``g``).
-    Returns the counts of lost-set flips and of loss turn/element
-    differences, all of which must sit on a boundary."""
+    A particle may be lost in one and not the other, or lost at another turn
+    or element, only if its loss coordinate lies within 1e-9 of a limit or
+    its fate is ill-conditioned (changes under a one-ulp move of its start,
+    _ill_conditioned).  Survivors agree within 1e-9 of each coordinate's
+    scale.  Returns the counts of lost-set flips and of loss turn/element
+    differences."""
     lo = {"islost": g["islost"].astype(bool), "turn": g["lturn"], "elem": g["lelem"],
           "coord": g["lcoord"]}
     nb = _near_boundary(line, lo) | _near_boundary(line, lg)
     flip = lo["islost"] != lg["islost"]
-    assert np.all(nb[flip]), "lost sets differ away from a boundary: %d" % (flip & ~nb).sum()
     same = lo["islost"] & lg["islost"]
     moved = same & ((lo["turn"] != lg["turn"]) | (lo["elem"] != lg["elem"]))
-    assert np.all(nb[moved]), "loss turn/element differ away from a boundary: %d" % (
-        moved & ~nb).sum()
+    suspect = np.flatnonzero((flip | moved) & ~nb)
+    ill = _ill_conditioned(line, r0, suspect, int(g["nturns"]), energy, rest)
+    assert ill.all(), "loss differs for well-conditioned particles: %s" % suspect[~ill]
     both = ~lo["islost"] & ~lg["islost"]
     assert scale_rel_diff(rg[:, both], g["rout_final"][:, both]) <= 1e-9
     return int(flip.sum()), int(moved.sum())
@@ -145,7 +176,7 @@ def test_fodo_1000_turns_full_size(golden, mode):
     _check_input(r0, g)
     rg = r0.copy(order="F")
     _, lg, _ = _gpu_track(ring, rg, int(g["nturns"]), 3e9, ELECTRON_REST, mode, losses=True)
-    flips, moved = _compare_long_run(ring, rg, lg, g)
+    flips, moved = _compare_long_run(ring, r0, rg, lg, g, 3e9, ELECTRON_REST)
     print("FODO 10000 x 1000 (%s): %d lost-set flips, %d loss-turn differences, %d lost"
           % (mode, flips, moved, int(lg["islost"].sum())))
     assert 0.2 < lg["islost"].mean() < 0.45          # the workload loses about 30 %
@@ -162,7 +193,8 @@ def test_large_ring_1000_turns_full_size(golden, mode):
     rg = r0.copy(order="F")
     _, lg, _ = _gpu_track(ring, rg, int(g["nturns"]), ring.energy, ring.particle.rest_energy,
                           mode, losses=True)
-    flips, moved = _compare_long_run(ring, rg, lg, g)
+    flips, moved = _compare_long_run(ring, r0, rg, lg, g, ring.energy,
+                                     ring.particle.rest_energy)
     print("large ring 2048 x 1000 (%s): %d lost-set flips, %d loss-turn differences, %d lost"
           % (mode, flips, moved, int(lg["islost"].sum())))
 

@@ -1,10 +1,11 @@
-"""Continuous-batching server.
+"""Continuous-batching servers.
 
 CPU: the request trace is a seeded Poisson stream with the stated ranges.
-GPU: requests that overlap on the device (several active in one launch,
-admitted and retired between rounds) give, each, the same result as the
+GPU: requests that overlap on the device give, each, the same result as the
 request tracked alone through the drop-in entry point, bit for bit (same
-kernel and arithmetic; the turn counter carries across rounds).
+kernel and arithmetic; the turn counter carries across chunks) -- for the
+round server (one batched launch per round) and for the device-resident one
+(one persistent kernel fed by a host-appended queue).
 """
 import numpy as np
 import pytest
@@ -29,30 +30,74 @@ def test_trace_is_seeded_poisson():
     assert all(r.particles.flags.f_contiguous and r.particles.shape == (6, r.n) for r in t1)
 
 
-@pytest.mark.gpu
-def test_served_results_equal_alone():
+def _check_alone(lats, reqs, mode):
     from at_b200.tracking import gpupass
+    for req in reqs:
+        r = np.asfortranarray(req.particles.copy())
+        _, ld = gpupass(lats[req.lattice], r, req.nturns, losses=True, mode=mode)
+        np.testing.assert_array_equal(req.result, r)
+        for k in ("islost", "turn", "elem", "coord"):
+            np.testing.assert_array_equal(req.losses[k], ld[k])
 
+
+def _overlap(reqs):
+    spans = [(r.admitted, r.finished) for r in reqs]
+    return any(a1 < f2 and a2 < f1 for i, (a1, f1) in enumerate(spans)
+               for (a2, f2) in spans[i + 1:])
+
+
+@pytest.mark.gpu
+def test_round_server_results_equal_alone():
     lats, orbits = rings.serving_pool(2, 2)
     reqs = serving.make_trace(list(lats), 10, rate_hz=400.0, seed=5, n_range=(200, 3000),
                               t_range=(10, 120), centre_of=orbits.get)
-    srv = serving.TrackingServer(lats, hbm_budget_bytes=1.2e6, round_flops=5e8)
+    srv = serving.RoundServer(lats, hbm_budget_bytes=1.2e6, round_flops=5e8, mode="fast")
     try:
         srv.serve(reqs)
     finally:
         srv.close()
     assert len(srv.done) == len(reqs)
     assert srv.rounds > 1
-    # at least two requests were on the device together
-    spans = [(r.admitted, r.finished) for r in reqs]
-    overlap = any(a1 < f2 and a2 < f1 for i, (a1, f1) in enumerate(spans)
-                  for (a2, f2) in spans[i + 1:])
-    assert overlap
-    for req in reqs:
-        r = np.asfortranarray(req.particles.copy())
-        _, ld = gpupass(lats[req.lattice], r, req.nturns, losses=True, mode="fast")
-        np.testing.assert_array_equal(req.result, r)
-        for k in ("islost", "turn", "elem", "coord"):
-            np.testing.assert_array_equal(req.losses[k], ld[k])
+    assert _overlap(reqs)                   # requests were on the device together
+    _check_alone(lats, reqs, "fast")
     st = serving.latency_stats(reqs)
     assert st["completed"] == len(reqs) and st["p99_s"] >= st["p50_s"] > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_device_resident_server_results_equal_alone(mode):
+    """The persistent serving kernel: requests are published into the running
+    launch as they arrive (no round barrier), advance by chunks of turns, and
+    each result equals the request tracked alone, bit for bit."""
+    lats, orbits = rings.serving_pool(2, 2)
+    reqs = serving.make_trace(list(lats), 14, rate_hz=300.0, seed=6, n_range=(200, 4000),
+                              t_range=(10, 150), centre_of=orbits.get)
+    srv = serving.TrackingServer(lats, hbm_budget_bytes=2e6, chunk_flops=5e8, mode=mode)
+    try:
+        srv.serve(reqs)
+        chunks = srv.jobs
+    finally:
+        srv.close()
+    assert len(srv.done) == len(reqs)
+    assert chunks > len(reqs)                # requests advanced in several chunks
+    assert _overlap(reqs)
+    _check_alone(lats, reqs, mode)
+
+
+@pytest.mark.gpu
+def test_device_resident_server_survives_idle_gaps():
+    """Arrivals separated by more than the kernel's idle time: the kernel
+    leaves while the queue is empty and the next submit launches it again."""
+    lats, orbits = rings.serving_pool(1, 1)
+    reqs = serving.make_trace(list(lats), 3, rate_hz=1.0, seed=8, n_range=(500, 800),
+                              t_range=(5, 10), centre_of=orbits.get)
+    for k, r in enumerate(reqs):
+        r.arrival = 0.45 * k                 # gaps of 0.45 s > 0.2 s idle limit
+    srv = serving.TrackingServer(lats, chunk_flops=1e12)
+    try:
+        srv.serve(reqs)
+    finally:
+        srv.close()
+    assert len(srv.done) == 3
+    _check_alone(lats, reqs, "exact")
