@@ -131,14 +131,18 @@ def find_orbit6(ring, guess=None, convergence: float = ORB_CONVERGENCE,
                 dp_step: float = DPSTEP, mode=None) -> np.ndarray:
     """6-D closed orbit at the ring entrance, as the reference defines it:
     M(x) = x + theta, theta the RF path-length slip of a particle with
-    beta < 1 (Newton on the one-turn map tracked by the engine)."""
-    from .tracking import elempass
+    beta < 1 (Newton on the one-turn map tracked by the engine).  The
+    synchronous-phase guess takes the radiation energy loss from one launch
+    over all elements (optics.energy_loss), equal to one elempass per
+    radiating element."""
+    from . import optics
 
-    def elem_track(e, r):
-        elempass(e, r, energy=ring.energy, particle=getattr(ring, "particle", None), mode=mode)
-
-    return _orbit6(ring, lambda r: _one_turn(ring, r, mode), guess, convergence,
-                   max_iterations, xy_step, dp_step, elem_track)
+    x0 = None
+    if guess is None:
+        x0 = np.zeros(6)
+        x0[5] = _ct_guess(ring, None, u0=optics.energy_loss(ring))
+    return _orbit6(ring, lambda r: _one_turn(ring, r, mode), guess if guess is not None else x0,
+                   convergence, max_iterations, xy_step, dp_step)
 
 
 def find_m66(ring, orbit=None, xy_step: float = XYSTEP, dp_step: float = DPSTEP,

@@ -72,7 +72,13 @@ def _args():
     ap.add_argument("--no-acceptance", action="store_true", help="skip the acceptance scan")
     ap.add_argument("--batch-turn-scale", type=float, default=0.01,
                     help="scale of the batched variants' turn counts (1.0: 500-5000 turns)")
+    ap.add_argument("--batch-sample", type=int, default=None,
+                    help="time the per-variant drop-in on this many seeded variants")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="only the batched-variant comparison (one JSON object)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fodo-line", action="store_true",
+                    help="skip the FODO (10,000 particles x 1000 turns) line")
     ap.add_argument("--no-alt-line", action="store_true",
                     help="skip timing the other arithmetic mode beside the headline's")
     return ap.parse_args()
@@ -155,6 +161,26 @@ def cpu_rate(workload, target_s=15.0, threads=None):
     return res
 
 
+def _atgpu_sample(workload, particles, turns, flat_r=False):
+    """The reference's own GPU backend (atgpu, built by oracle/build_ref.py
+    --atgpu) on the same workload, in a process of its own; None where it is
+    not built or no GPU answers."""
+    from oracle import ref_gpu_runner
+    if not ref_gpu_runner.available():
+        return None
+    cmd = [sys.executable, os.path.join(REPO, "oracle", "ref_gpu_runner.py"), workload,
+           "--particles", str(particles), "--turns", str(turns), "--steps", "2",
+           "--check", "1024"] + (["--flat-r"] if flat_r else [])
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "timed out"}
+    if out.returncode != 0:
+        return {"unavailable": out.stderr.strip().splitlines()[-1][:200] if out.stderr else
+                "exit %d" % out.returncode}
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -187,6 +213,14 @@ def run_reference(a):
                          "sample": "%d particles x 1 turn per step, %d steps" % (n, a.steps)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    # the reference's own GPU backend on the same workload, for comparison (its
+    # stock path, and with R1/R2 in the one-dimensional form it reads)
+    gpu_ref = {}
+    for tag, flat in (("stock", False), ("r1_r2_as_1d", True)):
+        if flat and a.workload != "large":
+            continue
+        gpu_ref[tag] = _atgpu_sample(a.workload, a.particles, a.turns_per_step, flat)
+    line["reference_gpu_backend"] = gpu_ref
     print(json.dumps(line), flush=True)
     return 0
 
@@ -365,7 +399,22 @@ def run_b200(a):
             xt.append(e0.elapsed_time(e1) * 1e-3)
             turn += T
         eng.sync(sptr)
+        # the same end to end through gpupass on pinned host arrays
+        hb2 = torch.empty((N, 6), dtype=torch.float64).pin_memory()
+        hb2.copy_(torch.from_numpy(np.ascontiguousarray(r0.T)))
+        rh2 = hb2.numpy().T
+        line2 = type(ring)(list(ring), energy=ring.energy, particle=ring.particle)
+        tracking.gpupass(line2, rh2, 1, losses=True, mode=alt, gpu_pool=[local])
+        et2 = []
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            tracking.gpupass(line2, rh2, T, losses=True, reuse=True, keep_counter=True,
+                             mode=alt, gpu_pool=[local])
+            et2.append(time.perf_counter() - t0)
         alt_line = {"arithmetic": alt, "value": N * T * len(xt) / sum(xt), "unit": UNIT,
+                    "e2e": {"value": N * T * len(et2) / sum(et2), "unit": UNIT,
+                            "api": "at_b200.gpupass, pinned host arrays"},
                     "ms_per_step": 1e3 * sum(xt) / len(xt), "steps": len(xt),
                     "one_turn_deviation_from_oracle":
                         "exact: <= 1e-13 of each coordinate's scale on every ring (bit-identical "
@@ -409,6 +458,10 @@ def run_b200(a):
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": "failed: %s" % str(exc)[:200]}
 
+    config0 = None
+    if world == 1 and a.workload == "large" and not a.no_fodo_line:
+        config0 = run_fodo_line(local, mode, rank == 0 and not a.no_cpu_baseline)
+
     serve = None
     if world == 1 and not a.no_serve:
         serve = run_serving(a.serve_requests, mode, local, full=a.serve_full,
@@ -418,7 +471,7 @@ def run_b200(a):
         dif = run_diff(local, a.diff_particles)
     bat = None
     if world == 1 and not a.no_batch:
-        bat = run_batching(local, mode, a.batch_turn_scale)
+        bat = run_batching(local, mode, a.batch_turn_scale, a.batch_sample)
     acc = None
     if world == 1 and not a.no_acceptance:
         acc = run_acceptance(mode, cpu)
@@ -447,6 +500,7 @@ def run_b200(a):
                          "frac_of_unfused_ceiling":
                              achieved / (fp64_peak / 2) if mode == "exact" else None},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps, "clocks": clk,
+            "config0_fodo": config0,
             "serving": serve, "differentiation": dif, "batching": bat, "acceptance": acc,
             "%s_arithmetic" % alt: alt_line,
         }
@@ -455,6 +509,68 @@ def run_b200(a):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run_fodo_line(device, mode, with_cpu):
+    """The FODO workload at its stated size: 10,000 particles (Gaussian,
+    seed 0) for 1000 turns with the loss map, device-resident (CUDA events on
+    the launching stream) and end to end through ``gpupass`` on pinned host
+    arrays; beside it the reference's own CPU engine on a sample of the same
+    ring.  10,000 particles fill only part of the GPU (one particle's chain per
+    turn bounds the time), so this line is latency-bound, not the roofline
+    case."""
+    import torch
+
+    from at_b200 import rings, tracking
+    from at_b200.engine import Engine
+    from at_b200.lattice import compile_lattice
+
+    ring = rings.fodo_ring()
+    n, nt = 10_000, 1000
+    r0 = rings.gaussian(n, seed=0)
+    dev = torch.device("cuda", device)
+    eng = Engine.get(device)
+    cl = compile_lattice(ring, ring.energy, ring.particle.rest_energy)
+    lid = eng.upload(cl)
+    st = torch.cuda.Stream(dev)
+    times = []
+    try:
+        for k in range(3):
+            rd = torch.from_numpy(np.ascontiguousarray(r0.T)).to(dev)
+            lp = tuple(torch.zeros(s, dtype=d, device=dev).data_ptr() for s, d in
+                       ((n, torch.uint8), (n, torch.int32), (n, torch.int32),
+                        ((n, 6), torch.float64)))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            eng.track_device(lid, rd.data_ptr(), n, nt, 0, losses=lp, mode=mode,
+                             stream=st.cuda_stream)
+            e1.record(st)
+            e1.synchronize()
+            eng.sync(st.cuda_stream)
+            if k:
+                times.append(e0.elapsed_time(e1) * 1e-3)
+    finally:
+        eng.free(lid)
+    hb = torch.empty((n, 6), dtype=torch.float64).pin_memory()
+    e2e = []
+    for _ in range(3):
+        hb.copy_(torch.from_numpy(np.ascontiguousarray(r0.T)))
+        rh = hb.numpy().T
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, ld = tracking.gpupass(ring, rh, nt, losses=True, mode=mode, gpu_pool=[device])
+        e2e.append(time.perf_counter() - t0)
+    out = {"workload": "FODO ring (385 elements), 10000 particles, 1000 turns, losses on",
+           "value": n * nt / min(times), "unit": UNIT, "device_s": min(times),
+           "e2e": {"value": n * nt / min(e2e[1:]), "unit": UNIT, "wall_s": min(e2e[1:]),
+                   "h2d_bytes": n * 48, "d2h_bytes": n * (48 + 57)},
+           "lost": int(ld["islost"].sum()), "arithmetic": mode}
+    if with_cpu:
+        c = cpu_rate("fodo")
+        out["cpu_baseline"] = {"value": c["rate"], "unit": UNIT, "cores": c["threads"],
+                               "kind": c["kind"], "sample": c["sample"]}
+    return out
 
 
 def run_serving(nreq, mode, device, full=False, time_limit=None):
@@ -510,13 +626,14 @@ def _survivor_turns(ld, nturns):
     return float(np.where(lost, ld["turn"].astype(np.float64) + 1.0, float(nturns)).sum())
 
 
-def run_batching(device, mode, turn_scale):
+def run_batching(device, mode, turn_scale, sample=None):
     """The batched-variant workload: 256 error-seeded copies of the large
     ring (seeds 2-257), each with N_i in [1024, 16384] particles on an x-y
     dynamic-aperture grid at delta in {-3 %, 0, +3 %} and T_i in [500, 5000]
     turns scaled by ``turn_scale``, as ONE graph-captured persistent launch
     (launch shape from the autotuner), against the plain drop-in called once
-    per variant on the same jobs."""
+    per variant on the same jobs (all of them, or a seeded sample of
+    ``sample`` variants timed and reported as a rate)."""
     from at_b200 import rings, tracking
     from at_b200.batch import BatchTracker
 
@@ -541,23 +658,28 @@ def run_batching(device, mode, turn_scale):
         bt.close()
     pt = sum(n * t for (_, n, t) in work)
     surv = sum(_survivor_turns(ld, t) for (_, ld), t in zip(res, turns))
+    ks = list(range(len(work)))
+    if sample is not None and sample < len(work):
+        ks = sorted(np.random.default_rng(1).choice(len(work), sample, replace=False).tolist())
     t0 = time.perf_counter()
     same = True
-    for k, (lat, p, t) in enumerate(zip(lats, parts, turns)):
-        r = p.copy(order="F")
-        tracking.gpupass(lat, r, t, losses=True, mode=mode, gpu_pool=[device])
-        if k % 32 == 0:
-            same = same and bool(np.array_equal(r, res[k][0], equal_nan=True))
+    for k in ks:
+        r = parts[k].copy(order="F")
+        tracking.gpupass(lats[k], r, turns[k], losses=True, mode=mode, gpu_pool=[device])
+        same = same and bool(np.array_equal(r, res[k][0], equal_nan=True))
     seq = time.perf_counter() - t0
+    pt_seq = sum(work[k][1] * work[k][2] for k in ks)
     return {"variants": len(work), "particles": int(sum(n for _, n, _ in work)),
             "turns": "U{500..5000} x %g" % turn_scale, "particle_turns": pt,
             "survivor_particle_turns": surv,
             "one_launch": {"device_s": dt, "wall_s_incl_reset": wall_batch,
                            "particle_turns_per_s": pt / dt,
                            "survivor_particle_turns_per_s": surv / dt},
-            "plain_drop_in_per_variant": {"wall_s": seq, "particle_turns_per_s": pt / seq},
+            "plain_drop_in_per_variant": {"variants_timed": len(ks), "wall_s": seq,
+                                          "particle_turns_per_s": pt_seq / seq,
+                                          "wall_s_all_variants_at_this_rate": pt / (pt_seq / seq)},
             "setup_s_compile_upload_tune_capture": setup,
-            "autotune": tuning, "results_identical_sampled": same}
+            "autotune": tuning, "results_identical": same}
 
 
 def run_acceptance(mode, cpu):
@@ -657,6 +779,10 @@ def main():
         return run_reference(a)
     if a.diff_only:
         print(json.dumps({"differentiation": run_diff(0, a.diff_particles)}), flush=True)
+        return 0
+    if a.batch_only:
+        print(json.dumps({"batching": run_batching(0, a.mode, a.batch_turn_scale,
+                                                   a.batch_sample)}), flush=True)
         return 0
     if a.serve_only:
         print(json.dumps({"serving": run_serving(a.serve_requests, a.mode, 0, full=a.serve_full,

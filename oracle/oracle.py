@@ -23,6 +23,10 @@ SRC = os.path.join(HERE, "oracle.c")
 LIB = os.path.join(HERE, "liboracle.so")
 SRC_Q = os.path.join(HERE, "oracle_q.c")
 LIB_Q = os.path.join(HERE, "liboracle_q.so")
+#: the same source with FMA contraction allowed: one rounding-level
+#: perturbation of every operation, used to tell whether a particle's fate is
+#: determined to rounding (tests only)
+LIB_FMA = os.path.join(HERE, "liboracle_fma.so")
 
 PASSES = {
     "IdentityPass": 0, "DriftPass": 1, "StrMPoleSymplectic4Pass": 2,
@@ -75,6 +79,11 @@ def build(force: bool = False) -> str:
                "-fPIC", "-shared", SRC, "-o", LIB + ".tmp", "-lm"]
         subprocess.run(cmd, check=True)
         os.replace(LIB + ".tmp", LIB)
+    if has_fma() and (force or _stale(LIB_FMA, [SRC])):
+        cmd = ["gcc", "-O2", "-std=gnu99", "-ffp-contract=fast", "-mfma", "-fno-fast-math",
+               "-fopenmp", "-fPIC", "-shared", SRC, "-o", LIB_FMA + ".tmp", "-lm"]
+        subprocess.run(cmd, check=True)
+        os.replace(LIB_FMA + ".tmp", LIB_FMA)
     if force or _stale(LIB_Q, [SRC, SRC_Q]):
         cmd = ["gcc", "-O2", "-std=gnu99", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
                "-fPIC", "-shared", SRC_Q, "-o", LIB_Q + ".tmp", "-lquadmath", "-lm"]
@@ -85,26 +94,46 @@ def build(force: bool = False) -> str:
 
 _lib = None
 _lib_q = None
+_lib_fma = None
 
 
-def _load():
-    global _lib
+def has_fma() -> bool:
+    """Whether this CPU has FMA instructions (the contracted build needs them)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            return " fma " in f.read()
+    except OSError:
+        return False
+
+
+def _load(variant: str = "reference"):
+    global _lib, _lib_fma
+    if variant == "fma":
+        if _lib_fma is None:
+            build()
+            if not os.path.exists(LIB_FMA):
+                raise RuntimeError("the FMA-contracted oracle needs a CPU with FMA")
+            _lib_fma = _bind(C.CDLL(LIB_FMA))
+        return _lib_fma
     if _lib is None:
         build()
-        L = C.CDLL(LIB)
-        f = L.oracle_track
-        f.argtypes = [C.POINTER(OElem), C.c_int, C.c_void_p, C.c_int64, C.c_int, C.c_int,
-                      C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
-                      C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                      C.c_void_p, C.c_int, C.POINTER(ORng)]
-        f.restype = C.c_int
-        L.oracle_rng_seed.argtypes = [C.POINTER(ORng), C.c_uint64, C.c_uint64]
-        L.oracle_rng_seed.restype = None
-        g = L.oracle_diffmatrix
-        g.argtypes = [C.POINTER(OElem), C.c_void_p, C.c_double, C.c_double, C.c_void_p]
-        g.restype = C.c_int
-        _lib = L
+        _lib = _bind(C.CDLL(LIB))
     return _lib
+
+
+def _bind(L):
+    f = L.oracle_track
+    f.argtypes = [C.POINTER(OElem), C.c_int, C.c_void_p, C.c_int64, C.c_int, C.c_int,
+                  C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                  C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                  C.c_void_p, C.c_int, C.POINTER(ORng)]
+    f.restype = C.c_int
+    L.oracle_rng_seed.argtypes = [C.POINTER(ORng), C.c_uint64, C.c_uint64]
+    L.oracle_rng_seed.restype = None
+    g = L.oracle_diffmatrix
+    g.argtypes = [C.POINTER(OElem), C.c_void_p, C.c_double, C.c_double, C.c_void_p]
+    g.restype = C.c_int
+    return L
 
 
 def _load_q():
@@ -180,13 +209,17 @@ def integrator_table(k: int):
 
 
 def track(line, r, nturns, refpts=None, turn=0, energy=0.0, rest_energy=0.0, losses=False,
-          start_elem=0, end_elem=None, nthreads=None, t0=None, element=False, integrator=4):
+          start_elem=0, end_elem=None, nthreads=None, t0=None, element=False, integrator=4,
+          arithmetic="reference"):
     """Track the (6, N) Fortran-ordered ``r`` in place with the C oracle.
     ``integrator`` (1-6) selects the thick multipoles' symplectic integrator
     as the reference GPU backend's gpupass does (4 is the CPU engine's).
 
+    ``arithmetic="fma"`` runs the same source compiled with FMA contraction
+    (a rounding-level perturbation of every operation; tests only).
+
     Returns ``(rout, lossdict or None)`` with the reference's layouts."""
-    lib = _load()
+    lib = _load(arithmetic)
     keep: list = []
     els = _elements(line, keep, integrator)
     nelem = len(line)

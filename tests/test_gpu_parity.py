@@ -12,8 +12,9 @@ Tolerances (stated per test):
     particles that survive in both, and the same lost set, loss turns and
     loss elements except for particles whose loss coordinate lies within 1e-9
     (relative) of the amplitude limit or of the loss element's aperture, or
-    whose fate is ill-conditioned (changes, in the reference's arithmetic,
-    when its start moves by one ulp); the counts are reported.
+    whose fate is ill-conditioned (changes when its start moves by one ulp
+    in any coordinate, or under FMA-contracted arithmetic); the counts are
+    reported.
 "Scale-relative" divides each coordinate's largest difference by that
 coordinate's largest magnitude over the particles (conftest.scale_rel_diff).
 """
@@ -114,26 +115,32 @@ def _near_boundary(line, ld, tol=1e-9):
 
 
 def _ill_conditioned(line, r0, idx, nturns, energy, rest):
-    """Per particle of ``idx``: does its loss (lost or not, turn, element)
-    change when its start is moved by one ulp?  The oracle (the reference's
-    arithmetic) tracks each particle and four copies with x or px moved by
-    one ulp either way; a particle whose loss point these copies do not
-    share sits on a loss boundary in the sense of the parity rule (its fate is
-    not determined to rounding), whatever its final distance to a limit."""
+    """Per particle of ``idx``: is its loss (lost or not, turn, element)
+    decided below the rounding level?  The oracle tracks the particle in the
+    reference's arithmetic, twelve copies with one coordinate moved by one
+    ulp either way, and the particle again in the same source compiled with
+    FMA contraction (a rounding-level change of every operation, the kind of
+    difference the engine's CUDA sin or fast arithmetic makes).  A particle
+    whose loss point these runs do not share sits on a loss boundary in the
+    sense of the parity rule, whatever its final distance to a limit."""
     out = []
     for i in idx:
         base = r0[:, i]
         cols = [base]
-        for c in (0, 1):
+        for c in range(6):
             for d in (np.inf, -np.inf):
                 p = base.copy()
                 p[c] = np.nextafter(p[c], d)
                 cols.append(p)
         r = np.asfortranarray(np.stack(cols, axis=1))
-        _, ld = oracle.track(line, r, nturns, energy=energy, rest_energy=rest, losses=True,
-                             nthreads=1)
+        _, ld = oracle.track(line, r, nturns, energy=energy, rest_energy=rest, losses=True)
         fates = {(bool(ld["islost"][k]), int(ld["turn"][k]), int(ld["elem"][k]))
                  for k in range(r.shape[1])}
+        if oracle.has_fma():
+            rf = np.asfortranarray(base.reshape(6, 1).copy())
+            _, lf = oracle.track(line, rf, nturns, energy=energy, rest_energy=rest, losses=True,
+                                 nthreads=1, arithmetic="fma")
+            fates.add((bool(lf["islost"][0]), int(lf["turn"][0]), int(lf["elem"][0])))
         out.append(len(fates) > 1)
     return np.array(out, dtype=bool)
 

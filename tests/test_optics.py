@@ -11,8 +11,9 @@ reference at tight tolerances.  GPU tests run the same functions on the
 engine.  Tolerances: closed orbits 1e-15 m (1e-13 for the batched engine
 runs); optics functions (beta, alpha, dispersion, R, A, M) 1e-9 relative to
 each array's scale; phases 1e-9 rad; tunes 1e-11; damping times 1e-8
-relative; chromaticities 1e-5 absolute (a difference of finite
-differences).
+relative; chromaticities 5e-5 absolute (a difference of two tunes divided by
+the momentum step of 3e-6, so tune rounding of a few 1e-11 alone moves it by
+1e-5).
 """
 import json
 import os
@@ -95,7 +96,8 @@ def _check_linopt(res, gold, tag, fields, orbit_tol=1e-15):
     e0, bd, el = res
     np.testing.assert_allclose(bd.tune, gold[tag + "_bd_tune"], rtol=0, atol=1e-11)
     np.testing.assert_allclose(bd.damping_time, gold[tag + "_bd_damping_time"], rtol=1e-8)
-    np.testing.assert_allclose(bd.chromaticity, gold[tag + "_bd_chromaticity"], rtol=0, atol=1e-5)
+    np.testing.assert_allclose(bd.chromaticity, gold[tag + "_bd_chromaticity"], rtol=0,
+                               atol=5e-5)
     for f in fields:
         for part, rec in (("el", el), ("e0", e0)):
             want = gold["%s_%s_%s" % (tag, part, f)]
