@@ -58,11 +58,9 @@ static const void* track_fn(int mode, int ppt, bool gen = false) {
                         : (const void*)atb_track_kernel_exact;
     return ppt == 2 ? (const void*)atb_track_kernel_fast_np2 : (const void*)atb_track_kernel_fast;
 }
-extern "C" __global__ void atb_serve_kernel_exact(const AtbJob*, const AtbTile*, const AtbServeCtl*,
-                                                  int*, unsigned long long*, unsigned long long*,
-                                                  int*, int, double*);
-extern "C" __global__ void atb_serve_kernel_fast(const AtbJob*, const AtbTile*, const AtbServeCtl*,
-                                                 int*, unsigned long long*, unsigned long long*,
+extern "C" __global__ void atb_serve_kernel_exact(const AtbJob*, const AtbTile*, AtbServeArgs,
+                                                  int*, int*, int, double*);
+extern "C" __global__ void atb_serve_kernel_fast(const AtbJob*, const AtbTile*, AtbServeArgs, int*,
                                                  int*, int, double*);
 extern "C" __global__ void atb_tangent_kernel(const AtbTangent);
 extern "C" __global__ void atb_element_maps_kernel(const AtbElemMaps);
@@ -172,7 +170,10 @@ struct atb_server {
     AtbServeCtl* ctl = nullptr;         /* host view of the mapped control words */
     AtbServeCtl* dctl = nullptr;        /* its device address                    */
     DevBuf jobs, tiles, counter, status, jobnext, done, compact;
-    unsigned long long* h_done = nullptr;   /* pinned: done counters + counter   */
+    DevBuf ring, ring_ctr;              /* continuation ring; head, tail, inflight */
+    int ring_cap = 0;
+    unsigned long long* h_done = nullptr;   /* pinned: done counters, claim counter,
+                                               ring cursors                       */
     AtbJob* h_job = nullptr;            /* pinned staging of one job record      */
     unsigned long long* h_zero = nullptr;   /* pinned zeros for the job counters */
     AtbTile* h_tiles = nullptr;         /* pinned staging of one job's tiles     */
@@ -1284,20 +1285,32 @@ int atb_sync(atb_handle* h, void* stream) {
 
 namespace {
 
+AtbServeArgs serve_args(atb_server* s) {
+    AtbServeArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = s->dctl;
+    a.ring.slots = s->ring.as<AtbServeCont>();
+    a.ring.cap = s->ring_cap;
+    a.ring.head = s->ring_ctr.as<int>();
+    a.ring.tail = s->ring_ctr.as<int>() + 1;
+    a.inflight = s->ring_ctr.as<int>() + 2;
+    a.done = s->done.as<unsigned long long>();
+    return a;
+}
+
 int serve_launch(atb_server* s) {
     const AtbJob* dj = s->jobs.as<AtbJob>();
     const AtbTile* dt = s->tiles.as<AtbTile>();
     int* cnt = s->counter.as<int>();
-    unsigned long long* jn = s->jobnext.as<unsigned long long>();
-    unsigned long long* dn = s->done.as<unsigned long long>();
     int* sts = s->status.as<int>();
     double* scr = s->compact.as<double>();
+    const AtbServeArgs a = serve_args(s);
     if (s->mode == ATB_MODE_EXACT)
         atb_serve_kernel_exact<<<s->grid, s->threads, s->smem, s->kstream>>>(
-            dj, dt, s->dctl, cnt, jn, dn, sts, s->seg_cap, scr);
+            dj, dt, a, cnt, sts, s->seg_cap, scr);
     else
         atb_serve_kernel_fast<<<s->grid, s->threads, s->smem, s->kstream>>>(
-            dj, dt, s->dctl, cnt, jn, dn, sts, s->seg_cap, scr);
+            dj, dt, a, cnt, sts, s->seg_cap, scr);
     ATB_CUDA(cudaGetLastError());
     s->launched = true;
     return ATB_OK;
@@ -1368,11 +1381,18 @@ int atb_serve_open(atb_handle* h, const int32_t* lattice_ids, int32_t nlat, int3
         s->compact.ensure((size_t)s->grid * s->threads * ATB_COMPACT_WORDS * sizeof(double)) !=
             cudaSuccess)
         return fail(ATB_ERR_NOMEM, "cudaMalloc(serving queue) failed");
+    /* continuation ring: a power of two at least the tile capacity (every
+       live tile has at most one entry) */
+    s->ring_cap = 1;
+    while (s->ring_cap < max_tiles + 128) s->ring_cap <<= 1;
+    if (s->ring.ensure((size_t)s->ring_cap * sizeof(AtbServeCont)) != cudaSuccess ||
+        s->ring_ctr.ensure(4 * sizeof(int)) != cudaSuccess)
+        return fail(ATB_ERR_NOMEM, "cudaMalloc(continuation ring) failed");
     ATB_CUDA(cudaHostAlloc((void**)&s->ctl, sizeof(AtbServeCtl), cudaHostAllocMapped));
     ATB_CUDA(cudaHostGetDevicePointer((void**)&s->dctl, s->ctl, 0));
     s->ctl->published = 0;
     s->ctl->stop = 0;
-    ATB_CUDA(cudaHostAlloc((void**)&s->h_done, ((size_t)max_jobs + 1) * sizeof(unsigned long long),
+    ATB_CUDA(cudaHostAlloc((void**)&s->h_done, ((size_t)max_jobs + 2) * sizeof(unsigned long long),
                            cudaHostAllocDefault));
     ATB_CUDA(cudaHostAlloc((void**)&s->h_job, sizeof(AtbJob), cudaHostAllocDefault));
     ATB_CUDA(cudaHostAlloc((void**)&s->h_zero, 2 * sizeof(unsigned long long),
@@ -1382,13 +1402,17 @@ int atb_serve_open(atb_handle* h, const int32_t* lattice_ids, int32_t nlat, int3
     ATB_CUDA(cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking));
     ATB_CUDA(cudaMemsetAsync(s->counter.p, 0, sizeof(int), s->cstream));
     ATB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(int), s->cstream));
+    ATB_CUDA(cudaMemsetAsync(s->ring_ctr.p, 0, 4 * sizeof(int), s->cstream));
+    ATB_CUDA(cudaMemsetAsync(s->ring.p, 0, (size_t)s->ring_cap * sizeof(AtbServeCont),
+                             s->cstream));
     ATB_CUDA(cudaStreamSynchronize(s->cstream));
     *out = s.release();
     return ATB_OK;
 }
 
-int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t* slot) {
+int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns, int32_t* slot) {
     if (!s || !d || !slot) return fail(ATB_ERR_ARG, "NULL argument");
+    if (chunk_turns < 0) return fail(ATB_ERR_ARG, "negative chunk");
     atb_handle* h = s->h;
     if (std::find(s->lattice_ids.begin(), s->lattice_ids.end(), d->lattice_id) ==
         s->lattice_ids.end())
@@ -1416,6 +1440,7 @@ int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t* slot) {
     J.lturn = d->lturn;
     J.lelem = d->lelem;
     J.lcoord = d->lcoord;
+    J.chunk = chunk_turns;
     if (ntl > s->h_tiles_cap) {
         if (s->h_tiles) cudaFreeHost(s->h_tiles);
         s->h_tiles = nullptr;
@@ -1471,16 +1496,36 @@ int atb_serve_poll(atb_server* s, int32_t first, int32_t nslots, uint64_t* done,
     for (int i = 0; i < nslots; ++i) done[i] = s->h_done[i];
     if (serve_finished(s)) {
         /* the kernel left: a failed wait is an error; after an idle exit it
-           is launched again while published work is unclaimed */
+           is launched again while published or re-enqueued work waits */
+        int ring[3] = {0, 0, 0};
         ATB_CUDA(cudaMemcpy(&status, s->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        ATB_CUDA(cudaMemcpy(ring, s->ring_ctr.p, 3 * sizeof(int), cudaMemcpyDeviceToHost));
         if (status & ATB_STATUS_WAIT_TIMEOUT)
             return fail(ATB_ERR_TIMEOUT, "a bounded shared-memory staging wait timed out");
-        if (claimed < s->ntiles && !s->ctl->stop) {
+        if ((claimed < s->ntiles || ring[0] < ring[1]) && !s->ctl->stop) {
             int rc = serve_launch(s);
             if (rc) return rc;
         }
     }
     if (running) *running = s->launched ? 1 : 0;
+    return ATB_OK;
+}
+
+int atb_serve_counters(atb_server* s, int32_t* out) {
+    if (!s || !out) return fail(ATB_ERR_ARG, "NULL argument");
+    DeviceGuard g(s->h->device);
+    int c = 0, ring[2] = {0, 0};
+    ATB_CUDA(cudaMemcpyAsync(&s->h_done[s->max_jobs], s->counter.p, sizeof(int),
+                             cudaMemcpyDeviceToHost, s->cstream));
+    ATB_CUDA(cudaMemcpyAsync(&s->h_done[s->max_jobs + 1], s->ring_ctr.p, 2 * sizeof(int),
+                             cudaMemcpyDeviceToHost, s->cstream));
+    ATB_CUDA(cudaStreamSynchronize(s->cstream));
+    std::memcpy(&c, &s->h_done[s->max_jobs], sizeof(int));
+    std::memcpy(ring, &s->h_done[s->max_jobs + 1], 2 * sizeof(int));
+    out[0] = s->ntiles;
+    out[1] = c;
+    out[2] = ring[1];
+    out[3] = ring[0];
     return ATB_OK;
 }
 
@@ -1494,8 +1539,13 @@ int atb_serve_reset(atb_server* s) {
     ATB_CUDA(cudaMemcpy(&claimed, s->counter.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (claimed < s->ntiles)
         return fail(ATB_ERR_ARG, "reset with published work unclaimed");
+    int ring[3] = {0, 0, 0};
+    ATB_CUDA(cudaMemcpy(ring, s->ring_ctr.p, 3 * sizeof(int), cudaMemcpyDeviceToHost));
+    if (ring[0] < ring[1]) return fail(ATB_ERR_ARG, "reset with continuations pending");
     ATB_CUDA(cudaMemset(s->counter.p, 0, sizeof(int)));
     ATB_CUDA(cudaMemset(s->status.p, 0, sizeof(int)));
+    ATB_CUDA(cudaMemset(s->ring_ctr.p, 0, 4 * sizeof(int)));
+    ATB_CUDA(cudaMemset(s->ring.p, 0, (size_t)s->ring_cap * sizeof(AtbServeCont)));
     s->njobs = 0;
     s->ntiles = 0;
     s->ctl->published = 0;
@@ -1517,7 +1567,7 @@ int atb_serve_close(atb_server* s) {
         if (rc == ATB_OK && (status & ATB_STATUS_WAIT_TIMEOUT))
             rc = fail(ATB_ERR_TIMEOUT, "a bounded shared-memory staging wait timed out");
         for (DevBuf* b : {&s->jobs, &s->tiles, &s->counter, &s->status, &s->jobnext, &s->done,
-                          &s->compact})
+                          &s->compact, &s->ring, &s->ring_ctr})
             b->release();
         if (s->ctl) cudaFreeHost(s->ctl);
         if (s->h_done) cudaFreeHost(s->h_done);

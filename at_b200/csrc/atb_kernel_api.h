@@ -37,6 +37,43 @@ typedef struct AtbServeCtl {
     volatile int32_t stop;
 } AtbServeCtl;
 
+typedef struct AtbTile {
+    int32_t job;
+    int32_t count;
+    int64_t first;
+} AtbTile;
+
+/* A tile that has run one chunk of its job's turns and waits for the next:
+   written by the block that ran it into the serving loop's continuation ring
+   (device memory), `seq` (its ring index + 1) last, after a fence. */
+typedef struct AtbServeCont {
+    AtbTile tile;
+    int32_t turn_off;           /* turns of the job already run             */
+    int32_t seq;
+} AtbServeCont;
+
+/* The serving loop's device-side queue: the continuation ring and its
+   cursors (device memory). */
+typedef struct AtbServeRing {
+    AtbServeCont* slots;
+    int32_t cap;                /* entries (power of two)                   */
+    int32_t pad;
+    int* head;                  /* next entry to claim                      */
+    int* tail;                  /* next entry to write                      */
+} AtbServeRing;
+
+#define ATB_STATUS_RING_FULL 8    /* a continuation found the ring full and
+                                     ran its remaining turns in place */
+
+/* Everything the serving kernel shares with the host besides the tile and
+   job arrays. */
+typedef struct AtbServeArgs {
+    const AtbServeCtl* ctl;     /* mapped host memory                       */
+    AtbServeRing ring;
+    int* inflight;              /* tiles claimed and not yet finished       */
+    unsigned long long* done;   /* per job: particles finished              */
+} AtbServeArgs;
+
 /* one staged lattice segment: consecutive element records */
 typedef struct AtbSeg {
     int32_t first_elem;
@@ -74,6 +111,9 @@ typedef struct AtbJob {
     uint32_t* alive;            /* optional: survivors after each turn     */
     double* moments;            /* optional: 12 sums per turn              */
     uint64_t rng_key;           /* key of the quantum-diffusion kicks      */
+    int32_t chunk;              /* serving: turns per claim, 0 all (a tile
+                                   re-enqueues itself for the rest)         */
+    int32_t pad_chunk;
 } AtbJob;
 
 /* Whether a job's particles may be handed out through a per-job cursor with
@@ -90,12 +130,6 @@ static inline int atb_job_refills(const AtbJob* J) {
            J->end_elem == J->nelem && J->nturns > 0 && J->nturns < (1 << 30) &&
            J->nseg_turn > 0 && J->nseg_first == J->nseg_turn;
 }
-
-typedef struct AtbTile {
-    int32_t job;
-    int32_t count;
-    int64_t first;
-} AtbTile;
 
 /* Tangent (forward-mode) tracking: one launch over np particles of one
  * lattice, with the Jacobian of the final coordinates with respect to the

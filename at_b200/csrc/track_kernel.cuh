@@ -667,6 +667,14 @@ __device__ __forceinline__ void load6(const double* src, P6& r) {
     r.x = a.x; r.px = a.y; r.y = b.x; r.py = b.y; r.dp = c.x; r.ct = c.y;
 }
 
+/* the same through L2 only: in the serving loop a tile's state may have been
+   written by another SM's block since this SM last cached those lines */
+__device__ __forceinline__ void load6_cg(const double* src, P6& r) {
+    const double2* s = reinterpret_cast<const double2*>(src);
+    double2 a = __ldcg(s), b = __ldcg(s + 1), c = __ldcg(s + 2);
+    r.x = a.x; r.px = a.y; r.y = b.x; r.py = b.y; r.dp = c.x; r.ct = c.y;
+}
+
 __device__ __forceinline__ void store6(double* dst, const P6& r) {
     double2* d = reinterpret_cast<double2*>(dst);
     d[0] = make_double2(r.x, r.px);
@@ -682,30 +690,79 @@ __device__ __forceinline__ int seg_at(const AtbJob& J, long long q) {
 
 /* ---------------- the kernel --------------------------------------------- */
 
-/* The serving loop's claim (one thread per block): the next tile if the host
- * has published it; otherwise wait (sleeping between looks) until it does,
- * until it sets `stop`, or for at most ATB_SERVE_IDLE_NS, after which the
- * block leaves.  A tile is taken only once published (compare-and-swap on
- * the counter), so a block that leaves holds no claim. */
-__device__ __forceinline__ int serve_claim(const AtbServeCtl* ctl, int* counter, int* status) {
-    const uint64_t t0 = global_ns();
+/* The serving loop's claim (one thread per block).  New work first: the
+ * next tile the host has published (taken by compare-and-swap on the counter
+ * only while it is below `published`, so a block never holds a claim the host
+ * has not published).  Then the continuation ring: a tile that has run a
+ * chunk of its job's turns and waits for the next (an entry is taken once
+ * its `seq` shows it written).  Without work the block sleeps between looks;
+ * it leaves when the host sets `stop`, or after ATB_SERVE_IDLE_NS with
+ * nothing claimed anywhere (no tile in flight that could still re-enqueue),
+ * or after a hundred times that while tiles are in flight.  Returns 1 with
+ * the tile and the turns of its job already run, or 0 to leave. */
+__device__ __forceinline__ int serve_claim(const AtbServeCtl* ctl, int* counter,
+                                           const AtbTile* tiles, const AtbServeRing& ring,
+                                           int* inflight, int* status, AtbTile* tile,
+                                           int* turn_off) {
+    uint64_t t0 = global_ns();
     while (true) {
+        if (ctl->stop) return 0;
         const int pub = ctl->published;
         const int c = atomicAdd(counter, 0);
         if (c < pub) {
             if (atomicCAS(counter, c, c + 1) == c) {
-                __threadfence_system();   /* records read after the flag */
-                return c;
+                atomicAdd(inflight, 1);
+                __threadfence_system();          /* records read after the flag */
+                const int4 tw = __ldcg(reinterpret_cast<const int4*>(tiles + c));
+                *tile = *reinterpret_cast<const AtbTile*>(&tw);
+                *turn_off = 0;
+                return 1;
             }
-            continue;                     /* another block took it: look again */
+            continue;                            /* another block took it */
         }
-        if (ctl->stop) return -1;
-        if (global_ns() - t0 > ATB_SERVE_IDLE_NS) {
+        const int h = atomicAdd(ring.head, 0);
+        const int t = atomicAdd(ring.tail, 0);
+        if (h < t) {
+            const AtbServeCont* e = ring.slots + (h & (ring.cap - 1));
+            if (__ldcg(&e->seq) == h + 1) {
+                if (atomicCAS(ring.head, h, h + 1) == h) {
+                    atomicAdd(inflight, 1);
+                    __threadfence();
+                    const int4 tw = __ldcg(reinterpret_cast<const int4*>(&e->tile));
+                    *tile = *reinterpret_cast<const AtbTile*>(&tw);
+                    *turn_off = __ldcg(&e->turn_off);
+                    return 1;
+                }
+                continue;
+            }
+            /* reserved by a producer and not yet written: look again */
+            t0 = global_ns();
+            continue;
+        }
+        const bool busy = atomicAdd(inflight, 0) > 0;
+        const uint64_t limit = busy ? 100ULL * ATB_SERVE_IDLE_NS : ATB_SERVE_IDLE_NS;
+        if (global_ns() - t0 > limit) {
             atomicOr(status, ATB_STATUS_IDLE);
-            return -1;
+            return 0;
         }
         __nanosleep(4000);
     }
+}
+
+/* Put a tile that has run `turn_off` turns of its job back in the
+ * continuation ring.  Returns false if the ring is full. */
+__device__ __forceinline__ bool serve_requeue(const AtbServeRing& ring, const AtbTile& tile,
+                                              int turn_off) {
+    const int h = atomicAdd(ring.head, 0);
+    const int t = atomicAdd(ring.tail, 0);
+    if (t - h >= ring.cap - 64) return false;      /* leave room for racing producers */
+    const int idx = atomicAdd(ring.tail, 1);
+    AtbServeCont* e = ring.slots + (idx & (ring.cap - 1));
+    e->tile = tile;
+    e->turn_off = turn_off;
+    __threadfence();
+    atomicExch(&e->seq, idx + 1);
+    return true;
 }
 
 #ifndef ATB_NO_TRACK_KERNEL
@@ -750,11 +807,15 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                                             unsigned long long* __restrict__ job_next,
                                             int* __restrict__ status, int smem_cap_words,
                                             double* __restrict__ scratch,
-                                            const AtbServeCtl* ctl = nullptr,
-                                            unsigned long long* __restrict__ done = nullptr) {
+                                            AtbServeArgs sv = AtbServeArgs{}) {
     extern __shared__ __align__(128) double smem[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_tile;
+    /* serving: the claimed tile, the turns of its job already run, the job's
+       full turn count, and whether the block keeps its tile for the next
+       chunk (continuation ring full) */
+    __shared__ AtbTile s_ctile;
+    __shared__ int s_toff, s_full, s_self;
     __shared__ unsigned long long s_first;
     __shared__ int s_warp[ATB_MAX_THREADS / 32];
     double* buf0 = smem;
@@ -768,36 +829,52 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
         mbar_init(&bars[1], 1);
         fence_mbar_init();
     }
+    if constexpr (SERVE) {
+        if (tid == 0) s_self = 0;
+    }
     __syncthreads();
 
     int resident_job = -1;   /* job whose whole table sits in buf0 */
 
     while (true) {
         if (tid == 0) {
-            if constexpr (SERVE) s_tile = serve_claim(ctl, tile_counter, status);
-            else s_tile = atomicAdd(tile_counter, 1);
+            if constexpr (SERVE) {
+                if (s_self) s_tile = 1;            /* the same tile, next chunk */
+                else s_tile = serve_claim(sv.ctl, tile_counter, tiles, sv.ring, sv.inflight,
+                                          status, &s_ctile, &s_toff);
+            } else {
+                s_tile = atomicAdd(tile_counter, 1);
+            }
         }
         __syncthreads();
         const int t = s_tile;
         __syncthreads();
         if constexpr (SERVE) {
-            if (t < 0) break;
+            if (t <= 0) break;
         } else {
             if (t >= ntiles) break;
         }
         AtbTile tile;
         const AtbJob* jp;
         if constexpr (SERVE) {
-            /* the host writes tile and job records while the kernel runs:
-               read them past the L1 cache, the job into shared memory (only
-               the serving kernel has this buffer) */
+            /* the host writes job records while the kernel runs: read the
+               record past the L1 cache into shared memory (only the serving
+               kernel has this buffer), then narrow it to this claim's chunk
+               of turns, continuing the absolute turn counter */
             __shared__ __align__(16) AtbJob s_job;
-            const int4 tw = __ldcg(reinterpret_cast<const int4*>(tiles + t));
-            tile = *reinterpret_cast<const AtbTile*>(&tw);
+            tile = s_ctile;
             const unsigned long long* src =
                 reinterpret_cast<const unsigned long long*>(jobs + tile.job);
             unsigned long long* dst = reinterpret_cast<unsigned long long*>(&s_job);
             for (int w = tid; w < (int)(sizeof(AtbJob) / 8); w += nthr) dst[w] = __ldcg(src + w);
+            __syncthreads();
+            if (tid == 0) {
+                const int full = s_job.nturns;
+                const int rem = full - s_toff;
+                s_full = full;
+                s_job.turn0 += s_toff;
+                s_job.nturns = (s_job.chunk > 0 && s_job.chunk < rem) ? s_job.chunk : rem;
+            }
             __syncthreads();
             jp = &s_job;
         } else {
@@ -834,8 +911,13 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
             lt0[k] = 0;
             lost[k] = false;
             if (active[k]) {
-                load6(J.r + 6 * p[k], r[k]);
-                if (J.losses) lost[k] = J.lost[p[k]] != 0;
+                if constexpr (SERVE) {
+                    load6_cg(J.r + 6 * p[k], r[k]);
+                    if (J.losses) lost[k] = __ldcg(J.lost + p[k]) != 0;
+                } else {
+                    load6(J.r + 6 * p[k], r[k]);
+                    if (J.losses) lost[k] = J.lost[p[k]] != 0;
+                }
             } else {
                 r[k].x = nan_d(); r[k].px = r[k].py = r[k].y = r[k].dp = r[k].ct = 0.0;
                 lost[k] = true;
@@ -1134,10 +1216,32 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
             }
         }
         if constexpr (SERVE) {
-            /* report the stored particles once they are visible device-wide */
+            /* the chunk is stored and visible device-wide: a tile with live
+               particles and turns left goes back to the continuation ring
+               (or, if the ring is full, stays with this block); otherwise its
+               particles count as done */
             __threadfence();
-            __syncthreads();
-            if (tid == 0) atomicAdd(&done[tile.job], (unsigned long long)taken);
+            bool live = false;
+#pragma unroll
+            for (int k = 0; k < NP; ++k)
+                live |= active[k] && !isnan(r[k].x) && !(J.losses && lost[k]);
+            const int any = __syncthreads_or(live);
+            if (tid == 0) {
+                const int ran = s_toff + J.nturns;
+                bool requeued = false, keep = false;
+                if (any && ran < s_full && !sv.ctl->stop) {
+                    requeued = serve_requeue(sv.ring, tile, ran);
+                    if (!requeued) {
+                        atomicOr(status, ATB_STATUS_RING_FULL);
+                        keep = true;
+                        s_toff = ran;
+                    }
+                }
+                if (!requeued && !keep && !(any && ran < s_full))
+                    atomicAdd(&sv.done[tile.job], (unsigned long long)taken);
+                if (!keep) atomicSub(sv.inflight, 1);
+                s_self = keep ? 1 : 0;
+            }
         }
         /* all threads must be past the last segment before the buffers are
            re-filled by the next tile */
@@ -1169,19 +1273,18 @@ ATB_CAT(ATB_CAT(atb_track_kernel, ATB_KSUFFIX), _gen)(const AtbJob* __restrict__
                          scratch);
 }
 
-/* The serving loop's persistent kernel: tiles come from a queue the host
-   appends to while it runs (AtbServeCtl); `done[job]` counts the particles of
-   each job that are back in memory. */
+/* The serving loop's persistent kernel: new tiles come from a queue the host
+   appends to while it runs (AtbServeCtl), continuations from the device-side
+   ring; `done[job]` counts the particles of each job that have run all their
+   turns (or were lost) and are back in memory.  No lane refill: a tile keeps
+   its particles from chunk to chunk. */
 extern "C" __global__ void __launch_bounds__(ATB_MAX_THREADS)
 ATB_CAT(atb_serve_kernel, ATB_KSUFFIX)(const AtbJob* __restrict__ jobs,
-                                       const AtbTile* __restrict__ tiles,
-                                       const AtbServeCtl* ctl, int* __restrict__ tile_counter,
-                                       unsigned long long* __restrict__ job_next,
-                                       unsigned long long* __restrict__ done,
-                                       int* __restrict__ status, int smem_cap_words,
-                                       double* __restrict__ scratch) {
-    track_tiles<1, false, true>(jobs, tiles, 0, tile_counter, job_next, status, smem_cap_words,
-                                scratch, ctl, done);
+                                       const AtbTile* __restrict__ tiles, AtbServeArgs sv,
+                                       int* __restrict__ tile_counter, int* __restrict__ status,
+                                       int smem_cap_words, double* __restrict__ scratch) {
+    track_tiles<1, false, true>(jobs, tiles, 0, tile_counter, nullptr, status, smem_cap_words,
+                                scratch, sv);
 }
 
 /* two particles per thread (the autotuner's particles-per-thread choice) */

@@ -8,10 +8,12 @@ not fit) and advances all of them together.
 ``TrackingServer`` is device-resident: ONE persistent kernel
 (``atb_serve_*``) claims tiles from a queue that the host appends to while it
 runs.  A request joins as soon as its particles are in HBM -- its tiles are
-published into the running launch -- and it advances by chunks of turns,
-each chunk a job appended when the previous one is done, so long requests
-share the GPU with short ones (processor sharing) without any global round
-barrier.  Admission copies and result copies run on a side stream (copy
+published into the running launch -- and is one job for all its turns.  A
+tile runs a chunk of turns per claim (a few tens of ms of one block's work)
+and then puts itself back in a device-side continuation ring that the blocks
+take from after new work, so long requests share the GPU with short ones
+tile by tile (processor sharing) with no host step and no barrier between
+chunks.  Admission copies and result copies run on a side stream (copy
 engine) beside the kernel.  ``RoundServer`` is the earlier form: one
 ``atb_track_batch`` launch per round over every active request, new arrivals
 joining at the next round.
@@ -186,7 +188,7 @@ class TrackingServer:
     """Device-resident continuous batching over one persistent kernel."""
 
     def __init__(self, lattices: dict, hbm_budget_bytes: float = 150e9, device: int = 0,
-                 mode="exact", chunk_flops: float = 2e12, max_chunk: int = 512,
+                 mode="exact", chunk_flops: float = 1e9, max_chunk: int = 512,
                  max_jobs: int = 1 << 16, max_tiles: int = 1 << 22):
         import ctypes as C
 
@@ -253,33 +255,38 @@ class TrackingServer:
             self.staging.append(req)
         self.waiting = keep
 
+    TILE = 256                                # particles per tile (the kernel's block)
+
     def _chunk(self, req) -> int:
-        per = req.n * self.fpt[req.lattice]
-        return int(max(1, min(self.max_chunk, req.nturns - req.done_turns,
-                              self.chunk_flops // max(per, 1.0))))
+        """Turns a tile runs per claim: about ``chunk_flops`` of work (a few
+        tens of ms on one block), so a tile of a long request goes back to
+        the device queue often enough for newer requests' tiles to start."""
+        per = min(req.n, self.TILE) * self.fpt[req.lattice]
+        return int(max(1, min(self.max_chunk, req.nturns, self.chunk_flops // max(per, 1.0))))
 
     def _submit(self, req):
         C = self.C
         from ._lib import AtbJobDesc
-        t = self._chunk(req)
         d = req.dev
         jd = AtbJobDesc()
         jd.lattice_id = self.lids[req.lattice]
-        jd.nturns = t
-        jd.turn0 = req.done_turns
+        jd.nturns = req.nturns
+        jd.turn0 = 0
         jd.losses = 1
         jd.r = d["r"].data_ptr()
         jd.np = req.n
         jd.islost, jd.lturn = d["lost"].data_ptr(), d["lturn"].data_ptr()
         jd.lelem, jd.lcoord = d["lelem"].data_ptr(), d["lcoord"].data_ptr()
         slot = C.c_int32(-1)
-        self.check(self.lib.atb_serve_submit(self.srv, C.byref(jd), C.byref(slot)))
-        req._slot, req._step = slot.value, t
+        self.check(self.lib.atb_serve_submit(self.srv, C.byref(jd), self._chunk(req),
+                                             C.byref(slot)))
+        req._slot = slot.value
         self.jobs = slot.value + 1
 
     # -- progress -------------------------------------------------------------------
     def _poll(self) -> int:
-        """Advance every request whose chunk is done; returns how many moved."""
+        """Publish staged requests and start the result copy of every request
+        whose particles are all done; returns how many moved."""
         C, torch = self.C, self.torch
         moved = 0
         for req in list(self.staging):
@@ -299,11 +306,8 @@ class TrackingServer:
                 if int(buf[req._slot - first]) != req.n:
                     continue
                 moved += 1
-                req.done_turns += req._step
-                self.particle_turns += req.n * req._step
-                if req.done_turns < req.nturns:
-                    self._submit(req)
-                    continue
+                req.done_turns = req.nturns
+                self.particle_turns += req.n * req.nturns
                 self.active.remove(req)
                 with torch.cuda.stream(self.copy):
                     for k in req.dev:
@@ -357,6 +361,13 @@ class TrackingServer:
             if time_limit is not None and time.perf_counter() - t0 > time_limit:
                 break
         return time.perf_counter() - t0
+
+    def counters(self) -> dict:
+        """Tiles published and claimed from the host queue and continuations
+        written to and taken from the device queue since the last reset."""
+        out = (self.C.c_int32 * 4)()
+        self.check(self.lib.atb_serve_counters(self.srv, out))
+        return dict(zip(("published", "claimed", "requeued", "resumed"), list(out)))
 
     def close(self):
         if self.srv:

@@ -597,13 +597,16 @@ def run_serving(nreq, mode, device, full=False, time_limit=None):
     for name, cls in forms:
         trace = serving.make_trace(list(lats), nreq, **kw)
         srv = cls(lats, hbm_budget_bytes=150e9, device=device, mode=mode)
+        extra = {}
         try:
             wall = srv.serve(trace, time_limit=time_limit)
+            if hasattr(srv, "counters"):
+                extra["tile_counters"] = srv.counters()
         finally:
             srv.close()
         st = serving.latency_stats(trace)
         pt = sum(r.n * r.nturns for r in trace if r.finished is not None)
-        out[name] = dict(st, particle_turns_per_s=pt / wall, wall_s=wall)
+        out[name] = dict(st, particle_turns_per_s=pt / wall, wall_s=wall, **extra)
         traces[name] = trace
     seq_trace = serving.make_trace(list(lats), nreq, **kw)
     wall_seq = serving.serve_sequential(lats, seq_trace, mode=mode, device=device,

@@ -256,15 +256,23 @@ int atb_track_noalloc(int32_t device, const double* table, int64_t nwords,
  *                     `mode`.  The kernel is launched by the first submit.
  *   atb_serve_submit  append a job (device buffers as in atb_track_batch:
  *                     whole turns from turn0, loss map when losses is 1) and
- *                     publish its tiles; returns its slot.  ATB_ERR_NOMEM when
- *                     the queue is full (atb_serve_reset it once every
- *                     published job has finished).
+ *                     publish its tiles; returns its slot.  With chunk_turns
+ *                     > 0 a tile runs that many turns per claim and then goes
+ *                     back to a device-side queue, so long jobs share the GPU
+ *                     with later ones tile by tile (0: all turns in one
+ *                     claim).  ATB_ERR_NOMEM when the queue is full
+ *                     (atb_serve_reset it once every job has finished).
  *   atb_serve_poll    the particles of slots [first, first + nslots) that are done and
- *                     back in memory (a job is finished when its count equals
- *                     its particle count; its buffers may then be read), and
+ *                     back in memory after all their turns (a job is
+ *                     finished when its count equals its particle count; its
+ *                     buffers may then be read), and
  *                     whether the kernel is running.  The kernel leaves after
  *                     ATB_SERVE_IDLE (0.2 s) without new work; poll and submit
- *                     launch it again while published work is unclaimed.
+ *                     launch it again while published or re-enqueued work
+ *                     waits.
+ *   atb_serve_counters  tiles published and claimed from the host queue, and
+ *                     continuations written to and taken from the device
+ *                     queue since the last reset (out[4]).
  *   atb_serve_reset   leave the kernel and empty the queue.
  *   atb_serve_close   leave the kernel (after the claimed work) and free.
  * A job's result is the same as tracking it alone: each particle runs the
@@ -272,9 +280,10 @@ int atb_track_noalloc(int32_t device, const double* table, int64_t nwords,
 typedef struct atb_server atb_server;
 int atb_serve_open(atb_handle* h, const int32_t* lattice_ids, int32_t nlat, int32_t mode,
                    int32_t max_jobs, int32_t max_tiles, atb_server** out);
-int atb_serve_submit(atb_server* s, const atb_job_desc* job, int32_t* slot);
+int atb_serve_submit(atb_server* s, const atb_job_desc* job, int32_t chunk_turns, int32_t* slot);
 int atb_serve_poll(atb_server* s, int32_t first, int32_t nslots, uint64_t* done,
                    int32_t* running);
+int atb_serve_counters(atb_server* s, int32_t* out);
 int atb_serve_reset(atb_server* s);
 int atb_serve_close(atb_server* s);
 

@@ -68,21 +68,46 @@ def test_round_server_results_equal_alone():
 @pytest.mark.parametrize("mode", ["exact", "fast"])
 def test_device_resident_server_results_equal_alone(mode):
     """The persistent serving kernel: requests are published into the running
-    launch as they arrive (no round barrier), advance by chunks of turns, and
-    each result equals the request tracked alone, bit for bit."""
+    launch as they arrive (no round barrier), each tile advances by chunks of
+    turns through the device-side continuation queue, and each result equals
+    the request tracked alone, bit for bit."""
     lats, orbits = rings.serving_pool(2, 2)
     reqs = serving.make_trace(list(lats), 14, rate_hz=300.0, seed=6, n_range=(200, 4000),
                               t_range=(10, 150), centre_of=orbits.get)
-    srv = serving.TrackingServer(lats, hbm_budget_bytes=2e6, chunk_flops=5e8, mode=mode)
+    srv = serving.TrackingServer(lats, hbm_budget_bytes=2e6, chunk_flops=1e8, mode=mode)
     try:
         srv.serve(reqs)
-        chunks = srv.jobs
+        c = srv.counters()
+        jobs = srv.jobs
     finally:
         srv.close()
-    assert len(srv.done) == len(reqs)
-    assert chunks > len(reqs)                # requests advanced in several chunks
+    assert len(srv.done) == len(reqs) == jobs           # one job per request
+    assert c["claimed"] == c["published"]
+    assert c["resumed"] == c["requeued"] > c["published"]   # tiles ran in several chunks
     assert _overlap(reqs)
     _check_alone(lats, reqs, mode)
+
+
+@pytest.mark.gpu
+def test_device_resident_chunks_keep_results_with_losses():
+    """Chunks of one turn on a bunch that loses particles along the way: the
+    loss turn, element and coordinates carry over from chunk to chunk."""
+    lats, orbits = rings.serving_pool(1, 1)
+    reqs = serving.make_trace(list(lats), 3, rate_hz=1000.0, seed=11, n_range=(600, 1500),
+                              t_range=(40, 60), centre_of=orbits.get)
+    for r in reqs:                                          # far out: losses over many turns
+        c = orbits[r.lattice][[0, 2], None]
+        r.particles[[0, 2]] = c + 6.0 * (r.particles[[0, 2]] - c)
+    srv = serving.TrackingServer(lats, chunk_flops=1.0)       # one turn per claim
+    try:
+        srv.serve(reqs)
+        c = srv.counters()
+    finally:
+        srv.close()
+    assert len(srv.done) == 3
+    assert c["requeued"] > 10 * c["published"]
+    assert any(r.losses["islost"].any() and not r.losses["islost"].all() for r in reqs)
+    _check_alone(lats, reqs, "exact")
 
 
 @pytest.mark.gpu
