@@ -25,10 +25,12 @@ UNITS = [
     ("track_exact.cu", ["-fmad=false"]),
     ("track_fast.cu", ["-fmad=true"]),
     ("tangent.cu", ["-fmad=false"]),
+    ("adjoint.cu", ["-fmad=false"]),
     ("atb200.cu", []),
     ("atb_noalloc.cu", []),
 ]
 DEPS = ["atb_physics.cuh", "atb_dual.cuh", "track_kernel.cuh", "tangent_kernel.cuh",
+        "adjoint_kernel.cuh",
         "atb_diffusion.cuh", "atb_integrators.h",
         "atb_kernel_api.h", "atb_table.h"]
 

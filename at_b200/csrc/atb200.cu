@@ -63,6 +63,8 @@ extern "C" __global__ void atb_serve_kernel_exact(const AtbJob*, const AtbTile*,
 extern "C" __global__ void atb_serve_kernel_fast(const AtbJob*, const AtbTile*, AtbServeArgs, int*,
                                                  int*, int, double*);
 extern "C" __global__ void atb_tangent_kernel(const AtbTangent);
+extern "C" __global__ void atb_adjoint_forward_kernel(const AtbAdjoint);
+extern "C" __global__ void atb_adjoint_turn_kernel(const AtbAdjoint);
 extern "C" __global__ void atb_element_maps_kernel(const AtbElemMaps);
 
 namespace {
@@ -151,7 +153,8 @@ struct atb_handle {
     int64_t rout_budget = 4LL << 30;
     std::vector<Lattice> lats;
     DevBuf r, rout, lost, lturn, lelem, lcoord, refpts, jobs, tiles, counter, status, alive,
-        moments, tan_pelem, tan_porder, compact, jobnext;
+        moments, tan_pelem, tan_porder, compact, jobnext, adj_pelem, adj_porder, adj_scratch,
+        adj_block, adj_state;
     std::vector<int32_t> h_pelem;
     std::vector<AtbTile> h_tiles;
     std::vector<struct Batch> batches;
@@ -562,6 +565,8 @@ int atb_destroy(atb_handle* h) {
         for (DevBuf* b : {&h->r, &h->rout, &h->lost, &h->lturn, &h->lelem, &h->lcoord,
                           &h->refpts, &h->jobs, &h->tiles, &h->counter, &h->status, &h->alive,
                           &h->moments, &h->tan_pelem, &h->tan_porder, &h->compact,
+                          &h->adj_pelem, &h->adj_porder, &h->adj_scratch, &h->adj_block,
+                          &h->adj_state,
                           &h->jobnext})
             b->release();
         if (h->stream) cudaStreamDestroy(h->stream);
@@ -937,23 +942,18 @@ int atb_element_pass(atb_handle* h, int32_t id, const double* r_in, double* r_ou
     return ATB_OK;
 }
 
-int atb_tangent_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t nturns,
-                       int32_t turn0, const int32_t* param_elem, const int32_t* param_order,
-                       const double* param_value, int32_t nparam, double* jac, double* grad,
-                       uint8_t* islost, void* stream) {
-    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
-    Lattice* L = get_lat(h, id);
-    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
-    if (np < 0 || nturns < 0 || nparam < 0) return fail(ATB_ERR_ARG, "negative size");
-    if (np > 0 && (!r || !jac)) return fail(ATB_ERR_ARG, "r or jac is NULL");
-    if (nparam > 0 && (!param_elem || !param_order || !param_value || (np > 0 && !grad)))
-        return fail(ATB_ERR_ARG, "parameter arrays missing");
-    /* the tangent kernel integrates with the CPU engine's Forest-Ruth steps */
+/* Checks shared by the derivative kernels: the lattice uses the default
+   integrator (the kernels integrate with the CPU engine's Forest-Ruth steps),
+   and each differentiated strength is PolynomB[k], k in [1, MaxOrder], of a
+   multipole element carrying no other strength.  Builds the per-element
+   parameter index in h->h_pelem. */
+int strength_map(atb_handle* h, const Lattice* L, const int32_t* param_elem,
+                 const int32_t* param_order, int32_t nparam, const char* who) {
     for (int e = 0; e < L->nelem; ++e)
         if ((L->hdr[e] >> ATB_H_FL_SHIFT) & ATB_F_INTEG)
-            return fail(ATB_ERR_ARG, "the tangent kernel needs a lattice compiled for the "
-                                     "default integrator (4)");
-    /* validate the differentiated strengths against the element headers */
+            return fail(ATB_ERR_ARG, std::string("the ") + who +
+                                         " kernel needs a lattice compiled for the "
+                                         "default integrator (4)");
     h->h_pelem.assign((size_t)std::max(L->nelem, 1), -1);
     for (int q = 0; q < nparam; ++q) {
         const int e = param_elem[q];
@@ -977,6 +977,22 @@ int atb_tangent_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t
                                          ": linear quadrupole-fringe maps are not differentiated");
         h->h_pelem[e] = q;
     }
+    return ATB_OK;
+}
+
+int atb_tangent_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t nturns,
+                       int32_t turn0, const int32_t* param_elem, const int32_t* param_order,
+                       const double* param_value, int32_t nparam, double* jac, double* grad,
+                       uint8_t* islost, void* stream) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Lattice* L = get_lat(h, id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    if (np < 0 || nturns < 0 || nparam < 0) return fail(ATB_ERR_ARG, "negative size");
+    if (np > 0 && (!r || !jac)) return fail(ATB_ERR_ARG, "r or jac is NULL");
+    if (nparam > 0 && (!param_elem || !param_order || !param_value || (np > 0 && !grad)))
+        return fail(ATB_ERR_ARG, "parameter arrays missing");
+    const int rc = strength_map(h, L, param_elem, param_order, nparam, "tangent");
+    if (rc != ATB_OK) return rc;
     if (np == 0) return ATB_OK;
     DeviceGuard g(h->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
@@ -1009,6 +1025,152 @@ int atb_tangent_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t
     const long long blocks = (np + ATB_TANGENT_THREADS - 1) / ATB_TANGENT_THREADS;
     if (blocks > 0x7fffffffLL) return fail(ATB_ERR_ARG, "too many particles");
     atb_tangent_kernel<<<(unsigned)blocks, ATB_TANGENT_THREADS, 0, st>>>(A);
+    ATB_CUDA(cudaGetLastError());
+    return ATB_OK;
+}
+
+/* the adjoint kernels' descriptor with the lattice and the strength map
+   (uploaded on st) */
+int adjoint_setup(atb_handle* h, const Lattice* L, const int32_t* param_order,
+                  const double* param_value, int32_t nparam, cudaStream_t st, AtbAdjoint& A) {
+    std::memset(&A, 0, sizeof(A));
+    A.table = L->words.as<double>();
+    A.elem_off = L->doff.as<uint32_t>();
+    A.nelem = L->nelem;
+    A.nparam = nparam;
+    if (nparam > 0) {
+        if (h->adj_pelem.ensure(h->h_pelem.size() * 4) != cudaSuccess ||
+            h->adj_porder.ensure((size_t)nparam * 4) != cudaSuccess)
+            return fail(ATB_ERR_NOMEM, "cudaMalloc(parameter map) failed");
+        /* pageable sources are staged before cudaMemcpyAsync returns */
+        ATB_CUDA(cudaMemcpyAsync(h->adj_pelem.p, h->h_pelem.data(), h->h_pelem.size() * 4,
+                                 cudaMemcpyHostToDevice, st));
+        ATB_CUDA(cudaMemcpyAsync(h->adj_porder.p, param_order, (size_t)nparam * 4,
+                                 cudaMemcpyHostToDevice, st));
+        A.pelem = h->adj_pelem.as<int32_t>();
+        A.porder = h->adj_porder.as<int32_t>();
+        A.pvalue = param_value;
+    }
+    return ATB_OK;
+}
+
+unsigned adjoint_blocks(int64_t n) {
+    return (unsigned)((n + ATB_ADJ_THREADS - 1) / ATB_ADJ_THREADS);
+}
+
+int atb_adjoint_forward(atb_handle* h, int32_t id, double* r, int64_t np, int32_t nturns,
+                        int32_t turn0, const int32_t* param_elem, const int32_t* param_order,
+                        const double* param_value, int32_t nparam, double* ckpt,
+                        int32_t stride, uint8_t* islost, void* stream) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Lattice* L = get_lat(h, id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    if (np < 0 || nturns < 0 || nparam < 0) return fail(ATB_ERR_ARG, "negative size");
+    if (stride < 1) return fail(ATB_ERR_ARG, "checkpoint stride must be at least 1");
+    if (np > 0 && !r) return fail(ATB_ERR_ARG, "r is NULL");
+    if (nparam > 0 && (!param_elem || !param_order || !param_value))
+        return fail(ATB_ERR_ARG, "parameter arrays missing");
+    if (np > (int64_t)ATB_ADJ_THREADS * 0x7fffffffLL) return fail(ATB_ERR_ARG, "too many particles");
+    const int rc = strength_map(h, L, param_elem, param_order, nparam, "adjoint");
+    if (rc != ATB_OK) return rc;
+    if (np == 0) return ATB_OK;
+    DeviceGuard g(h->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    AtbAdjoint A;
+    const int rs = adjoint_setup(h, L, param_order, param_value, nparam, st, A);
+    if (rs != ATB_OK) return rs;
+    A.nturns = nturns;
+    A.turn0 = turn0;
+    A.stride = stride;
+    A.np = np;
+    A.ld = np;
+    A.r = r;
+    A.ckpt = ckpt;
+    A.lost = islost;
+    atb_adjoint_forward_kernel<<<adjoint_blocks(np), ATB_ADJ_THREADS, 0, st>>>(A);
+    ATB_CUDA(cudaGetLastError());
+    return ATB_OK;
+}
+
+int atb_adjoint_backward(atb_handle* h, int32_t id, const double* ckpt, int64_t np,
+                         int32_t nturns, int32_t turn0, int32_t stride,
+                         const int32_t* param_elem, const int32_t* param_order,
+                         const double* param_value, int32_t nparam, double* lam,
+                         double* gparam, void* stream) {
+    if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
+    Lattice* L = get_lat(h, id);
+    if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
+    if (np < 0 || nturns < 0 || nparam < 0) return fail(ATB_ERR_ARG, "negative size");
+    if (stride < 1) return fail(ATB_ERR_ARG, "checkpoint stride must be at least 1");
+    if (np > 0 && nturns > 0 && (!ckpt || !lam)) return fail(ATB_ERR_ARG, "ckpt or lam is NULL");
+    if (nparam > 0 && (!param_elem || !param_order || !param_value || !gparam))
+        return fail(ATB_ERR_ARG, "parameter arrays missing");
+    if ((size_t)nparam * sizeof(double) > 48 * 1024)
+        return fail(ATB_ERR_ARG, "at most 6144 strengths");
+    if (np > (int64_t)ATB_ADJ_THREADS * 0x7fffffffLL) return fail(ATB_ERR_ARG, "too many particles");
+    const int rc = strength_map(h, L, param_elem, param_order, nparam, "adjoint");
+    if (rc != ATB_OK) return rc;
+    DeviceGuard g(h->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    if (nparam > 0) ATB_CUDA(cudaMemsetAsync(gparam, 0, (size_t)nparam * sizeof(double), st));
+    if (np == 0 || nturns == 0) return ATB_OK;
+    AtbAdjoint A;
+    const int rs = adjoint_setup(h, L, param_order, param_value, nparam, st, A);
+    if (rs != ATB_OK) return rs;
+    /* particles in chunks whose element-entry scratch fits 8 GiB */
+    const int64_t per = (int64_t)std::max(L->nelem, 1) * 6 * sizeof(double);
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(np, (8LL << 30) / per));
+    if (h->adj_scratch.ensure((size_t)(chunk * per)) != cudaSuccess)
+        return fail(ATB_ERR_NOMEM, "cudaMalloc(adjoint scratch) failed");
+    if (stride > 1 &&
+        (h->adj_block.ensure((size_t)stride * chunk * 6 * sizeof(double)) != cudaSuccess ||
+         h->adj_state.ensure((size_t)chunk * 6 * sizeof(double)) != cudaSuccess))
+        return fail(ATB_ERR_NOMEM, "cudaMalloc(adjoint checkpoints) failed");
+    const int nck = (nturns + stride - 1) / stride;
+    const size_t smem = (size_t)nparam * sizeof(double);
+    A.gparam = gparam;
+    A.scratch = h->adj_scratch.as<double>();
+    for (int64_t p0 = 0; p0 < np; p0 += chunk) {
+        const int64_t n = std::min(chunk, np - p0);
+        double* lp = lam + 6 * p0;
+        for (int b = nck - 1; b >= 0; --b) {
+            const int t0 = b * stride;
+            const int nt = std::min(stride, nturns - t0);
+            const double* slab = ckpt + 6 * ((int64_t)b * np + p0);
+            if (stride == 1) {
+                AtbAdjoint T = A;
+                T.np = n;
+                T.ckpt = const_cast<double*>(slab);
+                T.lam = lp;
+                T.turn0 = turn0 + t0;
+                atb_adjoint_turn_kernel<<<adjoint_blocks(n), ATB_ADJ_THREADS, smem, st>>>(T);
+                continue;
+            }
+            /* the block's turn entries, tracked again from its checkpoint */
+            double* tmp = h->adj_state.as<double>();
+            double* blk = h->adj_block.as<double>();
+            ATB_CUDA(cudaMemcpyAsync(tmp, slab, (size_t)n * 6 * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, st));
+            AtbAdjoint F = A;
+            F.np = n;
+            F.ld = n;
+            F.r = tmp;
+            F.ckpt = blk;
+            F.nturns = nt;
+            F.turn0 = turn0 + t0;
+            F.stride = 1;
+            F.skip_last = 1;
+            atb_adjoint_forward_kernel<<<adjoint_blocks(n), ATB_ADJ_THREADS, 0, st>>>(F);
+            for (int t = nt - 1; t >= 0; --t) {
+                AtbAdjoint T = A;
+                T.np = n;
+                T.ckpt = blk + 6 * ((int64_t)t * n);
+                T.lam = lp;
+                T.turn0 = turn0 + t0 + t;
+                atb_adjoint_turn_kernel<<<adjoint_blocks(n), ATB_ADJ_THREADS, smem, st>>>(T);
+            }
+        }
+    }
     ATB_CUDA(cudaGetLastError());
     return ATB_OK;
 }

@@ -153,6 +153,40 @@ typedef struct AtbTangent {
     uint8_t* lost;              /* optional (np): 1 if the particle was lost */
 } AtbTangent;
 
+/* Adjoint (reverse-mode) tracking, one thread per particle.  The forward
+ * kernel tracks `nturns` turns with the differentiated strengths substituted
+ * and stores the state entering every `stride`-th turn in `ckpt`
+ * ((turns / stride, ld, 6) slabs).  The turn kernel runs the adjoint of one
+ * turn (absolute number turn0) from its entry states `ckpt` ((np, 6)): it
+ * re-tracks the turn storing every element's entry state in `scratch`
+ * ((nelem, np, 6)), then maps the cotangent `lam` ((np, 6), in place) from
+ * the turn's exit to its entry and adds the strengths' gradient to
+ * `gparam`. */
+#define ATB_ADJ_THREADS 128
+
+typedef struct AtbAdjoint {
+    const double* table;        /* element table words                      */
+    const uint32_t* elem_off;   /* word offset of every element (+ end)     */
+    int32_t nelem;
+    int32_t nturns;             /* forward: turns tracked                   */
+    int32_t turn0;              /* absolute number of the first turn        */
+    int32_t stride;             /* forward: a checkpoint every stride turns */
+    const int32_t* pelem;       /* per element: parameter index or -1       */
+    const int32_t* porder;      /* per parameter: PolynomB order            */
+    const double* pvalue;       /* per parameter: strength used             */
+    int32_t nparam;
+    int32_t skip_last;          /* forward: store the last turn's entry, do
+                                   not track it                             */
+    int64_t np;
+    int64_t ld;                 /* forward: particles per checkpoint slab   */
+    double* r;                  /* forward: (np, 6) state, in place         */
+    double* ckpt;               /* forward: out; turn kernel: entry states  */
+    uint8_t* lost;              /* forward: optional loss flags (np)        */
+    double* lam;                /* turn kernel: (np, 6) cotangent           */
+    double* scratch;            /* turn kernel: (nelem, np, 6)              */
+    double* gparam;             /* turn kernel: (nparam), added to          */
+} AtbAdjoint;
+
 /* Per-element transfer and diffusion matrices for a particle entering each
  * element at orbits[6 * i]: one thread per element. */
 typedef struct AtbElemMaps {

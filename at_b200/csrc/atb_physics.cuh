@@ -243,8 +243,8 @@ __device__ __forceinline__ void seed_coef(double x, double y, int k, T& re, T& i
 
 /* Coefficient holder: for MO >= 0 the coefficients are copied into
  * registers once per element; MO < 0 reads them (broadcast) from the staged
- * table on every kick.  set_param() (tangent kernel only) replaces B_k by a
- * runtime strength and marks it as the differentiated parameter. */
+ * table on every kick.  set_param() (derivative kernels only) replaces B_k by
+ * a runtime strength and marks it as the differentiated parameter. */
 template <int MO, bool SKEW = true>
 struct Poly {
     double a[SKEW ? MO + 1 : 1], b[MO + 1];
@@ -290,6 +290,11 @@ struct Poly<-1> {
             for (int i = mo - 1; i >= 0; --i)
                 horner_step_dual(re, im, x, y, (i == sk) ? kv : b[i], a[i]);
             seed_coef(val(x), val(y), sk, re, im);
+        } else if (sk >= 0) {
+            re = (sk == mo) ? kv : b[mo];
+            im = a[mo];
+            for (int i = mo - 1; i >= 0; --i)
+                horner_step(re, im, x, y, (i == sk) ? kv : b[i], a[i]);
         } else {
             horner_dyn(a, b, mo, x, y, re, im);
         }

@@ -141,8 +141,9 @@ __device__ __forceinline__ void exit_misalign(P6T<T>& r, const Rec& e) {
 
 /* ---------------- pass methods ------------------------------------------- */
 
-/* A differentiated strength (tangent kernel only): PolynomB[k] of the
- * element is replaced by v and carried as the last derivative direction. */
+/* A differentiated strength (derivative kernels only): PolynomB[k] of the
+ * element is replaced by v and, on dual numbers, carried as the last
+ * derivative direction.  The tracking kernels pass k = -1. */
 struct Param {
     int k;        /* coefficient order, -1: none */
     double v;
@@ -158,6 +159,8 @@ __device__ __forceinline__ T fringe_b1(const Rec& e, const Param& pm) {
             b1.v = pm.v;
             b1.d[sizeof(b1.d) / sizeof(double) - 1] = 1.0;
         }
+    } else {
+        if (pm.k == 1) b1 = pm.v;
     }
     return b1;
 }
@@ -272,9 +275,7 @@ __device__ __forceinline__ void pass_multipole_n(P6T<T>* r, const Rec& e, const 
     const double* B = A + mo + 1;
     Poly<MO, SKEW> pl;
     pl.load(A, B, mo);
-    if constexpr (is_dual<T>::value) {
-        if (pm.k >= 0) pl.set_param(pm.k, pm.v);
-    }
+    if (pm.k >= 0) pl.set_param(pm.k, pm.v);
 
     T nl1[NP], nl2[NP];
 #pragma unroll
@@ -526,9 +527,7 @@ __device__ __forceinline__ void pass_thinmpole(P6T<T>& r, const Rec& e, const Pa
     const double* B = A + mo + 1;
     Poly<-1> pl;
     pl.load(A, B, mo);
-    if constexpr (is_dual<T>::value) {
-        if (pm.k >= 0) pl.set_param(pm.k, pm.v);
-    }
+    if (pm.k >= 0) pl.set_param(pm.k, pm.v);
     const double bax = e.f(ATB_TM_BAX), bay = e.f(ATB_TM_BAY);
     if (fl & ATB_F_SCALING) change_pref<kFast>(r, e.f(ATB_TM_SCALE));
     entrance_misalign(r, e);

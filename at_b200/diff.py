@@ -12,11 +12,19 @@ not finite differences.  It returns, per particle,
   K_q = PolynomB[order_q] of chosen elements (quadrupole and sextupole
   strengths, typically).
 
-``TrackFunction`` wraps one call as a ``torch.autograd.Function``: the forward
-pass returns the final coordinates, the backward pass contracts the saved
-Jacobians with the incoming gradient (the adjoint, or vector-Jacobian product)
-for both the initial coordinates and the strengths.  The strengths are read
-by the kernel from a device tensor, so they can be optimised directly.
+The adjoint kernels (``atb_adjoint_forward`` / ``atb_adjoint_backward``) give
+the reverse mode: a forward pass that stores the state entering every
+``stride``-th turn, and one backward sweep that maps dL/d r_final to
+dL/d r_initial and dL/dK for any scalar L, at a cost that does not grow with
+the number of strengths (:class:`AdjointTracker`).
+
+``track`` wraps one call as a ``torch.autograd.Function``: the forward pass
+returns the final coordinates; the backward pass is either the contraction of
+the tangent kernel's saved Jacobians with the incoming gradient
+(:class:`TangentTracker`) or the adjoint kernels' backward sweep
+(:class:`AdjointTracker`), for both the initial coordinates and the
+strengths.  The strengths are read by the kernels from a device tensor, so
+they can be optimised directly.
 """
 from __future__ import annotations
 
@@ -150,6 +158,77 @@ class TangentTracker:
             self.lid = None
 
 
+class AdjointTracker(TangentTracker):
+    """The same lattice and strengths set up for reverse mode: ``forward``
+    tracks and keeps checkpoints, ``backward`` runs the adjoint sweep."""
+
+    #: checkpoint memory above which turns are stored every ``stride`` turns
+    #: (each block of turns is then tracked again from its checkpoint)
+    CKPT_BUDGET = 8 << 30
+
+    def _stride(self, n: int, nturns: int) -> int:
+        per_turn = 48 * max(n, 1)
+        if nturns * per_turn <= self.CKPT_BUDGET:
+            return 1
+        s = max(1, int(np.ceil(np.sqrt(nturns))))
+        while ((nturns + s - 1) // s + s) * per_turn > self.CKPT_BUDGET and s < nturns:
+            s *= 2
+        return s
+
+    def forward(self, r0, strengths=None, nturns: int = 1, turn0: int = 0, stride=None):
+        """Track ``r0`` ((N, 6) float64 tensor on this device, not modified)
+        with ``strengths`` ((P,) tensor, default: the lattice's own).
+        Returns ``(r, lost, state)``: final coordinates (N, 6), loss flags
+        (N,) and what :meth:`backward` needs."""
+        torch = self.torch
+        if r0.dtype != torch.float64 or r0.dim() != 2 or r0.shape[1] != 6:
+            raise ValueError("r0 must be an (N, 6) float64 tensor")
+        if r0.device != self.dev:
+            raise ValueError("r0 must be on %s" % self.dev)
+        k = self.k0 if strengths is None else strengths
+        if k.dtype != torch.float64 or k.shape != (self.nparam,) or k.device != self.dev:
+            raise ValueError("strengths must be a (%d,) float64 tensor on %s" %
+                             (self.nparam, self.dev))
+        k = k.detach().contiguous().clone()
+        n, nturns = int(r0.shape[0]), int(nturns)
+        stride = self._stride(n, nturns) if stride is None else int(stride)
+        nck = max(1, (nturns + stride - 1) // stride)
+        r = r0.detach().contiguous().clone()
+        ckpt = torch.empty((nck, n, 6), dtype=torch.float64, device=self.dev)
+        lost = torch.empty((n,), dtype=torch.uint8, device=self.dev)
+        cur = torch.cuda.current_stream(self.dev)
+        self.stream.wait_stream(cur)
+        self.eng.adjoint_forward(self.lid, r.data_ptr(), n, nturns, int(turn0), self.pelem,
+                                 self.porder, k.data_ptr() if self.nparam else None,
+                                 ckpt.data_ptr(), stride, lost.data_ptr(),
+                                 self.stream.cuda_stream)
+        cur.wait_stream(self.stream)
+        state = {"ckpt": ckpt, "k": k, "n": n, "nturns": nturns, "turn0": int(turn0),
+                 "stride": stride}
+        return r, lost.bool(), state
+
+    def backward(self, state, g):
+        """dL/d r0 (N, 6) and dL/dK (P,) for the cotangent ``g`` = dL/d r_final
+        ((N, 6) float64 on this device).  Lost particles get NaN rows and add
+        nothing to dL/dK."""
+        torch = self.torch
+        n = state["n"]
+        if g.dtype != torch.float64 or tuple(g.shape) != (n, 6) or g.device != self.dev:
+            raise ValueError("g must be an (%d, 6) float64 tensor on %s" % (n, self.dev))
+        lam = g.detach().contiguous().clone()
+        gk = torch.zeros((self.nparam,), dtype=torch.float64, device=self.dev)
+        k = state["k"]
+        cur = torch.cuda.current_stream(self.dev)
+        self.stream.wait_stream(cur)
+        self.eng.adjoint_backward(self.lid, state["ckpt"].data_ptr(), n, state["nturns"],
+                                  state["turn0"], state["stride"], self.pelem, self.porder,
+                                  k.data_ptr() if self.nparam else None, lam.data_ptr(),
+                                  gk.data_ptr() if self.nparam else None,
+                                  self.stream.cuda_stream)
+        cur.wait_stream(self.stream)
+        return lam, gk
+
+
 def _track_function():
     import torch
 
@@ -174,7 +253,25 @@ def _track_function():
                 g_k = torch.einsum("ni,pin->p", g, grad)
             return g_r0, g_k, None, None, None
 
-    return TrackFunction
+    class AdjointFunction(torch.autograd.Function):
+        """r_final = track(r0, K).  Forward: the adjoint kernels' forward pass
+        (final coordinates and turn checkpoints).  Backward: their reverse
+        sweep, grad_r0 and grad_K in one pass."""
+
+        @staticmethod
+        def forward(ctx, r0, strengths, tracker, nturns, turn0):
+            r, _, state = tracker.forward(r0, strengths, nturns, turn0)
+            ctx.tracker, ctx.state = tracker, state
+            return r
+
+        @staticmethod
+        def backward(ctx, g):
+            g_r0, g_k = ctx.tracker.backward(ctx.state, g.contiguous())
+            ctx.state = None
+            return (g_r0 if ctx.needs_input_grad[0] else None,
+                    g_k if ctx.needs_input_grad[1] else None, None, None, None)
+
+    return TrackFunction, AdjointFunction
 
 
 _TF = None
@@ -184,12 +281,15 @@ def track(tracker: TangentTracker, r0, strengths=None, nturns: int = 1, turn0: i
     """Differentiable multi-turn tracking: returns the final (N, 6)
     coordinates as a tensor that back-propagates to ``r0`` and ``strengths``
     (both float64 tensors on the tracker's device; ``strengths`` defaults to
-    a copy of the lattice's own, which then receives no gradient)."""
+    a copy of the lattice's own, which then receives no gradient).  An
+    :class:`AdjointTracker` back-propagates through the adjoint kernels, a
+    :class:`TangentTracker` through its saved Jacobians."""
     global _TF
     if _TF is None:
         _TF = _track_function()
     k = tracker.k0.clone() if strengths is None else strengths
-    return _TF.apply(r0, k, tracker, int(nturns), int(turn0))
+    fn = _TF[1] if isinstance(tracker, AdjointTracker) else _TF[0]
+    return fn.apply(r0, k, tracker, int(nturns), int(turn0))
 
 
 def find_m66(line, orbit=None, energy=None, particle=None, device: int = 0):

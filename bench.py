@@ -715,7 +715,9 @@ def run_diff(device, n=65536):
     workload): 65,536 particles, sigma 1e-6 around the closed orbit, with
     respect to the initial coordinates and the 64 quadrupole + 64 sextupole
     strengths, for 1 and 100 turns.  Device time of the tangent launch (CUDA
-    events), of the autograd backward contraction, and of the 2 x 128 + 12
+    events), of the autograd backward contraction, of the adjoint kernels'
+    forward pass and backward sweep for the same vector-Jacobian product
+    (with their agreement with the tangent's), and of the 2 x 128 + 12
     exact-mode tracking runs that central differences would need instead."""
     import torch
 
@@ -727,6 +729,7 @@ def run_diff(device, n=65536):
     r0 = rings.gaussian(n, [1e-6] * 6, seed=11, centre=orbit)
     params = diff.multipole_strengths(ring)
     tr = diff.TangentTracker(ring, params, device=device)
+    adj = diff.AdjointTracker(ring, params, device=device)
     dev = torch.device("cuda", device)
     x = torch.tensor(np.ascontiguousarray(r0.T), dtype=torch.float64, device=dev)
     out = {"workload": "FODO ring (385 elements), %d particles sigma 1e-6 around the closed "
@@ -745,11 +748,28 @@ def run_diff(device, n=65536):
             # the adjoint (vector-Jacobian) products of the autograd backward
             g = torch.randn_like(r)
             e0.record()
-            torch.einsum("ni,nij->nj", g, jac)
-            torch.einsum("ni,pin->p", g, grad)
+            vjp_x = torch.einsum("ni,nij->nj", g, jac)
+            vjp_k = torch.einsum("ni,pin->p", g, grad)
             e1.record()
             e1.synchronize()
             t_bwd = e0.elapsed_time(e1) * 1e-3
+            # the same products from the adjoint kernels
+            _, _, st = adj.forward(x, None, nt)       # warm-up
+            adj.backward(st, g)
+            e0.record()
+            _, _, st = adj.forward(x, None, nt)
+            e1.record()
+            e1.synchronize()
+            t_afwd = e0.elapsed_time(e1) * 1e-3
+            e0.record()
+            ax, ak = adj.backward(st, g)
+            e1.record()
+            e1.synchronize()
+            t_abwd = e0.elapsed_time(e1) * 1e-3
+            del st
+
+            def rel(a, b):
+                return float(((a - b).abs().max() / b.abs().max()).item())
             # one exact-mode tracking of the same particles (device resident)
             xr = x.clone()
             eng.track_device(lid, xr.data_ptr(), n, nt, mode="exact",
@@ -769,10 +789,16 @@ def run_diff(device, n=65536):
                 "lost": int(lost.sum().item()),
                 "exact_tracking_ms": 1e3 * t_trk,
                 "central_differences_ms": 1e3 * t_trk * runs,
-                "speedup_vs_central_differences": t_trk * runs / t_tan}
+                "speedup_vs_central_differences": t_trk * runs / t_tan,
+                "adjoint": {"forward_ms": 1e3 * t_afwd, "backward_ms": 1e3 * t_abwd,
+                            "particle_turns_per_s": n * nt / (t_afwd + t_abwd),
+                            "speedup_vs_tangent_vjp": (t_tan + t_bwd) / (t_afwd + t_abwd),
+                            "rel_diff_vs_tangent": {"d_r0": rel(ax, vjp_x),
+                                                    "d_strengths": rel(ak, vjp_k)}}}
     finally:
         eng.free(lid)
         tr.close()
+        adj.close()
     return out
 
 

@@ -163,6 +163,36 @@ int atb_tangent_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np,
                        const double* param_value, int32_t nparam, double* jac, double* grad,
                        uint8_t* islost, void* stream);
 
+/* Adjoint (reverse-mode) tracking, device pointers, enqueued on `stream`
+ * (NULL: the handle's stream); strengths as for atb_tangent_device.
+ *   atb_adjoint_forward   tracks the (6, np) particles `r` in place for
+ *       `nturns` whole turns (exact arithmetic, the strengths param_value
+ *       substituted) and, when ckpt is not NULL, stores the state entering
+ *       turns 0, stride, 2 stride, ... in ckpt ((ceil(nturns / stride), np, 6)).
+ *       Lost particles come back NaN (islost, optional, marks them).
+ *   atb_adjoint_backward  from those checkpoints (same np, nturns, turn0,
+ *       stride and strengths) and the cotangent lam = dL/d r_final
+ *       ((6, np), in place), writes lam = dL/d r_initial and
+ *       gparam (nparam) = dL/dK_q = sum over particles, for any scalar L of
+ *       the final coordinates: one backward sweep, one launch per turn, whose
+ *       cost does not grow with the number of strengths.  With stride > 1
+ *       each block of turns is tracked again from its checkpoint.  Lost
+ *       particles get NaN in lam and add nothing to gparam.
+ * Work buffers live on the handle: calls on one handle from different
+ * streams must be ordered by the caller.  Replaces, for a scalar objective,
+ * the finite differences a caller of lattice_pass would take; the reference's
+ * own diff_* routines (atintegrators/diff_*.c) propagate diffusion matrices,
+ * not gradients. */
+int atb_adjoint_forward(atb_handle* h, int32_t lattice_id, double* r, int64_t np,
+                        int32_t nturns, int32_t turn0, const int32_t* param_elem,
+                        const int32_t* param_order, const double* param_value, int32_t nparam,
+                        double* ckpt, int32_t stride, uint8_t* islost, void* stream);
+int atb_adjoint_backward(atb_handle* h, int32_t lattice_id, const double* ckpt, int64_t np,
+                         int32_t nturns, int32_t turn0, int32_t stride,
+                         const int32_t* param_elem, const int32_t* param_order,
+                         const double* param_value, int32_t nparam, double* lam,
+                         double* gparam, void* stream);
+
 /* Element maps for Ohmi's envelope (device pointers, enqueued on `stream`):
  * for a particle entering element i at orbits[6 i .. 6 i + 5], its transfer
  * matrix m66[i] (exact derivatives, row-major d out / d in) and its radiation
