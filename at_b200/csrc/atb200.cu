@@ -1447,6 +1447,9 @@ int atb_sync(atb_handle* h, void* stream) {
 
 namespace {
 
+static_assert(sizeof(AtbTile) == 16 && sizeof(AtbServeCont) == 32,
+              "the serving kernel reads tiles with 16-byte vector loads");
+
 AtbServeArgs serve_args(atb_server* s) {
     AtbServeArgs a;
     std::memset(&a, 0, sizeof(a));

@@ -45,11 +45,13 @@ typedef struct AtbTile {
 
 /* A tile that has run one chunk of its job's turns and waits for the next:
    written by the block that ran it into the serving loop's continuation ring
-   (device memory), `seq` (its ring index + 1) last, after a fence. */
+   (device memory), `seq` (its ring index + 1) last, after a fence.  32 bytes,
+   so that every entry's tile is 16-byte aligned for its vector load. */
 typedef struct AtbServeCont {
     AtbTile tile;
     int32_t turn_off;           /* turns of the job already run             */
     int32_t seq;
+    int64_t pad;
 } AtbServeCont;
 
 /* The serving loop's device-side queue: the continuation ring and its
