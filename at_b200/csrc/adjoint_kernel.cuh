@@ -138,24 +138,88 @@ __device__ __forceinline__ void adj_pass_drift(const P6& s, double* lam, const R
 
 /* ---- thick multipoles ---------------------------------------------------- */
 
-/* F'(z) for F(z) = sum_n (B_n + i A_n) z^n, B_sk replaced by kv */
-__device__ __forceinline__ void field_prime(const double* A, const double* B, int mo, int sk,
-                                            double kv, double x, double y, double& dr,
-                                            double& di) {
-    if (mo <= 0) {
-        dr = 0.0;
-        di = 0.0;
-        return;
+/* The element's multipole coefficients for the reverse pass, B_sk replaced
+ * by the differentiated strength kv: in registers for MaxOrder MO in 0..3,
+ * read from the table for MO = -1 (any order).  field() is F(z) =
+ * sum_n (B_n + i A_n) z^n by Horner's rule with fused multiply-adds (the
+ * recomputed steps inside an element only feed derivatives, so they need not
+ * round as the tracking does); prime() is F'(z) by the same recursion. */
+template <int MO>
+struct AdjCoef {
+    double a[MO + 1], b[MO + 1];
+    int sk;
+    __device__ __forceinline__ void load(const double* A, const double* B, int, int k,
+                                         double v) {
+#pragma unroll
+        for (int i = 0; i <= MO; ++i) {
+            a[i] = A[i];
+            b[i] = (i == k) ? v : B[i];
+        }
+        sk = k;
     }
-    dr = (double)mo * ((sk == mo) ? kv : B[mo]);
-    di = (double)mo * A[mo];
-    for (int n = mo - 1; n >= 1; --n) {
-        const double b = (sk == n) ? kv : B[n];
-        const double t = fma(dr, x, fma(-di, y, (double)n * b));
-        di = fma(di, x, fma(dr, y, (double)n * A[n]));
-        dr = t;
+    __device__ __forceinline__ void field(double x, double y, double& re, double& im) const {
+        re = b[MO];
+        im = a[MO];
+#pragma unroll
+        for (int i = MO - 1; i >= 0; --i) {
+            const double t = fma(re, x, fma(-im, y, b[i]));
+            im = fma(im, x, fma(re, y, a[i]));
+            re = t;
+        }
     }
-}
+    __device__ __forceinline__ void prime(double x, double y, double& dr, double& di) const {
+        if constexpr (MO == 0) {
+            dr = 0.0;
+            di = 0.0;
+        } else {
+            dr = (double)MO * b[MO];
+            di = (double)MO * a[MO];
+#pragma unroll
+            for (int n = MO - 1; n >= 1; --n) {
+                const double t = fma(dr, x, fma(-di, y, (double)n * b[n]));
+                di = fma(di, x, fma(dr, y, (double)n * a[n]));
+                dr = t;
+            }
+        }
+    }
+};
+
+template <>
+struct AdjCoef<-1> {
+    const double* a;
+    const double* b;
+    int mo;
+    int sk;
+    double kv;
+    __device__ __forceinline__ void load(const double* A, const double* B, int m, int k,
+                                         double v) {
+        a = A; b = B; mo = m; sk = k; kv = v;
+    }
+    __device__ __forceinline__ double bk(int i) const { return (i == sk) ? kv : b[i]; }
+    __device__ __forceinline__ void field(double x, double y, double& re, double& im) const {
+        re = bk(mo);
+        im = a[mo];
+        for (int i = mo - 1; i >= 0; --i) {
+            const double t = fma(re, x, fma(-im, y, bk(i)));
+            im = fma(im, x, fma(re, y, a[i]));
+            re = t;
+        }
+    }
+    __device__ __forceinline__ void prime(double x, double y, double& dr, double& di) const {
+        if (mo <= 0) {
+            dr = 0.0;
+            di = 0.0;
+            return;
+        }
+        dr = (double)mo * bk(mo);
+        di = (double)mo * a[mo];
+        for (int n = mo - 1; n >= 1; --n) {
+            const double t = fma(dr, x, fma(-di, y, (double)n * bk(n)));
+            di = fma(di, x, fma(dr, y, (double)n * a[n]));
+            dr = t;
+        }
+    }
+};
 
 /* (x + i y)^k */
 __device__ __forceinline__ void zpow(double x, double y, int k, double& zr, double& zi) {
@@ -168,29 +232,20 @@ __device__ __forceinline__ void zpow(double x, double y, int k, double& zr, doub
     }
 }
 
-struct KickAdj {
-    const double* A;
-    const double* B;
-    int mo;
-    int sk;          /* differentiated order, -1: none */
-    double kv;
-    double irho;     /* bends */
-};
-
 /* strthinkick / bndthinkick of length L at input (x, y):
  * px -= L (Re F - [bend] (dp - x irho) irho), py += L Im F,
  * [bend] ct += lirho x */
-template <bool BEND>
-__device__ __forceinline__ void adj_kick(const KickAdj& c, double x, double y, double L,
-                                         double lirho, double* lam, double& g) {
+template <bool BEND, int MO>
+__device__ __forceinline__ void adj_kick(const AdjCoef<MO>& c, double x, double y, double L,
+                                         double lirho, double irho, double* lam, double& g) {
     double dr, di;
-    field_prime(c.A, c.B, c.mo, c.sk, c.kv, x, y, dr, di);
+    c.prime(x, y, dr, di);
     const double lpx = lam[1], lpy = lam[3];
     double ax = L * fma(-dr, lpx, di * lpy);
     const double ay = L * fma(di, lpx, dr * lpy);
     if (BEND) {
-        ax = fma(-L * c.irho * c.irho, lpx, fma(lirho, lam[5], ax));
-        lam[4] = fma(L * c.irho, lpx, lam[4]);
+        ax = fma(-L * irho * irho, lpx, fma(lirho, lam[5], ax));
+        lam[4] = fma(L * irho, lpx, lam[4]);
     }
     lam[0] += ax;
     lam[2] += ay;
@@ -215,18 +270,39 @@ __device__ __forceinline__ void adj_fastdrift(double px, double py, double h, do
     lnl += fma(lx, px, fma(ly, py, lc * S * h));
 }
 
-/* one Forest-Ruth step of the exact non-radiating kernel on r (the stage
- * order of StrMPoleSymplectic4Pass.c:73-93) */
-template <bool BEND, class PL>
-__device__ __forceinline__ void fr_step(P6& r, const PL& pl, double nl1, double nl2, double K1,
-                                        double K2, double irho, double k1i, double k2i) {
-    fastdrift<false>(r, nl1, 0.0);
-    if (BEND) bndthinkick(r, pl, K1, irho, k1i); else strthinkick(r, pl, K1);
-    fastdrift<false>(r, nl2, 0.0);
-    if (BEND) bndthinkick(r, pl, K2, irho, k2i); else strthinkick(r, pl, K2);
-    fastdrift<false>(r, nl2, 0.0);
-    if (BEND) bndthinkick(r, pl, K1, irho, k1i); else strthinkick(r, pl, K1);
-    fastdrift<false>(r, nl1, 0.0);
+/* The transverse coordinates inside a non-radiating magnet, where dp is
+ * constant and ct feeds nothing: what the recomputed steps carry. */
+struct XY {
+    double x, px, y, py;
+};
+
+__device__ __forceinline__ void xy_drift(XY& q, double nl) {
+    q.x = fma(nl, q.px, q.x);
+    q.y = fma(nl, q.py, q.y);
+}
+
+template <bool BEND, int MO>
+__device__ __forceinline__ void xy_kick(XY& q, const AdjCoef<MO>& c, double L, double irho,
+                                        double dp) {
+    double re, im;
+    c.field(q.x, q.y, re, im);
+    if (BEND) re = fma(-fma(-q.x, irho, dp), irho, re);     /* re - (dp - x irho) irho */
+    q.px = fma(-L, re, q.px);
+    q.py = fma(L, im, q.py);
+}
+
+/* one Forest-Ruth step (StrMPoleSymplectic4Pass.c:73-93) on the transverse
+ * coordinates */
+template <bool BEND, int MO>
+__device__ __forceinline__ void xy_step(XY& q, const AdjCoef<MO>& c, double nl1, double nl2,
+                                        double K1, double K2, double irho, double dp) {
+    xy_drift(q, nl1);
+    xy_kick<BEND>(q, c, K1, irho, dp);
+    xy_drift(q, nl2);
+    xy_kick<BEND>(q, c, K2, irho, dp);
+    xy_drift(q, nl2);
+    xy_kick<BEND>(q, c, K1, irho, dp);
+    xy_drift(q, nl1);
 }
 
 /* edge_fringe (methods other than 3, exact arithmetic) at input s:
@@ -265,20 +341,20 @@ __device__ __forceinline__ bool adj_by_hand(const Rec& e, bool bend) {
 }
 
 /* StrMPoleSymplectic4Pass.c:29-109 / BndMPoleSymplectic4Pass.c:38-129 in
- * reverse; `ss` is the thread's step-entry store */
-template <bool BEND>
-__device__ __forceinline__ void adj_pass_multipole(const P6& s, double* lam, const Rec& e,
-                                                   const Param& pm, double& g,
-                                                   double (*ss)[4]) {
+ * reverse; `ss` is the thread's step-entry store.  The entry transforms run
+ * in the tracking arithmetic from the stored entry state; the steps are
+ * recomputed on the transverse coordinates. */
+template <bool BEND, int MO>
+__device__ __forceinline__ void adj_multipole_mo(const P6& s, double* lam, const Rec& e,
+                                                 const Param& pm, double& g,
+                                                 double (*ss)[4]) {
     const uint32_t fl = e.flags();
     const double L1 = e.f(ATB_SM_L1), L2 = e.f(ATB_SM_L2);
     const double K1 = e.f(ATB_SM_K1), K2 = e.f(ATB_SM_K2);
     const int mo = e.mo();
     const double* A = e.p + (BEND ? ATB_BM_POLY : ATB_SM_POLY);
-    const double* B = A + mo + 1;
-    Poly<-1> pl;
-    pl.load(A, B, mo);
-    if (pm.k >= 0) pl.set_param(pm.k, pm.v);
+    AdjCoef<MO> c;
+    c.load(A, A + mo + 1, mo, pm.k, pm.v);
 
     /* forward to every step entry */
     P6 r = s;
@@ -297,52 +373,52 @@ __device__ __forceinline__ void adj_pass_multipole(const P6& s, double* lam, con
         edge_fringe<false>(r, irho, e.f(ATB_BM_EIN), e.f(ATB_BM_FCIN), e.f(ATB_BM_FXIN),
                            e.f(ATB_BM_FYIN), m_in, fl & ATB_F_FC0_IN, 1.0);
     }
-    const int ns = e.nsteps();
-    const int stride = ns > ATB_ADJ_STEPS ? (ns + ATB_ADJ_STEPS - 1) / ATB_ADJ_STEPS : 1;
-    for (int m = 0; m < ns; ++m) {
-        if (m % stride == 0) {
-            double* q = ss[m / stride];
-            q[0] = r.x; q[1] = r.px; q[2] = r.y; q[3] = r.py;
-        }
-        fr_step<BEND>(r, pl, nl1, nl2, K1, K2, irho, k1i, k2i);
-    }
     const double dp = r.dp;                  /* constant through the steps */
     const double h = 1.0 / (2.0 * (1.0 + dp));
+    const int ns = e.nsteps();
+    const int stride = ns > ATB_ADJ_STEPS ? (ns + ATB_ADJ_STEPS - 1) / ATB_ADJ_STEPS : 1;
+    XY q{r.x, r.px, r.y, r.py};
+    for (int m = 0; m < ns; ++m) {
+        if (m % stride == 0) {
+            double* w = ss[m / stride];
+            w[0] = q.x; w[1] = q.px; w[2] = q.y; w[3] = q.py;
+        }
+        xy_step<BEND>(q, c, nl1, nl2, K1, K2, irho, dp);
+    }
 
     /* reverse */
     adj_exit_misalign(lam, e);
-    if (BEND)
-        adj_edge(r, lam, irho, e.f(ATB_BM_EOUT), e.f(ATB_BM_FCOUT), e.f(ATB_BM_FXOUT),
+    if (BEND) {
+        P6 so;
+        so.x = q.x; so.px = q.px; so.y = q.y; so.py = q.py; so.dp = dp; so.ct = 0.0;
+        adj_edge(so, lam, irho, e.f(ATB_BM_EOUT), e.f(ATB_BM_FCOUT), e.f(ATB_BM_FXOUT),
                  e.f(ATB_BM_FYOUT), m_out);
-    const KickAdj kc{A, B, mo, pm.k, pm.v, irho};
+    }
     double lnl1 = 0.0, lnl2 = 0.0;
     for (int m = ns - 1; m >= 0; --m) {
-        const int c = m / stride;
-        P6 q;
-        q.x = ss[c][0]; q.px = ss[c][1]; q.y = ss[c][2]; q.py = ss[c][3];
-        q.dp = dp; q.ct = 0.0;
-        for (int j = c * stride; j < m; ++j)
-            fr_step<BEND>(q, pl, nl1, nl2, K1, K2, irho, k1i, k2i);
+        const int cb = m / stride;
+        XY t{ss[cb][0], ss[cb][1], ss[cb][2], ss[cb][3]};
+        for (int j = cb * stride; j < m; ++j) xy_step<BEND>(t, c, nl1, nl2, K1, K2, irho, dp);
         /* the step once more, keeping the input of every stage */
-        const double px0 = q.px, py0 = q.py;
-        fastdrift<false>(q, nl1, 0.0);
-        const double x1 = q.x, y1 = q.y;
-        if (BEND) bndthinkick(q, pl, K1, irho, k1i); else strthinkick(q, pl, K1);
-        const double px2 = q.px, py2 = q.py;
-        fastdrift<false>(q, nl2, 0.0);
-        const double x3 = q.x, y3 = q.y;
-        if (BEND) bndthinkick(q, pl, K2, irho, k2i); else strthinkick(q, pl, K2);
-        const double px4 = q.px, py4 = q.py;
-        fastdrift<false>(q, nl2, 0.0);
-        const double x5 = q.x, y5 = q.y;
-        if (BEND) bndthinkick(q, pl, K1, irho, k1i); else strthinkick(q, pl, K1);
-        const double px6 = q.px, py6 = q.py;
+        const double px0 = t.px, py0 = t.py;
+        xy_drift(t, nl1);
+        const double x1 = t.x, y1 = t.y;
+        xy_kick<BEND>(t, c, K1, irho, dp);
+        const double px2 = t.px, py2 = t.py;
+        xy_drift(t, nl2);
+        const double x3 = t.x, y3 = t.y;
+        xy_kick<BEND>(t, c, K2, irho, dp);
+        const double px4 = t.px, py4 = t.py;
+        xy_drift(t, nl2);
+        const double x5 = t.x, y5 = t.y;
+        xy_kick<BEND>(t, c, K1, irho, dp);
+        const double px6 = t.px, py6 = t.py;
         adj_fastdrift(px6, py6, h, nl1, lam, lnl1);
-        adj_kick<BEND>(kc, x5, y5, K1, k1i, lam, g);
+        adj_kick<BEND>(c, x5, y5, K1, k1i, irho, lam, g);
         adj_fastdrift(px4, py4, h, nl2, lam, lnl2);
-        adj_kick<BEND>(kc, x3, y3, K2, k2i, lam, g);
+        adj_kick<BEND>(c, x3, y3, K2, k2i, irho, lam, g);
         adj_fastdrift(px2, py2, h, nl2, lam, lnl2);
-        adj_kick<BEND>(kc, x1, y1, K1, k1i, lam, g);
+        adj_kick<BEND>(c, x1, y1, K1, k1i, irho, lam, g);
         adj_fastdrift(px0, py0, h, nl1, lam, lnl1);
     }
     if (BEND)
@@ -351,6 +427,19 @@ __device__ __forceinline__ void adj_pass_multipole(const P6& s, double* lam, con
     adj_entrance_misalign(lam, e);
     /* nl1, nl2 = L1, L2 / (1 + dp) of the entry momentum */
     lam[4] -= fma(lnl1, L1, lnl2 * L2) * pn0 * pn0;
+}
+
+template <bool BEND>
+__device__ __forceinline__ void adj_pass_multipole(const P6& s, double* lam, const Rec& e,
+                                                   const Param& pm, double& g,
+                                                   double (*ss)[4]) {
+    switch (e.mo()) {
+        case 0: adj_multipole_mo<BEND, 0>(s, lam, e, pm, g, ss); break;
+        case 1: adj_multipole_mo<BEND, 1>(s, lam, e, pm, g, ss); break;
+        case 2: adj_multipole_mo<BEND, 2>(s, lam, e, pm, g, ss); break;
+        case 3: adj_multipole_mo<BEND, 3>(s, lam, e, pm, g, ss); break;
+        default: adj_multipole_mo<BEND, -1>(s, lam, e, pm, g, ss); break;
+    }
 }
 
 /* ---- thin elements -------------------------------------------------------- */
@@ -395,8 +484,9 @@ __device__ __forceinline__ void adj_pass_thinmpole(const P6& s, double* lam, con
     lam[4] = fma(bax, lam[1], fma(-bay, lam[3], lam[4]));
     lam[0] = fma(-bax, lam[5], lam[0]);
     lam[2] = fma(bay, lam[5], lam[2]);
-    const KickAdj kc{A, B, mo, pm.k, pm.v, 0.0};
-    adj_kick<false>(kc, r.x, r.y, 1.0, 0.0, lam, g);
+    AdjCoef<-1> c;
+    c.load(A, B, mo, pm.k, pm.v);
+    adj_kick<false>(c, r.x, r.y, 1.0, 0.0, 0.0, lam, g);
     adj_entrance_misalign(lam, e);
 }
 

@@ -267,7 +267,6 @@ def _track_function():
         @staticmethod
         def backward(ctx, g):
             g_r0, g_k = ctx.tracker.backward(ctx.state, g.contiguous())
-            ctx.state = None
             return (g_r0 if ctx.needs_input_grad[0] else None,
                     g_k if ctx.needs_input_grad[1] else None, None, None, None)
 

@@ -14,7 +14,10 @@ and then puts itself back in a device-side continuation ring that the blocks
 take from after new work, so long requests share the GPU with short ones
 tile by tile (processor sharing) with no host step and no barrier between
 chunks.  Admission copies and result copies run on a side stream (copy
-engine) beside the kernel.  ``RoundServer`` is the earlier form: one
+engine) beside the kernel.  Admission keeps a few waves of tiles in flight
+and, by default, takes the waiting requests with the least work first (any
+request that has waited longer than ``max_wait`` goes ahead of them), so
+that under overload short requests do not queue behind long ones.  ``RoundServer`` is the earlier form: one
 ``atb_track_batch`` launch per round over every active request, new arrivals
 joining at the next round.
 
@@ -189,7 +192,8 @@ class TrackingServer:
 
     def __init__(self, lattices: dict, hbm_budget_bytes: float = 150e9, device: int = 0,
                  mode="exact", chunk_flops: float = 1e9, max_chunk: int = 512,
-                 max_jobs: int = 1 << 16, max_tiles: int = 1 << 22):
+                 max_jobs: int = 1 << 16, max_tiles: int = 1 << 22, policy: str = "sjf",
+                 waves: float = 4.0, max_wait: float = 30.0):
         import ctypes as C
 
         import torch
@@ -227,14 +231,47 @@ class TrackingServer:
         self.first_live = 0                   # lowest slot still polled
         self.particle_turns = 0
         self.launches_seen = 0
+        if policy not in ("sjf", "fifo"):
+            raise ValueError("policy must be 'sjf' or 'fifo'")
+        self.policy = policy
+        self.max_wait = float(max_wait)
+        sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
+        #: tiles in flight (admitted, not finished) above which nothing more is
+        #: admitted: a few waves of the persistent grid (two blocks per SM)
+        self.max_live_tiles = int(waves * 2 * sms)
+        self.live_tiles = 0
 
     # -- admission ----------------------------------------------------------------
+    def _work(self, req) -> float:
+        return req.n * req.nturns * self.fpt[req.lattice]
+
+    def _order(self, now: float) -> list:
+        """Admission order.  "fifo": arrival order.  "sjf": requests that have
+        waited longer than ``max_wait`` first (in arrival order), then the
+        others by increasing work (N x T x flops per particle-turn), which
+        keeps short requests from queueing behind long ones when the offered
+        load exceeds the GPU."""
+        if self.policy == "fifo":
+            return list(self.waiting)
+        old = [r for r in self.waiting if now - r.arrival > self.max_wait]
+        new = sorted((r for r in self.waiting if now - r.arrival <= self.max_wait),
+                     key=self._work)
+        return old + new
+
+    def _tiles(self, req) -> int:
+        return (req.n + self.TILE - 1) // self.TILE
+
     def _admit(self, now: float):
+        """Admit waiting requests (particles copied to HBM on the side stream)
+        while the HBM budget holds and fewer than ``max_live_tiles`` tiles are
+        in flight (one request is always admitted into an idle server)."""
         torch = self.torch
         keep = []
-        for req in self.waiting:
+        for req in self._order(now):
             need = req.n * BYTES_PER_PARTICLE
-            if self.used + need > self.budget:
+            busy = self.live_tiles > 0
+            if self.used + need > self.budget or (
+                    busy and self.live_tiles + self._tiles(req) > self.max_live_tiles):
                 keep.append(req)
                 continue
             n = req.n
@@ -251,9 +288,10 @@ class TrackingServer:
                 ev.record(self.copy)
             req.dev, req._host, req._event = d, host, ev
             self.used += need
+            self.live_tiles += self._tiles(req)
             req.admitted = now
             self.staging.append(req)
-        self.waiting = keep
+        self.waiting = sorted(keep, key=lambda r: r.arrival)
 
     TILE = 256                                # particles per tile (the kernel's block)
 
@@ -308,6 +346,7 @@ class TrackingServer:
                 moved += 1
                 req.done_turns = req.nturns
                 self.particle_turns += req.n * req.nturns
+                self.live_tiles -= self._tiles(req)
                 self.active.remove(req)
                 with torch.cuda.stream(self.copy):
                     for k in req.dev:

@@ -736,6 +736,9 @@ def run_diff(device, n=65536):
                        "orbit, %d strengths (64 quadrupole + 64 sextupole)" % (n, len(params))}
     eng = Engine.get(device)
     lid = eng.upload(tr.cl)
+    # the exact tracking runs on a stream of its own with its events (the
+    # legacy default stream's handle would read as NULL: the engine's stream)
+    trk = torch.cuda.Stream(dev)
     try:
         for nt in (1, 100):
             tr.track(x, None, nt)                     # warm-up
@@ -772,15 +775,15 @@ def run_diff(device, n=65536):
                 return float(((a - b).abs().max() / b.abs().max()).item())
             # one exact-mode tracking of the same particles (device resident)
             xr = x.clone()
-            eng.track_device(lid, xr.data_ptr(), n, nt, mode="exact",
-                             stream=torch.cuda.current_stream(dev).cuda_stream)
+            trk.wait_stream(torch.cuda.current_stream(dev))
+            eng.track_device(lid, xr.data_ptr(), n, nt, mode="exact", stream=trk.cuda_stream)
             xr = x.clone()
-            e0.record()
-            eng.track_device(lid, xr.data_ptr(), n, nt, mode="exact",
-                             stream=torch.cuda.current_stream(dev).cuda_stream)
-            e1.record()
+            trk.wait_stream(torch.cuda.current_stream(dev))
+            e0.record(trk)
+            eng.track_device(lid, xr.data_ptr(), n, nt, mode="exact", stream=trk.cuda_stream)
+            e1.record(trk)
             e1.synchronize()
-            eng.sync(torch.cuda.current_stream(dev).cuda_stream)
+            eng.sync(trk.cuda_stream)
             t_trk = e0.elapsed_time(e1) * 1e-3
             runs = 2 * len(params) + 12
             out["turns_%d" % nt] = {

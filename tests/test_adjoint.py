@@ -137,7 +137,7 @@ def test_stride_does_not_change_the_gradients():
     for r, gr0, gk, _ in out[1:]:
         assert torch.equal(r, out[0][0])
         assert torch.equal(gr0, out[0][1])
-        assert torch.allclose(gk, out[0][2], rtol=1e-14, atol=0)   # atomic sums
+        assert _scale_rel(gk.cpu(), out[0][2].cpu()) <= 1e-13   # sums in atomic order
 
 
 @pytest.mark.gpu
