@@ -1575,7 +1575,8 @@ int atb_serve_open(atb_handle* h, const int32_t* lattice_ids, int32_t nlat, int3
     return ATB_OK;
 }
 
-int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns, int32_t* slot) {
+int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns, int32_t* pidx,
+                     int32_t* slot) {
     if (!s || !d || !slot) return fail(ATB_ERR_ARG, "NULL argument");
     if (chunk_turns < 0) return fail(ATB_ERR_ARG, "negative chunk");
     atb_handle* h = s->h;
@@ -1606,6 +1607,7 @@ int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns, 
     J.lelem = d->lelem;
     J.lcoord = d->lcoord;
     J.chunk = chunk_turns;
+    J.pidx = pidx;
     if (ntl > s->h_tiles_cap) {
         if (s->h_tiles) cudaFreeHost(s->h_tiles);
         s->h_tiles = nullptr;

@@ -116,6 +116,9 @@ typedef struct AtbJob {
     int32_t chunk;              /* serving: turns per claim, 0 all (a tile
                                    re-enqueues itself for the rest)         */
     int32_t pad_chunk;
+    int32_t* pidx;              /* serving, optional: the particle at each
+                                   tile position; a re-enqueued tile keeps
+                                   only its live particles, packed first    */
 } AtbJob;
 
 /* Whether a job's particles may be handed out through a per-job cursor with

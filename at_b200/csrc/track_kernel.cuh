@@ -907,6 +907,9 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
         for (int k = 0; k < NP; ++k) {
             p[k] = first + (long long)k * nthr + tid;
             active[k] = (k * nthr + tid) < count;
+            if constexpr (SERVE) {
+                if (J.pidx && active[k]) p[k] = __ldcg(J.pidx + p[k]);
+            }
             lt0[k] = 0;
             lost[k] = false;
             if (active[k]) {
@@ -1218,26 +1221,59 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
             /* the chunk is stored and visible device-wide: a tile with live
                particles and turns left goes back to the continuation ring
                (or, if the ring is full, stays with this block); otherwise its
-               particles count as done */
+               particles count as done.  With a particle index (NP = 1) the
+               tile keeps only its live particles, their indices packed at
+               the front of its range, and the others count as done now. */
             __threadfence();
             bool live = false;
 #pragma unroll
             for (int k = 0; k < NP; ++k)
                 live |= active[k] && !isnan(r[k].x) && !(J.losses && lost[k]);
-            const int any = __syncthreads_or(live);
+            const int nlive = __syncthreads_count(live);
+            const bool more = nlive > 0 && s_toff + J.nturns < s_full;
+            int keep_count = count;
+            if (NP == 1 && J.pidx && more && nlive < count) {
+                const unsigned ball = __ballot_sync(0xffffffffu, live);
+                const int lane = tid & 31, warp = tid >> 5;
+                if (lane == 0) s_warp[warp] = __popc(ball);
+                __syncthreads();
+                if (tid == 0) {
+                    int acc = 0;
+                    for (int w = 0; w < (nthr + 31) / 32; ++w) {
+                        const int c = s_warp[w];
+                        s_warp[w] = acc;
+                        acc += c;
+                    }
+                }
+                __syncthreads();
+                if (live) {
+                    const int rank = s_warp[warp] + __popc(ball & ((1u << lane) - 1u));
+                    J.pidx[tile.first + rank] = (int32_t)p[0];
+                }
+                __threadfence();
+                __syncthreads();
+                keep_count = nlive;
+            }
             if (tid == 0) {
                 const int ran = s_toff + J.nturns;
                 bool requeued = false, keep = false;
-                if (any && ran < s_full && !sv.ctl->stop) {
-                    requeued = serve_requeue(sv.ring, tile, ran);
+                if (more && !sv.ctl->stop) {
+                    AtbTile nt = tile;
+                    nt.count = keep_count;
+                    requeued = serve_requeue(sv.ring, nt, ran);
                     if (!requeued) {
                         atomicOr(status, ATB_STATUS_RING_FULL);
                         keep = true;
                         s_toff = ran;
+                        s_ctile = nt;
                     }
                 }
-                if (!requeued && !keep && !(any && ran < s_full))
+                if (requeued || keep) {
+                    if (keep_count < taken)
+                        atomicAdd(&sv.done[tile.job], (unsigned long long)(taken - keep_count));
+                } else if (!more) {
                     atomicAdd(&sv.done[tile.job], (unsigned long long)taken);
+                }
                 if (!keep) atomicSub(sv.inflight, 1);
                 s_self = keep ? 1 : 0;
             }

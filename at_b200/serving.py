@@ -39,7 +39,7 @@ from .engine import Engine, mode_code
 from .lattice import compile_lattice
 from .tracking import gpupass
 
-BYTES_PER_PARTICLE = 48 + 1 + 4 + 4 + 48      # state + loss map
+BYTES_PER_PARTICLE = 48 + 1 + 4 + 4 + 48 + 4  # state + loss map + particle index
 
 
 @dataclass
@@ -193,7 +193,7 @@ class TrackingServer:
     def __init__(self, lattices: dict, hbm_budget_bytes: float = 150e9, device: int = 0,
                  mode="exact", chunk_flops: float = 1e9, max_chunk: int = 512,
                  max_jobs: int = 1 << 16, max_tiles: int = 1 << 22, policy: str = "sjf",
-                 waves: float = 4.0, max_wait: float = 30.0):
+                 waves: float = 4.0, max_wait: float = 30.0, pack: bool = True):
         import ctypes as C
 
         import torch
@@ -240,6 +240,10 @@ class TrackingServer:
         #: admitted: a few waves of the persistent grid (two blocks per SM)
         self.max_live_tiles = int(waves * 2 * sms)
         self.live_tiles = 0
+        #: re-enqueued tiles keep only their live particles (a per-request
+        #: particle index, filled from a pinned 0..n-1 on the copy stream)
+        self.pack = bool(pack)
+        self._iota = torch.empty(0, dtype=torch.int32)
 
     # -- admission ----------------------------------------------------------------
     def _work(self, req) -> float:
@@ -281,9 +285,16 @@ class TrackingServer:
                     "lelem": torch.zeros(n, dtype=torch.int32).pin_memory(),
                     "lcoord": torch.zeros((n, 6), dtype=torch.float64).pin_memory()}
             d = {k: torch.empty(v.shape, dtype=v.dtype, device=self.dev) for k, v in host.items()}
+            if self.pack:
+                if self._iota.numel() < n:
+                    self._iota = torch.arange(max(n, 2 * self._iota.numel()),
+                                              dtype=torch.int32).pin_memory()
+                d["pidx"] = torch.empty(n, dtype=torch.int32, device=self.dev)
             with torch.cuda.stream(self.copy):
-                for k in d:
+                for k in host:
                     d[k].copy_(host[k], non_blocking=True)    # copy engine, beside the kernel
+                if self.pack:
+                    d["pidx"].copy_(self._iota[:n], non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(self.copy)
             req.dev, req._host, req._event = d, host, ev
@@ -316,7 +327,8 @@ class TrackingServer:
         jd.islost, jd.lturn = d["lost"].data_ptr(), d["lturn"].data_ptr()
         jd.lelem, jd.lcoord = d["lelem"].data_ptr(), d["lcoord"].data_ptr()
         slot = C.c_int32(-1)
-        self.check(self.lib.atb_serve_submit(self.srv, C.byref(jd), self._chunk(req),
+        pidx = d["pidx"].data_ptr() if "pidx" in d else None
+        self.check(self.lib.atb_serve_submit(self.srv, C.byref(jd), self._chunk(req), pidx,
                                              C.byref(slot)))
         req._slot = slot.value
         self.jobs = slot.value + 1
@@ -349,7 +361,7 @@ class TrackingServer:
                 self.live_tiles -= self._tiles(req)
                 self.active.remove(req)
                 with torch.cuda.stream(self.copy):
-                    for k in req.dev:
+                    for k in req._host:
                         req._host[k].copy_(req.dev[k], non_blocking=True)
                     ev = torch.cuda.Event()
                     ev.record(self.copy)

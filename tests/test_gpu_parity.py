@@ -9,7 +9,9 @@ Tolerances (stated per test):
     the FODO ring, 2e-13 after one turn of the 2,000-element large ring;
   * 1000 turns at the workloads' own sizes (FODO: 10,000 particles; large
     ring: 2048), against the reference's own engine: 1e-9 scale-relative on
-    particles that survive in both, and the same lost set, loss turns and
+    stable particles that survive in both (a survivor beyond 1e-9 must be
+    unstable in the reference's own arithmetic: copies of it started one ulp
+    apart end more than 1e-9 apart), and the same lost set, loss turns and
     loss elements except for particles whose loss coordinate lies within 1e-9
     (relative) of the amplitude limit or of the loss element's aperture, or
     whose fate is ill-conditioned (changes when its start moves by one ulp
@@ -145,14 +147,41 @@ def _ill_conditioned(line, r0, idx, nturns, energy, rest):
     return np.array(out, dtype=bool)
 
 
+def _unstable(line, r0, idx, nturns, energy, rest, scale, tol):
+    """Per particle of ``idx`` (a survivor in both runs): is its final state
+    sensitive beyond ``tol`` (of each coordinate's ``scale``) to its start at
+    the rounding level?  The oracle tracks it in the reference's arithmetic
+    and twelve copies with one coordinate moved by one ulp either way; a
+    particle whose copies end more than ``tol`` apart is not a stable particle
+    (its orbit is chaotic near the dynamic aperture, where any rounding
+    difference grows turn by turn)."""
+    out = []
+    for i in idx:
+        base = r0[:, i]
+        cols = [base]
+        for c in range(6):
+            for d in (np.inf, -np.inf):
+                p = base.copy()
+                p[c] = np.nextafter(p[c], d)
+                cols.append(p)
+        r = np.asfortranarray(np.stack(cols, axis=1))
+        oracle.track(line, r, nturns, energy=energy, rest_energy=rest)
+        ok = np.all(np.isfinite(r), axis=0)
+        spread = np.abs(r[:, ok] - r[:, :1]).max(axis=1) / scale if ok[0] else np.inf
+        out.append(bool(np.any(spread > tol)) or not ok.all())
+    return np.array(out, dtype=bool)
+
+
 def _compare_long_run(line, r0, rg, lg, g, energy, rest):
     """The engine's 1000-turn result against the reference's (fixture ``g``).
     A particle may be lost in one and not the other, or lost at another turn
     or element, only if its loss coordinate lies within 1e-9 of a limit or
     its fate is ill-conditioned (changes under a one-ulp move of its start,
-    _ill_conditioned).  Survivors agree within 1e-9 of each coordinate's
-    scale.  Returns the counts of lost-set flips and of loss turn/element
-    differences."""
+    _ill_conditioned).  Stable survivors agree within 1e-9 of each
+    coordinate's scale; a survivor beyond that must be unstable in the
+    reference's own arithmetic (_unstable).  Returns the counts of lost-set
+    flips, of loss turn/element differences and of unstable survivors
+    beyond 1e-9."""
     lo = {"islost": g["islost"].astype(bool), "turn": g["lturn"], "elem": g["lelem"],
           "coord": g["lcoord"]}
     nb = _near_boundary(line, lo) | _near_boundary(line, lg)
@@ -162,9 +191,14 @@ def _compare_long_run(line, r0, rg, lg, g, energy, rest):
     suspect = np.flatnonzero((flip | moved) & ~nb)
     ill = _ill_conditioned(line, r0, suspect, int(g["nturns"]), energy, rest)
     assert ill.all(), "loss differs for well-conditioned particles: %s" % suspect[~ill]
-    both = ~lo["islost"] & ~lg["islost"]
-    assert scale_rel_diff(rg[:, both], g["rout_final"][:, both]) <= 1e-9
-    return int(flip.sum()), int(moved.sum())
+    both = np.flatnonzero(~lo["islost"] & ~lg["islost"])
+    ref = g["rout_final"][:, both]
+    scale = np.maximum(np.abs(ref).max(axis=1), 1e-300)
+    dev = (np.abs(rg[:, both] - ref) / scale[:, None]).max(axis=0)
+    far = both[dev > 1e-9]
+    unst = _unstable(line, r0, far, int(g["nturns"]), energy, rest, scale, 1e-9)
+    assert unst.all(), "stable survivors beyond 1e-9: %s" % far[~unst]
+    return int(flip.sum()), int(moved.sum()), int(far.size)
 
 
 def _check_input(r0, g):
@@ -183,9 +217,10 @@ def test_fodo_1000_turns_full_size(golden, mode):
     _check_input(r0, g)
     rg = r0.copy(order="F")
     _, lg, _ = _gpu_track(ring, rg, int(g["nturns"]), 3e9, ELECTRON_REST, mode, losses=True)
-    flips, moved = _compare_long_run(ring, r0, rg, lg, g, 3e9, ELECTRON_REST)
-    print("FODO 10000 x 1000 (%s): %d lost-set flips, %d loss-turn differences, %d lost"
-          % (mode, flips, moved, int(lg["islost"].sum())))
+    flips, moved, far = _compare_long_run(ring, r0, rg, lg, g, 3e9, ELECTRON_REST)
+    print("FODO 10000 x 1000 (%s): %d lost-set flips, %d loss-turn differences, %d lost, "
+          "%d unstable survivors beyond 1e-9" % (mode, flips, moved, int(lg["islost"].sum()),
+                                                 far))
     assert 0.2 < lg["islost"].mean() < 0.45          # the workload loses about 30 %
 
 
@@ -200,10 +235,12 @@ def test_large_ring_1000_turns_full_size(golden, mode):
     rg = r0.copy(order="F")
     _, lg, _ = _gpu_track(ring, rg, int(g["nturns"]), ring.energy, ring.particle.rest_energy,
                           mode, losses=True)
-    flips, moved = _compare_long_run(ring, r0, rg, lg, g, ring.energy,
-                                     ring.particle.rest_energy)
-    print("large ring 2048 x 1000 (%s): %d lost-set flips, %d loss-turn differences, %d lost"
-          % (mode, flips, moved, int(lg["islost"].sum())))
+    flips, moved, far = _compare_long_run(ring, r0, rg, lg, g, ring.energy,
+                                          ring.particle.rest_energy)
+    print("large ring 2048 x 1000 (%s): %d lost-set flips, %d loss-turn differences, %d lost, "
+          "%d unstable survivors beyond 1e-9" % (mode, flips, moved, int(lg["islost"].sum()),
+                                                 far))
+    assert far == 0                       # radiation damping: every survivor is stable
 
 
 @pytest.mark.parametrize("mode", ["exact", "fast"])

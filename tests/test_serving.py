@@ -104,16 +104,18 @@ def test_device_resident_server_results_equal_alone(mode):
 
 
 @pytest.mark.gpu
-def test_device_resident_chunks_keep_results_with_losses():
+@pytest.mark.parametrize("pack", [True, False])
+def test_device_resident_chunks_keep_results_with_losses(pack):
     """Chunks of one turn on a bunch that loses particles along the way: the
-    loss turn, element and coordinates carry over from chunk to chunk."""
+    loss turn, element and coordinates carry over from chunk to chunk, with
+    the tiles packed to their live particles at every chunk end or not."""
     lats, orbits = rings.serving_pool(1, 1)
     reqs = serving.make_trace(list(lats), 3, rate_hz=1000.0, seed=11, n_range=(600, 1500),
                               t_range=(40, 60), centre_of=orbits.get)
     for r in reqs:                                          # far out: losses over many turns
         c = orbits[r.lattice][[0, 2], None]
         r.particles[[0, 2]] = c + 6.0 * (r.particles[[0, 2]] - c)
-    srv = serving.TrackingServer(lats, chunk_flops=1.0)       # one turn per claim
+    srv = serving.TrackingServer(lats, chunk_flops=1.0, pack=pack)   # one turn per claim
     try:
         srv.serve(reqs)
         c = srv.counters()
