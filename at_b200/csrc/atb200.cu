@@ -173,7 +173,7 @@ struct atb_server {
     AtbServeCtl* ctl = nullptr;         /* host view of the mapped control words */
     AtbServeCtl* dctl = nullptr;        /* its device address                    */
     DevBuf jobs, tiles, counter, status, jobnext, done, compact;
-    DevBuf ring, ring_ctr;              /* continuation ring; head, tail, inflight */
+    DevBuf ring, ring_ctr;              /* continuation rings; heads, tails, inflight */
     int ring_cap = 0;
     unsigned long long* h_done = nullptr;   /* pinned: done counters, claim counter,
                                                ring cursors                       */
@@ -1450,15 +1450,41 @@ namespace {
 static_assert(sizeof(AtbTile) == 16 && sizeof(AtbServeCont) == 32,
               "the serving kernel reads tiles with 16-byte vector loads");
 
+/* the ring cursors: ATB_SERVE_CLASSES heads, as many tails, the in-flight
+   count (and one spare) */
+constexpr int kRingCtr = 2 * ATB_SERVE_CLASSES + 2;
+
+/* The continuation rings' cursors, read through pinned memory: whether any
+   ring holds work, and the entries written and taken over all rings. */
+int ring_cursors(atb_server* s, bool* pending, long long* written, long long* taken) {
+    int* hc = reinterpret_cast<int*>(&s->h_done[s->max_jobs + 2]);
+    ATB_CUDA(cudaMemcpyAsync(hc, s->ring_ctr.p, 2 * ATB_SERVE_CLASSES * sizeof(int),
+                             cudaMemcpyDeviceToHost, s->cstream));
+    ATB_CUDA(cudaStreamSynchronize(s->cstream));
+    bool p = false;
+    long long w = 0, t = 0;
+    for (int q = 0; q < ATB_SERVE_CLASSES; ++q) {
+        const int h = hc[q], tl = hc[ATB_SERVE_CLASSES + q];
+        p |= h < tl;
+        w += tl;
+        t += h;
+    }
+    if (pending) *pending = p;
+    if (written) *written = w;
+    if (taken) *taken = t;
+    return ATB_OK;
+}
+
 AtbServeArgs serve_args(atb_server* s) {
     AtbServeArgs a;
     std::memset(&a, 0, sizeof(a));
     a.ctl = s->dctl;
     a.ring.slots = s->ring.as<AtbServeCont>();
     a.ring.cap = s->ring_cap;
+    a.ring.nring = ATB_SERVE_CLASSES;
     a.ring.head = s->ring_ctr.as<int>();
-    a.ring.tail = s->ring_ctr.as<int>() + 1;
-    a.inflight = s->ring_ctr.as<int>() + 2;
+    a.ring.tail = s->ring_ctr.as<int>() + ATB_SERVE_CLASSES;
+    a.inflight = s->ring_ctr.as<int>() + 2 * ATB_SERVE_CLASSES;
     a.done = s->done.as<unsigned long long>();
     return a;
 }
@@ -1550,14 +1576,15 @@ int atb_serve_open(atb_handle* h, const int32_t* lattice_ids, int32_t nlat, int3
        live tile has at most one entry) */
     s->ring_cap = 1;
     while (s->ring_cap < max_tiles + 128) s->ring_cap <<= 1;
-    if (s->ring.ensure((size_t)s->ring_cap * sizeof(AtbServeCont)) != cudaSuccess ||
-        s->ring_ctr.ensure(4 * sizeof(int)) != cudaSuccess)
+    if (s->ring.ensure((size_t)ATB_SERVE_CLASSES * s->ring_cap * sizeof(AtbServeCont)) !=
+            cudaSuccess ||
+        s->ring_ctr.ensure(kRingCtr * sizeof(int)) != cudaSuccess)
         return fail(ATB_ERR_NOMEM, "cudaMalloc(continuation ring) failed");
     ATB_CUDA(cudaHostAlloc((void**)&s->ctl, sizeof(AtbServeCtl), cudaHostAllocMapped));
     ATB_CUDA(cudaHostGetDevicePointer((void**)&s->dctl, s->ctl, 0));
     s->ctl->published = 0;
     s->ctl->stop = 0;
-    ATB_CUDA(cudaHostAlloc((void**)&s->h_done, ((size_t)max_jobs + 2) * sizeof(unsigned long long),
+    ATB_CUDA(cudaHostAlloc((void**)&s->h_done, ((size_t)max_jobs + 2 + ATB_SERVE_CLASSES) * sizeof(unsigned long long),
                            cudaHostAllocDefault));
     ATB_CUDA(cudaHostAlloc((void**)&s->h_job, sizeof(AtbJob), cudaHostAllocDefault));
     ATB_CUDA(cudaHostAlloc((void**)&s->h_zero, 2 * sizeof(unsigned long long),
@@ -1567,16 +1594,17 @@ int atb_serve_open(atb_handle* h, const int32_t* lattice_ids, int32_t nlat, int3
     ATB_CUDA(cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking));
     ATB_CUDA(cudaMemsetAsync(s->counter.p, 0, sizeof(int), s->cstream));
     ATB_CUDA(cudaMemsetAsync(s->status.p, 0, sizeof(int), s->cstream));
-    ATB_CUDA(cudaMemsetAsync(s->ring_ctr.p, 0, 4 * sizeof(int), s->cstream));
-    ATB_CUDA(cudaMemsetAsync(s->ring.p, 0, (size_t)s->ring_cap * sizeof(AtbServeCont),
+    ATB_CUDA(cudaMemsetAsync(s->ring_ctr.p, 0, kRingCtr * sizeof(int), s->cstream));
+    ATB_CUDA(cudaMemsetAsync(s->ring.p, 0,
+                             (size_t)ATB_SERVE_CLASSES * s->ring_cap * sizeof(AtbServeCont),
                              s->cstream));
     ATB_CUDA(cudaStreamSynchronize(s->cstream));
     *out = s.release();
     return ATB_OK;
 }
 
-int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns, int32_t* pidx,
-                     int32_t* slot) {
+int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns, int32_t prio,
+                     int32_t* pidx, int32_t* slot) {
     if (!s || !d || !slot) return fail(ATB_ERR_ARG, "NULL argument");
     if (chunk_turns < 0) return fail(ATB_ERR_ARG, "negative chunk");
     atb_handle* h = s->h;
@@ -1607,6 +1635,7 @@ int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns, 
     J.lelem = d->lelem;
     J.lcoord = d->lcoord;
     J.chunk = chunk_turns;
+    J.prio = std::max(0, std::min(prio, ATB_SERVE_CLASSES - 1));
     J.pidx = pidx;
     if (ntl > s->h_tiles_cap) {
         if (s->h_tiles) cudaFreeHost(s->h_tiles);
@@ -1664,12 +1693,13 @@ int atb_serve_poll(atb_server* s, int32_t first, int32_t nslots, uint64_t* done,
     if (serve_finished(s)) {
         /* the kernel left: a failed wait is an error; after an idle exit it
            is launched again while published or re-enqueued work waits */
-        int ring[3] = {0, 0, 0};
+        bool pending = false;
         ATB_CUDA(cudaMemcpy(&status, s->status.p, sizeof(int), cudaMemcpyDeviceToHost));
-        ATB_CUDA(cudaMemcpy(ring, s->ring_ctr.p, 3 * sizeof(int), cudaMemcpyDeviceToHost));
+        const int rr = ring_cursors(s, &pending, nullptr, nullptr);
+        if (rr) return rr;
         if (status & ATB_STATUS_WAIT_TIMEOUT)
             return fail(ATB_ERR_TIMEOUT, "a bounded shared-memory staging wait timed out");
-        if ((claimed < s->ntiles || ring[0] < ring[1]) && !s->ctl->stop) {
+        if ((claimed < s->ntiles || pending) && !s->ctl->stop) {
             int rc = serve_launch(s);
             if (rc) return rc;
         }
@@ -1681,18 +1711,18 @@ int atb_serve_poll(atb_server* s, int32_t first, int32_t nslots, uint64_t* done,
 int atb_serve_counters(atb_server* s, int32_t* out) {
     if (!s || !out) return fail(ATB_ERR_ARG, "NULL argument");
     DeviceGuard g(s->h->device);
-    int c = 0, ring[2] = {0, 0};
+    int c = 0;
     ATB_CUDA(cudaMemcpyAsync(&s->h_done[s->max_jobs], s->counter.p, sizeof(int),
-                             cudaMemcpyDeviceToHost, s->cstream));
-    ATB_CUDA(cudaMemcpyAsync(&s->h_done[s->max_jobs + 1], s->ring_ctr.p, 2 * sizeof(int),
                              cudaMemcpyDeviceToHost, s->cstream));
     ATB_CUDA(cudaStreamSynchronize(s->cstream));
     std::memcpy(&c, &s->h_done[s->max_jobs], sizeof(int));
-    std::memcpy(ring, &s->h_done[s->max_jobs + 1], 2 * sizeof(int));
+    long long w = 0, t = 0;
+    const int rr = ring_cursors(s, nullptr, &w, &t);
+    if (rr) return rr;
     out[0] = s->ntiles;
     out[1] = c;
-    out[2] = ring[1];
-    out[3] = ring[0];
+    out[2] = (int32_t)std::min<long long>(w, INT32_MAX);
+    out[3] = (int32_t)std::min<long long>(t, INT32_MAX);
     return ATB_OK;
 }
 
@@ -1706,13 +1736,15 @@ int atb_serve_reset(atb_server* s) {
     ATB_CUDA(cudaMemcpy(&claimed, s->counter.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (claimed < s->ntiles)
         return fail(ATB_ERR_ARG, "reset with published work unclaimed");
-    int ring[3] = {0, 0, 0};
-    ATB_CUDA(cudaMemcpy(ring, s->ring_ctr.p, 3 * sizeof(int), cudaMemcpyDeviceToHost));
-    if (ring[0] < ring[1]) return fail(ATB_ERR_ARG, "reset with continuations pending");
+    bool pending = false;
+    const int rr = ring_cursors(s, &pending, nullptr, nullptr);
+    if (rr) return rr;
+    if (pending) return fail(ATB_ERR_ARG, "reset with continuations pending");
     ATB_CUDA(cudaMemset(s->counter.p, 0, sizeof(int)));
     ATB_CUDA(cudaMemset(s->status.p, 0, sizeof(int)));
-    ATB_CUDA(cudaMemset(s->ring_ctr.p, 0, 4 * sizeof(int)));
-    ATB_CUDA(cudaMemset(s->ring.p, 0, (size_t)s->ring_cap * sizeof(AtbServeCont)));
+    ATB_CUDA(cudaMemset(s->ring_ctr.p, 0, kRingCtr * sizeof(int)));
+    ATB_CUDA(cudaMemset(s->ring.p, 0,
+                        (size_t)ATB_SERVE_CLASSES * s->ring_cap * sizeof(AtbServeCont)));
     s->njobs = 0;
     s->ntiles = 0;
     s->ctl->published = 0;

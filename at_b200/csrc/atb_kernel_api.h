@@ -54,14 +54,16 @@ typedef struct AtbServeCont {
     int64_t pad;
 } AtbServeCont;
 
-/* The serving loop's device-side queue: the continuation ring and its
-   cursors (device memory). */
+/* The serving loop's device-side queue: one continuation ring per priority
+   class (class 0 first) and their cursors (device memory). */
+#define ATB_SERVE_CLASSES 8
+
 typedef struct AtbServeRing {
-    AtbServeCont* slots;
-    int32_t cap;                /* entries (power of two)                   */
-    int32_t pad;
-    int* head;                  /* next entry to claim                      */
-    int* tail;                  /* next entry to write                      */
+    AtbServeCont* slots;        /* nring rings of cap entries               */
+    int32_t cap;                /* entries per ring (power of two)          */
+    int32_t nring;
+    int* head;                  /* per ring: next entry to claim            */
+    int* tail;                  /* per ring: next entry to write            */
 } AtbServeRing;
 
 #define ATB_STATUS_RING_FULL 8    /* a continuation found the ring full and
@@ -115,7 +117,7 @@ typedef struct AtbJob {
     uint64_t rng_key;           /* key of the quantum-diffusion kicks      */
     int32_t chunk;              /* serving: turns per claim, 0 all (a tile
                                    re-enqueues itself for the rest)         */
-    int32_t pad_chunk;
+    int32_t prio;               /* serving: continuation class, 0 first     */
     int32_t* pidx;              /* serving, optional: the particle at each
                                    tile position; a re-enqueued tile keeps
                                    only its live particles, packed first    */

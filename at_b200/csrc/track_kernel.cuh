@@ -692,9 +692,9 @@ __device__ __forceinline__ int seg_at(const AtbJob& J, long long q) {
 /* The serving loop's claim (one thread per block).  New work first: the
  * next tile the host has published (taken by compare-and-swap on the counter
  * only while it is below `published`, so a block never holds a claim the host
- * has not published).  Then the continuation ring: a tile that has run a
- * chunk of its job's turns and waits for the next (an entry is taken once
- * its `seq` shows it written).  Without work the block sleeps between looks;
+ * has not published).  Then the continuation rings, class 0 first: a tile
+ * that has run a chunk of its job's turns and waits for the next (an entry is
+ * taken once its `seq` shows it written).  Without work the block sleeps between looks;
  * it leaves when the host sets `stop`, or after ATB_SERVE_IDLE_NS with
  * nothing claimed anywhere (no tile in flight that could still re-enqueue),
  * or after a hundred times that while tiles are in flight.  Returns 1 with
@@ -719,22 +719,26 @@ __device__ __forceinline__ int serve_claim(const AtbServeCtl* ctl, int* counter,
             }
             continue;                            /* another block took it */
         }
-        const int h = atomicAdd(ring.head, 0);
-        const int t = atomicAdd(ring.tail, 0);
-        if (h < t) {
-            const AtbServeCont* e = ring.slots + (h & (ring.cap - 1));
-            if (__ldcg(&e->seq) == h + 1) {
-                if (atomicCAS(ring.head, h, h + 1) == h) {
-                    atomicAdd(inflight, 1);
-                    __threadfence();
-                    const int4 tw = __ldcg(reinterpret_cast<const int4*>(&e->tile));
-                    *tile = *reinterpret_cast<const AtbTile*>(&tw);
-                    *turn_off = __ldcg(&e->turn_off);
-                    return 1;
-                }
-                continue;
+        /* continuations, the lowest class first; an entry reserved by a
+           producer and not yet written, or lost to another block, sends the
+           claim back to the top */
+        bool again = false;
+        for (int q = 0; q < ring.nring && !again; ++q) {
+            const int h = atomicAdd(ring.head + q, 0);
+            const int t = atomicAdd(ring.tail + q, 0);
+            if (h >= t) continue;
+            const AtbServeCont* e = ring.slots + (size_t)q * ring.cap + (h & (ring.cap - 1));
+            if (__ldcg(&e->seq) == h + 1 && atomicCAS(ring.head + q, h, h + 1) == h) {
+                atomicAdd(inflight, 1);
+                __threadfence();
+                const int4 tw = __ldcg(reinterpret_cast<const int4*>(&e->tile));
+                *tile = *reinterpret_cast<const AtbTile*>(&tw);
+                *turn_off = __ldcg(&e->turn_off);
+                return 1;
             }
-            /* reserved by a producer and not yet written: look again */
+            again = true;
+        }
+        if (again) {
             t0 = global_ns();
             continue;
         }
@@ -749,14 +753,15 @@ __device__ __forceinline__ int serve_claim(const AtbServeCtl* ctl, int* counter,
 }
 
 /* Put a tile that has run `turn_off` turns of its job back in the
- * continuation ring.  Returns false if the ring is full. */
+ * continuation ring of class q.  Returns false if that ring is full. */
 __device__ __forceinline__ bool serve_requeue(const AtbServeRing& ring, const AtbTile& tile,
-                                              int turn_off) {
-    const int h = atomicAdd(ring.head, 0);
-    const int t = atomicAdd(ring.tail, 0);
+                                              int turn_off, int q) {
+    q = q < 0 ? 0 : (q >= ring.nring ? ring.nring - 1 : q);
+    const int h = atomicAdd(ring.head + q, 0);
+    const int t = atomicAdd(ring.tail + q, 0);
     if (t - h >= ring.cap - 64) return false;      /* leave room for racing producers */
-    const int idx = atomicAdd(ring.tail, 1);
-    AtbServeCont* e = ring.slots + (idx & (ring.cap - 1));
+    const int idx = atomicAdd(ring.tail + q, 1);
+    AtbServeCont* e = ring.slots + (size_t)q * ring.cap + (idx & (ring.cap - 1));
     e->tile = tile;
     e->turn_off = turn_off;
     __threadfence();
@@ -1260,7 +1265,7 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                 if (more && !sv.ctl->stop) {
                     AtbTile nt = tile;
                     nt.count = keep_count;
-                    requeued = serve_requeue(sv.ring, nt, ran);
+                    requeued = serve_requeue(sv.ring, nt, ran, J.prio);
                     if (!requeued) {
                         atomicOr(status, ATB_STATUS_RING_FULL);
                         keep = true;

@@ -14,10 +14,12 @@ and then puts itself back in a device-side continuation ring that the blocks
 take from after new work, so long requests share the GPU with short ones
 tile by tile (processor sharing) with no host step and no barrier between
 chunks.  Admission copies and result copies run on a side stream (copy
-engine) beside the kernel.  Admission keeps a few waves of tiles in flight
-and, by default, takes the waiting requests with the least work first (any
-request that has waited longer than ``max_wait`` goes ahead of them), so
-that under overload short requests do not queue behind long ones.  ``RoundServer`` is the earlier form: one
+engine) beside the kernel.  By default ("sjf") a request's continuations
+wait in one of eight device queues by its work (a class per decade), which
+blocks take lowest class first, so short requests preempt long ones chunk by
+chunk; admission takes the waiting requests with the least work first (any
+request that has waited longer than ``max_wait`` goes ahead of them) and
+stops while many waves of tiles are already in flight.  ``RoundServer`` is the earlier form: one
 ``atb_track_batch`` launch per round over every active request, new arrivals
 joining at the next round.
 
@@ -193,7 +195,7 @@ class TrackingServer:
     def __init__(self, lattices: dict, hbm_budget_bytes: float = 150e9, device: int = 0,
                  mode="exact", chunk_flops: float = 1e9, max_chunk: int = 512,
                  max_jobs: int = 1 << 16, max_tiles: int = 1 << 22, policy: str = "sjf",
-                 waves: float = 4.0, max_wait: float = 30.0, pack: bool = True):
+                 waves: float = 64.0, max_wait: float = 30.0, pack: bool = True):
         import ctypes as C
 
         import torch
@@ -262,6 +264,16 @@ class TrackingServer:
                      key=self._work)
         return old + new
 
+    def _prio(self, req) -> int:
+        """The request's continuation class under "sjf": one class per decade
+        of work above 1e10 flops (0-7; a 1e3-particle FODO request of 100
+        turns is class 0, a 2e6 x 1e4 large-ring request class 6); 0 for all
+        under "fifo"."""
+        if self.policy == "fifo":
+            return 0
+        w = max(self._work(req), 1.0)
+        return int(min(7, max(0, np.floor(np.log10(w)) - 10)))
+
     def _tiles(self, req) -> int:
         return (req.n + self.TILE - 1) // self.TILE
 
@@ -328,8 +340,8 @@ class TrackingServer:
         jd.lelem, jd.lcoord = d["lelem"].data_ptr(), d["lcoord"].data_ptr()
         slot = C.c_int32(-1)
         pidx = d["pidx"].data_ptr() if "pidx" in d else None
-        self.check(self.lib.atb_serve_submit(self.srv, C.byref(jd), self._chunk(req), pidx,
-                                             C.byref(slot)))
+        self.check(self.lib.atb_serve_submit(self.srv, C.byref(jd), self._chunk(req),
+                                             self._prio(req), pidx, C.byref(slot)))
         req._slot = slot.value
         self.jobs = slot.value + 1
 
