@@ -67,8 +67,8 @@ _SIGS = {
     "atb_element_maps": ([_vp, _i32, _vp, _vp, _vp, C.c_double, _vp], C.c_int),
     "atb_element_pass": ([_vp, _i32, _vp, _vp, _vp, _vp], C.c_int),
     "atb_serve_open": ([_vp, _vp, _i32, _i32, _i32, _i32, C.POINTER(_vp)], C.c_int),
-    "atb_serve_submit": ([_vp, C.POINTER(AtbJobDesc), _i32, _i32, _vp, C.POINTER(_i32)],
-                         C.c_int),
+    "atb_serve_submit": ([_vp, C.POINTER(AtbJobDesc), _i32, C.c_double, _vp,
+                          C.POINTER(_i32)], C.c_int),
     "atb_serve_poll": ([_vp, _i32, _i32, _vp, C.POINTER(_i32)], C.c_int),
     "atb_serve_counters": ([_vp, C.POINTER(_i32)], C.c_int),
     "atb_serve_reset": ([_vp], C.c_int),

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -1603,8 +1604,8 @@ int atb_serve_open(atb_handle* h, const int32_t* lattice_ids, int32_t nlat, int3
     return ATB_OK;
 }
 
-int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns, int32_t prio,
-                     int32_t* pidx, int32_t* slot) {
+int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns,
+                     double turn_cost, int32_t* pidx, int32_t* slot) {
     if (!s || !d || !slot) return fail(ATB_ERR_ARG, "NULL argument");
     if (chunk_turns < 0) return fail(ATB_ERR_ARG, "negative chunk");
     atb_handle* h = s->h;
@@ -1635,7 +1636,7 @@ int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns, 
     J.lelem = d->lelem;
     J.lcoord = d->lcoord;
     J.chunk = chunk_turns;
-    J.prio = std::max(0, std::min(prio, ATB_SERVE_CLASSES - 1));
+    J.turn_cost = turn_cost > 0.0 && std::isfinite(turn_cost) ? turn_cost : 0.0;
     J.pidx = pidx;
     if (ntl > s->h_tiles_cap) {
         if (s->h_tiles) cudaFreeHost(s->h_tiles);

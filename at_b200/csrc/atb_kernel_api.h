@@ -117,7 +117,10 @@ typedef struct AtbJob {
     uint64_t rng_key;           /* key of the quantum-diffusion kicks      */
     int32_t chunk;              /* serving: turns per claim, 0 all (a tile
                                    re-enqueues itself for the rest)         */
-    int32_t prio;               /* serving: continuation class, 0 first     */
+    int32_t pad_serve;
+    double turn_cost;           /* serving: relative cost of one turn; a
+                                   continuation's class is the decade of
+                                   (turns left) x turn_cost, 0: one class   */
     int32_t* pidx;              /* serving, optional: the particle at each
                                    tile position; a re-enqueued tile keeps
                                    only its live particles, packed first    */

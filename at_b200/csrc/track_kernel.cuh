@@ -1265,7 +1265,11 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                 if (more && !sv.ctl->stop) {
                     AtbTile nt = tile;
                     nt.count = keep_count;
-                    requeued = serve_requeue(sv.ring, nt, ran, J.prio);
+                    /* class: decade of the tile's remaining time, so that
+                       tiles near their end go first */
+                    const double key = (double)(s_full - ran) * J.turn_cost;
+                    const int q = key >= 1.0 ? (int)floor(log10(key)) : 0;
+                    requeued = serve_requeue(sv.ring, nt, ran, q);
                     if (!requeued) {
                         atomicOr(status, ATB_STATUS_RING_FULL);
                         keep = true;

@@ -14,12 +14,13 @@ and then puts itself back in a device-side continuation ring that the blocks
 take from after new work, so long requests share the GPU with short ones
 tile by tile (processor sharing) with no host step and no barrier between
 chunks.  Admission copies and result copies run on a side stream (copy
-engine) beside the kernel.  By default ("sjf") a request's continuations
-wait in one of eight device queues by its work (a class per decade), which
-blocks take lowest class first, so short requests preempt long ones chunk by
-chunk; admission takes the waiting requests with the least work first (any
-request that has waited longer than ``max_wait`` goes ahead of them) and
-stops while many waves of tiles are already in flight.  ``RoundServer`` is the earlier form: one
+engine) beside the kernel.  By default ("sjf") a re-enqueued tile waits in
+one of eight device queues by the decade of its remaining time (turns left x
+the cost of a turn), which blocks take lowest first: a tile needs all its
+turns whatever the request's particle count, so the tiles nearest their end
+go ahead chunk by chunk; admission takes the waiting requests with the least
+work first (any request that has waited longer than ``max_wait`` goes ahead
+of them) and stops while many waves of tiles are already in flight.  ``RoundServer`` is the earlier form: one
 ``atb_track_batch`` launch per round over every active request, new arrivals
 joining at the next round.
 
@@ -264,15 +265,19 @@ class TrackingServer:
                      key=self._work)
         return old + new
 
-    def _prio(self, req) -> int:
-        """The request's continuation class under "sjf": one class per decade
-        of work above 1e10 flops (0-7; a 1e3-particle FODO request of 100
-        turns is class 0, a 2e6 x 1e4 large-ring request class 6); 0 for all
-        under "fifo"."""
+    #: flops of one particle-turn that count as one unit of tile time
+    TURN_UNIT = 2e5
+
+    def _turn_cost(self, req) -> float:
+        """Relative cost of one turn of the request's lattice (a FODO turn is
+        about 1, a large-ring turn 10).  Under "sjf" a re-enqueued tile waits
+        in the device queue of the decade of (turns left) x this cost, so the
+        tiles closest to their end -- what bounds a request's latency, as a
+        tile needs all its turns whatever the particle count -- go first.
+        0 under "fifo": one queue, round robin."""
         if self.policy == "fifo":
-            return 0
-        w = max(self._work(req), 1.0)
-        return int(min(7, max(0, np.floor(np.log10(w)) - 10)))
+            return 0.0
+        return max(self.fpt[req.lattice] / self.TURN_UNIT, 1e-3)
 
     def _tiles(self, req) -> int:
         return (req.n + self.TILE - 1) // self.TILE
@@ -341,7 +346,7 @@ class TrackingServer:
         slot = C.c_int32(-1)
         pidx = d["pidx"].data_ptr() if "pidx" in d else None
         self.check(self.lib.atb_serve_submit(self.srv, C.byref(jd), self._chunk(req),
-                                             self._prio(req), pidx, C.byref(slot)))
+                                             self._turn_cost(req), pidx, C.byref(slot)))
         req._slot = slot.value
         self.jobs = slot.value + 1
 

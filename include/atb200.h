@@ -290,10 +290,11 @@ int atb_track_noalloc(int32_t device, const double* table, int64_t nwords,
  *                     > 0 a tile runs that many turns per claim and then goes
  *                     back to a device-side queue, so long jobs share the GPU
  *                     with later ones tile by tile (0: all turns in one
- *                     claim).  Re-enqueued tiles wait in one of 8 queues by
- *                     prio (0-7, clamped); blocks take new tiles first, then
- *                     queue 0, 1, ..., so a job of a lower class preempts
- *                     the continuations of higher ones chunk by chunk.
+ *                     claim).  Re-enqueued tiles wait in one of 8 queues, the
+ *                     decade of (turns left) x turn_cost (clamped to 0-7;
+ *                     turn_cost <= 0: queue 0 only); blocks take new tiles
+ *                     first, then queue 0, 1, ..., so tiles near their end
+ *                     go ahead of long ones chunk by chunk.
  *                     With pidx (device, np int32 holding 0, 1,
  *                     ..., np - 1; NULL: none) a re-enqueued tile keeps
  *                     only its live particles, their indices packed at the
@@ -319,8 +320,8 @@ int atb_track_noalloc(int32_t device, const double* table, int64_t nwords,
 typedef struct atb_server atb_server;
 int atb_serve_open(atb_handle* h, const int32_t* lattice_ids, int32_t nlat, int32_t mode,
                    int32_t max_jobs, int32_t max_tiles, atb_server** out);
-int atb_serve_submit(atb_server* s, const atb_job_desc* job, int32_t chunk_turns, int32_t prio,
-                     int32_t* pidx, int32_t* slot);
+int atb_serve_submit(atb_server* s, const atb_job_desc* job, int32_t chunk_turns,
+                     double turn_cost, int32_t* pidx, int32_t* slot);
 int atb_serve_poll(atb_server* s, int32_t first, int32_t nslots, uint64_t* done,
                    int32_t* running);
 int atb_serve_counters(atb_server* s, int32_t* out);
