@@ -153,3 +153,82 @@ class BatchTracker:
         for lid, _ in self._lids.values():
             self.eng.free(lid)
         self._lids = {}
+
+
+def partition_jobs(work, ndev: int) -> list[list[int]]:
+    """Split jobs of the given ``work`` (e.g. particles x turns x flops per
+    particle-turn) over ``ndev`` devices: longest processing time first, each
+    job to the device with the least work so far (Graham's LPT rule, within
+    4/3 of the optimal makespan).  Returns the job indices of each device in
+    ascending order."""
+    if ndev < 1:
+        raise ValueError("ndev must be at least 1")
+    load = [0.0] * ndev
+    parts: list[list[int]] = [[] for _ in range(ndev)]
+    for k in sorted(range(len(work)), key=lambda i: (-float(work[i]), i)):
+        d = min(range(ndev), key=lambda j: (load[j], j))
+        parts[d].append(k)
+        load[d] += float(work[k])
+    return [sorted(p) for p in parts]
+
+
+class ShardedBatchTracker:
+    """The batched workload over several GPUs of one process: the variants
+    are split by :func:`partition_jobs` (there is no exchange between them),
+    each device runs its share as one :class:`BatchTracker` launch, all
+    devices at once from a thread each, and ``results()`` returns every job's
+    result in the caller's order."""
+
+    def __init__(self, lattices, particles, nturns, devices, turn0=0, mode="exact",
+                 tune: bool = True, graph: bool = True):
+        from . import flops
+
+        self.devices = list(devices)
+        fpt = {}
+        work = []
+        for lat, p, t in zip(lattices, particles, nturns):
+            k = id(lat)
+            if k not in fpt:
+                cl = compile_lattice(lat, getattr(lat, "energy", 0.0),
+                                     getattr(getattr(lat, "particle", None), "rest_energy",
+                                             0.0))
+                fpt[k] = flops.flops_per_particle_turn(cl)[0]
+            work.append(np.asarray(p).shape[1] * int(t) * fpt[k])
+        self.parts = [p for p in partition_jobs(work, len(self.devices))]
+        self.trackers = []
+        for dev, idx in zip(self.devices, self.parts):
+            if not idx:
+                self.trackers.append(None)
+                continue
+            self.trackers.append(BatchTracker([lattices[i] for i in idx],
+                                              [particles[i] for i in idx],
+                                              [nturns[i] for i in idx], turn0=turn0, mode=mode,
+                                              device=dev, tune=tune, graph=graph))
+
+    def _each(self, fn):
+        from concurrent.futures import ThreadPoolExecutor
+        live = [t for t in self.trackers if t is not None]
+        with ThreadPoolExecutor(max_workers=max(1, len(live))) as ex:
+            return list(ex.map(fn, live))
+
+    def run(self) -> float:
+        """Every device's launch at once; returns the longest device time."""
+        return max(self._each(lambda t: t.run()), default=0.0)
+
+    def reset(self):
+        self._each(lambda t: t.reset())
+
+    def results(self):
+        out = [None] * sum(len(p) for p in self.parts)
+        for idx, t in zip(self.parts, self.trackers):
+            if t is None:
+                continue
+            for i, res in zip(idx, t.results()):
+                out[i] = res
+        return out
+
+    def close(self):
+        for t in self.trackers:
+            if t is not None:
+                t.close()
+        self.trackers = []

@@ -61,8 +61,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
         : "memory");
 }
 
-/* global -> shared bulk copy, completion signalled on the mbarrier
- * (no multicast: the source is always this GPU's own memory) */
+/* global -> shared bulk copy into this CTA's own shared memory, completion
+ * signalled on the mbarrier; the source is always this GPU's own memory */
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
                                          uint64_t* bar) {
     asm volatile(

@@ -446,6 +446,61 @@ class TrackingServer:
         self.lids = {}
 
 
+class ShardedTrackingServer:
+    """One device-resident server per GPU of the process, requests dealt out
+    as they arrive to the server with the least work outstanding (admitted
+    or waiting, N x T x flops per particle-turn).  The devices share nothing:
+    a request runs whole on one GPU, as in the reference a call runs whole
+    on one process."""
+
+    def __init__(self, lattices: dict, devices, **kw):
+        self.servers = [TrackingServer(lattices, device=d, **kw) for d in devices]
+
+    @staticmethod
+    def _outstanding(srv) -> float:
+        return sum(srv._work(r) for r in srv.waiting + srv.staging + srv.active)
+
+    def _assign(self, req):
+        srv = min(self.servers, key=lambda s: (self._outstanding(s), self.servers.index(s)))
+        srv.waiting.append(req)
+        return srv
+
+    @property
+    def done(self) -> list[Request]:
+        return [r for s in self.servers for r in s.done]
+
+    def serve(self, requests: list[Request], time_limit: float | None = None):
+        """Replay a trace over all servers; returns the wall time."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        t0 = time.perf_counter()
+        i = 0
+
+        def busy():
+            return any(s.waiting or s.staging or s.active or s.retiring for s in self.servers)
+
+        while i < len(pending) or busy():
+            now = time.perf_counter() - t0
+            while i < len(pending) and pending[i].arrival <= now:
+                self._assign(pending[i])
+                i += 1
+            moved = 0
+            for s in self.servers:
+                s._admit(now)
+                moved += s._poll()
+                s._retire(time.perf_counter() - t0)
+                s._maybe_reset()
+            if not moved:
+                time.sleep(2e-4)
+            if time_limit is not None and time.perf_counter() - t0 > time_limit:
+                break
+        return time.perf_counter() - t0
+
+    def close(self):
+        for s in self.servers:
+            s.close()
+        self.servers = []
+
+
 def serve_sequential(lattices: dict, requests: list[Request], mode="exact", device: int = 0,
                      time_limit: float | None = None):
     """The plain drop-in as a server: one blocking ``gpupass`` call per request,

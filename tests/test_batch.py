@@ -137,3 +137,55 @@ def test_refill_claims_give_the_same_results(tmp_path, monkeypatch):
     _, lr = tracking.gpupass(lats[0], ref, turns[0], losses=True, mode="fast")
     np.testing.assert_array_equal(out[8][0][0], ref)
     np.testing.assert_array_equal(out[8][0][1]["islost"], lr["islost"])
+
+
+def test_partition_jobs_longest_first_balanced():
+    """Variants split over devices (host logic): every job once, each
+    device's list ascending, and the LPT makespan within 4/3 of the bound."""
+    from at_b200.batch import partition_jobs
+    rng = np.random.default_rng(0)
+    work = rng.uniform(1.0, 100.0, 257)
+    for nd in (1, 2, 3, 8):
+        parts = partition_jobs(work, nd)
+        assert len(parts) == nd
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(257))
+        assert all(p == sorted(p) for p in parts)
+        loads = [work[p].sum() for p in parts]
+        bound = max(work.sum() / nd, work.max())
+        assert max(loads) <= 4.0 / 3.0 * bound
+    assert partition_jobs([5.0, 1.0, 1.0, 1.0, 1.0, 1.0], 2) == [[0], [1, 2, 3, 4, 5]]
+    with pytest.raises(ValueError):
+        partition_jobs([1.0], 0)
+
+
+@pytest.mark.gpu
+def test_sharded_batch_on_one_device_equals_one_batch(tmp_path, monkeypatch):
+    """The sharded tracker over a device list (here the one GPU twice:
+    two shards, two launches at once) returns, in the caller's order, the
+    results of one batched launch."""
+    monkeypatch.setenv("AT_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    from at_b200.batch import BatchTracker, ShardedBatchTracker
+
+    work = rings.batch_workload(5, turn_scale=0.004, seed=2)
+    lats = [rings.large_ring_variant(s) for s, _, _ in work]
+    parts = [rings.da_grid(max(200, n // 10), seed=s) for s, n, _ in work]
+    turns = [t for _, _, t in work]
+    one = BatchTracker(lats, parts, turns, mode="exact", tune=False, graph=False)
+    try:
+        one.run()
+        ref = one.results()
+    finally:
+        one.close()
+    sh = ShardedBatchTracker(lats, parts, turns, devices=[0, 0], mode="exact", tune=False,
+                             graph=False)
+    try:
+        assert all(p for p in sh.parts)
+        sh.run()
+        got = sh.results()
+    finally:
+        sh.close()
+    for (ra, la), (rb, lb) in zip(got, ref):
+        np.testing.assert_array_equal(ra, rb)
+        for key in ("islost", "turn", "elem", "coord"):
+            np.testing.assert_array_equal(la[key], lb[key])

@@ -143,3 +143,38 @@ def test_device_resident_server_survives_idle_gaps():
         srv.close()
     assert len(srv.done) == 3
     _check_alone(lats, reqs, "exact")
+
+
+def test_sharded_server_deals_requests_to_the_least_loaded():
+    """Host logic of the one-server-per-GPU dispatcher, on stand-in servers:
+    each arrival goes to the server with the least work outstanding."""
+    class Stub:
+        def __init__(self):
+            self.waiting, self.staging, self.active = [], [], []
+            self.fpt = {"a": 1.0}
+
+        def _work(self, r):
+            return r.n * r.nturns * self.fpt[r.lattice]
+
+    sh = serving.ShardedTrackingServer.__new__(serving.ShardedTrackingServer)
+    sh.servers = [Stub(), Stub(), Stub()]
+    mk = lambda k, n, t: serving.Request(k, "a", np.zeros((6, n)), t, 0.0)
+    got = [sh.servers.index(sh._assign(mk(k, n, t)))
+           for k, (n, t) in enumerate([(100, 10), (10, 10), (10, 10), (50, 1), (10, 1)])]
+    assert got == [0, 1, 2, 1, 2]          # loads 1000 / 150 / 110 at the end
+    assert [len(s.waiting) for s in sh.servers] == [1, 2, 2]
+
+
+@pytest.mark.gpu
+def test_sharded_server_on_one_device_equals_alone():
+    lats, orbits = rings.serving_pool(1, 1)
+    reqs = serving.make_trace(list(lats), 6, rate_hz=300.0, seed=12, n_range=(200, 2000),
+                              t_range=(10, 60), centre_of=orbits.get)
+    sh = serving.ShardedTrackingServer(lats, [0], chunk_flops=1e8)
+    try:
+        sh.serve(reqs)
+        done = sh.done
+    finally:
+        sh.close()
+    assert len(done) == len(reqs)
+    _check_alone(lats, reqs, "exact")
