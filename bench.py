@@ -64,6 +64,10 @@ def _args():
                     help="end each served trace after this many seconds")
     ap.add_argument("--serve-only", action="store_true",
                     help="only the serving comparison (one JSON object)")
+    ap.add_argument("--serve-chunk-flops", type=float, default=None,
+                    help="device-resident server: algorithmic flops per tile chunk")
+    ap.add_argument("--serve-forms", default="device,rounds,sequential",
+                    help="comma-separated serving forms to run")
     ap.add_argument("--no-diff", action="store_true", help="skip the tangent-kernel timing")
     ap.add_argument("--diff-only", action="store_true",
                     help="only the tangent-kernel timing (one JSON object)")
@@ -465,7 +469,8 @@ def run_b200(a):
     serve = None
     if world == 1 and not a.no_serve:
         serve = run_serving(a.serve_requests, mode, local, full=a.serve_full,
-                            time_limit=a.serve_time_limit)
+                            time_limit=a.serve_time_limit, chunk_flops=a.serve_chunk_flops,
+                            forms_wanted=tuple(a.serve_forms.split(",")))
     dif = None
     if world == 1 and not a.no_diff:
         dif = run_diff(local, a.diff_particles)
@@ -585,7 +590,8 @@ def run_fodo_line(device, with_cpu):
     return out
 
 
-def run_serving(nreq, mode, device, full=False, time_limit=None):
+def run_serving(nreq, mode, device, full=False, time_limit=None, chunk_flops=None,
+                forms_wanted=("device", "rounds", "sequential")):
     """A finite Poisson trace (200 requests/s) over the 16-lattice pool,
     served three ways on the same trace: the device-resident server (one
     persistent kernel fed by a queue the host appends to), the round server
@@ -603,12 +609,17 @@ def run_serving(nreq, mode, device, full=False, time_limit=None):
     out = {"requests": nreq, "rate_hz": 200.0, "lattices": len(lats),
            "sizes": "N log-uniform [%g, %g], T log-uniform [%g, %g]" % (*n_range, *t_range),
            "arithmetic": mode}
-    forms = [("continuous_batching_device_resident", serving.TrackingServer),
-             ("continuous_batching_rounds", serving.RoundServer)]
+    forms = [f for f in (("continuous_batching_device_resident", serving.TrackingServer, "device"),
+                         ("continuous_batching_rounds", serving.RoundServer, "rounds"))
+             if f[2] in forms_wanted]
     traces = {}
-    for name, cls in forms:
+    for name, cls, _ in forms:
         trace = serving.make_trace(list(lats), nreq, **kw)
-        srv = cls(lats, hbm_budget_bytes=150e9, device=device, mode=mode)
+        extra_kw = {}
+        if cls is serving.TrackingServer and chunk_flops:
+            extra_kw["chunk_flops"] = float(chunk_flops)
+            out["chunk_flops"] = float(chunk_flops)
+        srv = cls(lats, hbm_budget_bytes=150e9, device=device, mode=mode, **extra_kw)
         extra = {}
         try:
             wall = srv.serve(trace, time_limit=time_limit)
@@ -620,19 +631,20 @@ def run_serving(nreq, mode, device, full=False, time_limit=None):
         pt = sum(r.n * r.nturns for r in trace if r.finished is not None)
         out[name] = dict(st, particle_turns_per_s=pt / wall, wall_s=wall, **extra)
         traces[name] = trace
-    seq_trace = serving.make_trace(list(lats), nreq, **kw)
-    wall_seq = serving.serve_sequential(lats, seq_trace, mode=mode, device=device,
-                                        time_limit=time_limit)
-    sq = serving.latency_stats(seq_trace)
-    pt = sum(r.n * r.nturns for r in seq_trace if r.finished is not None)
-    out["plain_drop_in_sequential"] = dict(sq, particle_turns_per_s=pt / wall_seq,
-                                           wall_s=wall_seq)
-    same = True
-    for name, _ in forms:
-        for a, b in zip(traces[name], seq_trace):
-            if a.finished is not None and b.finished is not None:
-                same = same and bool(np.array_equal(a.result, b.result, equal_nan=True))
-    out["results_identical"] = same
+    if "sequential" in forms_wanted:
+        seq_trace = serving.make_trace(list(lats), nreq, **kw)
+        wall_seq = serving.serve_sequential(lats, seq_trace, mode=mode, device=device,
+                                            time_limit=time_limit)
+        sq = serving.latency_stats(seq_trace)
+        pt = sum(r.n * r.nturns for r in seq_trace if r.finished is not None)
+        out["plain_drop_in_sequential"] = dict(sq, particle_turns_per_s=pt / wall_seq,
+                                               wall_s=wall_seq)
+        same = True
+        for name, _, _ in forms:
+            for a, b in zip(traces[name], seq_trace):
+                if a.finished is not None and b.finished is not None:
+                    same = same and bool(np.array_equal(a.result, b.result, equal_nan=True))
+        out["results_identical"] = same
     return out
 
 
@@ -829,8 +841,10 @@ def main():
                                                    a.batch_sample)}), flush=True)
         return 0
     if a.serve_only:
-        print(json.dumps({"serving": run_serving(a.serve_requests, a.mode, 0, full=a.serve_full,
-                                                 time_limit=a.serve_time_limit)}), flush=True)
+        print(json.dumps({"serving": run_serving(
+            a.serve_requests, a.mode, 0, full=a.serve_full, time_limit=a.serve_time_limit,
+            chunk_flops=a.serve_chunk_flops,
+            forms_wanted=tuple(a.serve_forms.split(",")))}), flush=True)
         return 0
     return run_b200(a)
 
