@@ -14,13 +14,15 @@ and then puts itself back in a device-side continuation ring that the blocks
 take from after new work, so long requests share the GPU with short ones
 tile by tile (processor sharing) with no host step and no barrier between
 chunks.  Admission copies and result copies run on a side stream (copy
-engine) beside the kernel.  By default ("sjf") a re-enqueued tile waits in
-one of eight device queues by the decade of its remaining time (turns left x
-the cost of a turn), which blocks take lowest first: a tile needs all its
-turns whatever the request's particle count, so the tiles nearest their end
-go ahead chunk by chunk; admission takes the waiting requests with the least
-work first (any request that has waited longer than ``max_wait`` goes ahead
-of them) and stops while many waves of tiles are already in flight.  ``RoundServer`` is the earlier form: one
+engine) beside the kernel.  By default ("sjf") admission takes the waiting
+requests with the least work first (any request that has waited longer than
+``max_wait`` goes ahead of them) while the work admitted and not finished
+would take the GPU at most ``horizon_s`` seconds: a burst the GPU can absorb
+is admitted whole and shared tile by tile, and under sustained overload the
+short requests run first instead of every request sharing the GPU and few
+finishing.  With ``classes=True`` re-enqueued tiles wait in one of eight
+device queues by the decade of their remaining time instead of one (measured
+slower on the bench traces, kept as an option).  ``RoundServer`` is the earlier form: one
 ``atb_track_batch`` launch per round over every active request, new arrivals
 joining at the next round.
 
@@ -196,7 +198,8 @@ class TrackingServer:
     def __init__(self, lattices: dict, hbm_budget_bytes: float = 150e9, device: int = 0,
                  mode="exact", chunk_flops: float = 1e9, max_chunk: int = 512,
                  max_jobs: int = 1 << 16, max_tiles: int = 1 << 22, policy: str = "sjf",
-                 waves: float = 64.0, max_wait: float = 30.0, pack: bool = True):
+                 horizon_s: float = 30.0, max_wait: float = 30.0, pack: bool = True,
+                 classes: bool = False):
         import ctypes as C
 
         import torch
@@ -238,11 +241,14 @@ class TrackingServer:
             raise ValueError("policy must be 'sjf' or 'fifo'")
         self.policy = policy
         self.max_wait = float(max_wait)
-        sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
-        #: tiles in flight (admitted, not finished) above which nothing more is
-        #: admitted: a few waves of the persistent grid (two blocks per SM)
-        self.max_live_tiles = int(waves * 2 * sms)
-        self.live_tiles = 0
+        #: algorithmic flops the GPU tracks per second in this arithmetic (the
+        #: large-ring bench rates: exact 10 TFLOP/s, fast 24 TFLOP/s), and the
+        #: admission horizon: under "sjf" nothing more is admitted while the
+        #: admitted, unfinished work would take longer than horizon_s
+        self.gpu_flops = 1.0e13 if mode_code(mode) == mode_code("exact") else 2.4e13
+        self.horizon_s = float(horizon_s)
+        self.live_work = 0.0
+        self.classes = bool(classes)
         #: re-enqueued tiles keep only their live particles (a per-request
         #: particle index, filled from a pinned 0..n-1 on the copy stream)
         self.pack = bool(pack)
@@ -270,12 +276,13 @@ class TrackingServer:
 
     def _turn_cost(self, req) -> float:
         """Relative cost of one turn of the request's lattice (a FODO turn is
-        about 1, a large-ring turn 10).  Under "sjf" a re-enqueued tile waits
+        about 1, a large-ring turn 10).  With classes a re-enqueued tile waits
         in the device queue of the decade of (turns left) x this cost, so the
         tiles closest to their end -- what bounds a request's latency, as a
         tile needs all its turns whatever the particle count -- go first.
-        0 under "fifo": one queue, round robin."""
-        if self.policy == "fifo":
+        0 (one queue, round robin) unless the server was opened with
+        ``classes=True``."""
+        if not self.classes:
             return 0.0
         return max(self.fpt[req.lattice] / self.TURN_UNIT, 1e-3)
 
@@ -284,15 +291,18 @@ class TrackingServer:
 
     def _admit(self, now: float):
         """Admit waiting requests (particles copied to HBM on the side stream)
-        while the HBM budget holds and fewer than ``max_live_tiles`` tiles are
-        in flight (one request is always admitted into an idle server)."""
+        while the HBM budget holds and, under "sjf", while the admitted and
+        unfinished work stays within the horizon (one request is always
+        admitted into an idle server)."""
         torch = self.torch
         keep = []
+        limit = self.horizon_s * self.gpu_flops
         for req in self._order(now):
             need = req.n * BYTES_PER_PARTICLE
-            busy = self.live_tiles > 0
-            if self.used + need > self.budget or (
-                    busy and self.live_tiles + self._tiles(req) > self.max_live_tiles):
+            busy = self.live_work > 0
+            over = (self.policy == "sjf" and busy and
+                    self.live_work + self._work(req) > limit)
+            if self.used + need > self.budget or over:
                 keep.append(req)
                 continue
             n = req.n
@@ -316,7 +326,7 @@ class TrackingServer:
                 ev.record(self.copy)
             req.dev, req._host, req._event = d, host, ev
             self.used += need
-            self.live_tiles += self._tiles(req)
+            self.live_work += self._work(req)
             req.admitted = now
             self.staging.append(req)
         self.waiting = sorted(keep, key=lambda r: r.arrival)
@@ -375,7 +385,7 @@ class TrackingServer:
                 moved += 1
                 req.done_turns = req.nturns
                 self.particle_turns += req.n * req.nturns
-                self.live_tiles -= self._tiles(req)
+                self.live_work -= self._work(req)
                 self.active.remove(req)
                 with torch.cuda.stream(self.copy):
                     for k in req._host:

@@ -68,6 +68,8 @@ def _args():
                     help="device-resident server: algorithmic flops per tile chunk")
     ap.add_argument("--serve-forms", default="device,rounds,sequential",
                     help="comma-separated serving forms to run")
+    ap.add_argument("--serve-opts", default="{}",
+                    help="device-resident server: keyword arguments as JSON")
     ap.add_argument("--no-diff", action="store_true", help="skip the tangent-kernel timing")
     ap.add_argument("--diff-only", action="store_true",
                     help="only the tangent-kernel timing (one JSON object)")
@@ -470,7 +472,8 @@ def run_b200(a):
     if world == 1 and not a.no_serve:
         serve = run_serving(a.serve_requests, mode, local, full=a.serve_full,
                             time_limit=a.serve_time_limit, chunk_flops=a.serve_chunk_flops,
-                            forms_wanted=tuple(a.serve_forms.split(",")))
+                            forms_wanted=tuple(a.serve_forms.split(",")),
+                            opts=json.loads(a.serve_opts))
     dif = None
     if world == 1 and not a.no_diff:
         dif = run_diff(local, a.diff_particles)
@@ -591,7 +594,7 @@ def run_fodo_line(device, with_cpu):
 
 
 def run_serving(nreq, mode, device, full=False, time_limit=None, chunk_flops=None,
-                forms_wanted=("device", "rounds", "sequential")):
+                forms_wanted=("device", "rounds", "sequential"), opts=None):
     """A finite Poisson trace (200 requests/s) over the 16-lattice pool,
     served three ways on the same trace: the device-resident server (one
     persistent kernel fed by a queue the host appends to), the round server
@@ -619,6 +622,9 @@ def run_serving(nreq, mode, device, full=False, time_limit=None, chunk_flops=Non
         if cls is serving.TrackingServer and chunk_flops:
             extra_kw["chunk_flops"] = float(chunk_flops)
             out["chunk_flops"] = float(chunk_flops)
+        if cls is serving.TrackingServer and opts:
+            extra_kw.update(opts)
+            out["server_options"] = dict(opts)
         srv = cls(lats, hbm_budget_bytes=150e9, device=device, mode=mode, **extra_kw)
         extra = {}
         try:
@@ -844,7 +850,8 @@ def main():
         print(json.dumps({"serving": run_serving(
             a.serve_requests, a.mode, 0, full=a.serve_full, time_limit=a.serve_time_limit,
             chunk_flops=a.serve_chunk_flops,
-            forms_wanted=tuple(a.serve_forms.split(",")))}), flush=True)
+            forms_wanted=tuple(a.serve_forms.split(",")),
+            opts=json.loads(a.serve_opts))}), flush=True)
         return 0
     return run_b200(a)
 
