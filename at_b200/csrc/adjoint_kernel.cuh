@@ -28,7 +28,7 @@
  *    Symplectic4 passes (plain or bend-edge entrance/exit, misaligned or
  *    not): written out by hand.  In a thick magnet the
  *    (x, px, y, py) entering each integration step are recomputed from the
- *    element's entry state into a per-thread array (every step up to
+ *    element's entry state into a per-thread store in shared memory (every step up to
  *    ATB_ADJ_STEPS steps, every ceil(n / ATB_ADJ_STEPS)-th beyond, the rest
  *    recomputed from the nearest), each step is re-run with the inputs of its
  *    seven stages kept in registers, and the stages are reversed: the
@@ -49,7 +49,19 @@
 
 namespace atb {
 
-#define ATB_ADJ_STEPS 32   /* integration-step entry states kept per thread */
+/* integration-step entry states kept per thread, in shared memory */
+#define ATB_ADJ_STEPS ATB_ADJ_STEPS_SMEM
+
+/* A thread's step-entry store in the block's shared memory: entry c,
+ * component k (x, px, y, py) at base[(4 c + k) * stride], stride the block
+ * size, so a warp's accesses fall on consecutive words. */
+struct StepStore {
+    double* base;
+    int stride;
+    __device__ __forceinline__ double& at(int c, int k) const {
+        return base[(4 * c + k) * stride];
+    }
+};
 #ifndef ATB_ADJ_MIN_BLOCKS
 #define ATB_ADJ_MIN_BLOCKS 4   /* 128 registers a thread: the dual-number
                                   fallback spills, the common path does not */
@@ -347,7 +359,7 @@ __device__ __forceinline__ bool adj_by_hand(const Rec& e, bool bend) {
 template <bool BEND, int MO>
 __device__ __forceinline__ void adj_multipole_mo(const P6& s, double* lam, const Rec& e,
                                                  const Param& pm, double& g,
-                                                 double (*ss)[4]) {
+                                                 const StepStore& ss) {
     const uint32_t fl = e.flags();
     const double L1 = e.f(ATB_SM_L1), L2 = e.f(ATB_SM_L2);
     const double K1 = e.f(ATB_SM_K1), K2 = e.f(ATB_SM_K2);
@@ -380,8 +392,8 @@ __device__ __forceinline__ void adj_multipole_mo(const P6& s, double* lam, const
     XY q{r.x, r.px, r.y, r.py};
     for (int m = 0; m < ns; ++m) {
         if (m % stride == 0) {
-            double* w = ss[m / stride];
-            w[0] = q.x; w[1] = q.px; w[2] = q.y; w[3] = q.py;
+            const int c = m / stride;
+            ss.at(c, 0) = q.x; ss.at(c, 1) = q.px; ss.at(c, 2) = q.y; ss.at(c, 3) = q.py;
         }
         xy_step<BEND>(q, c, nl1, nl2, K1, K2, irho, dp);
     }
@@ -397,7 +409,7 @@ __device__ __forceinline__ void adj_multipole_mo(const P6& s, double* lam, const
     double lnl1 = 0.0, lnl2 = 0.0;
     for (int m = ns - 1; m >= 0; --m) {
         const int cb = m / stride;
-        XY t{ss[cb][0], ss[cb][1], ss[cb][2], ss[cb][3]};
+        XY t{ss.at(cb, 0), ss.at(cb, 1), ss.at(cb, 2), ss.at(cb, 3)};
         for (int j = cb * stride; j < m; ++j) xy_step<BEND>(t, c, nl1, nl2, K1, K2, irho, dp);
         /* the step once more, keeping the input of every stage */
         const double px0 = t.px, py0 = t.py;
@@ -432,7 +444,7 @@ __device__ __forceinline__ void adj_multipole_mo(const P6& s, double* lam, const
 template <bool BEND>
 __device__ __forceinline__ void adj_pass_multipole(const P6& s, double* lam, const Rec& e,
                                                    const Param& pm, double& g,
-                                                   double (*ss)[4]) {
+                                                   const StepStore& ss) {
     switch (e.mo()) {
         case 0: adj_multipole_mo<BEND, 0>(s, lam, e, pm, g, ss); break;
         case 1: adj_multipole_mo<BEND, 1>(s, lam, e, pm, g, ss); break;
@@ -529,7 +541,7 @@ __device__ __noinline__ Lam6 adj_dual7(P6 s, Lam6 in, Rec e, int nturn, Param pm
 
 /* lambda <- J_e(s)^T lambda; g += the strength's term */
 __device__ __forceinline__ void adj_element(const P6& s, double* lam, const Rec& e, int nturn,
-                                            const Param& pm, double& g, double (*ss)[4]) {
+                                            const Param& pm, double& g, const StepStore& ss) {
     switch (e.op()) {
         case ATB_OP_DRIFT: adj_pass_drift(s, lam, e); return;
         case ATB_OP_IDENTITY:
@@ -604,7 +616,9 @@ atb_adjoint_forward_kernel(const AtbAdjoint A) {
 
 extern "C" __global__ void __launch_bounds__(ATB_ADJ_THREADS, ATB_ADJ_MIN_BLOCKS)
 atb_adjoint_turn_kernel(const AtbAdjoint A) {
-    extern __shared__ double sg[];          /* the block's strength gradient */
+    /* the block's strength gradient (nparam words), then the threads' step
+       stores (ATB_ADJ_STEPS x 4 x blockDim words) */
+    extern __shared__ double sg[];
     for (int q = threadIdx.x; q < A.nparam; q += blockDim.x) sg[q] = 0.0;
     __syncthreads();
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -629,7 +643,7 @@ atb_adjoint_turn_kernel(const AtbAdjoint A) {
             if (is_bad(s)) live = false;      /* lost in this turn */
         }
     }
-    double ss[ATB_ADJ_STEPS][4];
+    const StepStore ss{sg + A.nparam + threadIdx.x, (int)blockDim.x};
     for (int ei = A.nelem - 1; ei >= 0; --ei) {
         const Param pm = adj_param(A, ei);
         double g = 0.0;

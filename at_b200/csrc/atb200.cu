@@ -1106,8 +1106,9 @@ int atb_adjoint_backward(atb_handle* h, int32_t id, const double* ckpt, int64_t 
     if (np > 0 && nturns > 0 && (!ckpt || !lam)) return fail(ATB_ERR_ARG, "ckpt or lam is NULL");
     if (nparam > 0 && (!param_elem || !param_order || !param_value || !gparam))
         return fail(ATB_ERR_ARG, "parameter arrays missing");
-    if ((size_t)nparam * sizeof(double) > 48 * 1024)
-        return fail(ATB_ERR_ARG, "at most 6144 strengths");
+    if (((size_t)nparam + (size_t)ATB_ADJ_STEPS_SMEM * 4 * ATB_ADJ_THREADS) * sizeof(double) >
+        48 * 1024)
+        return fail(ATB_ERR_ARG, "at most 1024 strengths");
     if (np > (int64_t)ATB_ADJ_THREADS * 0x7fffffffLL) return fail(ATB_ERR_ARG, "too many particles");
     const int rc = strength_map(h, L, param_elem, param_order, nparam, "adjoint");
     if (rc != ATB_OK) return rc;
@@ -1128,7 +1129,8 @@ int atb_adjoint_backward(atb_handle* h, int32_t id, const double* ckpt, int64_t 
          h->adj_state.ensure((size_t)chunk * 6 * sizeof(double)) != cudaSuccess))
         return fail(ATB_ERR_NOMEM, "cudaMalloc(adjoint checkpoints) failed");
     const int nck = (nturns + stride - 1) / stride;
-    const size_t smem = (size_t)nparam * sizeof(double);
+    const size_t smem =
+        ((size_t)nparam + (size_t)ATB_ADJ_STEPS_SMEM * 4 * ATB_ADJ_THREADS) * sizeof(double);
     A.gparam = gparam;
     A.scratch = h->adj_scratch.as<double>();
     for (int64_t p0 = 0; p0 < np; p0 += chunk) {

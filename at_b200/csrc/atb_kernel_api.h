@@ -173,6 +173,7 @@ typedef struct AtbTangent {
  * the turn's exit to its entry and adds the strengths' gradient to
  * `gparam`. */
 #define ATB_ADJ_THREADS 128
+#define ATB_ADJ_STEPS_SMEM 10      /* step entries a thread keeps in shared memory */
 
 typedef struct AtbAdjoint {
     const double* table;        /* element table words                      */

@@ -14,13 +14,14 @@ and then puts itself back in a device-side continuation ring that the blocks
 take from after new work, so long requests share the GPU with short ones
 tile by tile (processor sharing) with no host step and no barrier between
 chunks.  Admission copies and result copies run on a side stream (copy
-engine) beside the kernel.  By default ("sjf") admission takes the waiting
+engine) beside the kernel.  By default ("sjf") requests are admitted in
+arrival order while the admitted and waiting work would take the GPU at
+most ``horizon_s`` seconds, so a burst the GPU can absorb is admitted whole
+and shared tile by tile; beyond that (overload) admission takes the waiting
 requests with the least work first (any request that has waited longer than
-``max_wait`` goes ahead of them) while the work admitted and not finished
-would take the GPU at most ``horizon_s`` seconds: a burst the GPU can absorb
-is admitted whole and shared tile by tile, and under sustained overload the
-short requests run first instead of every request sharing the GPU and few
-finishing.  With ``classes=True`` re-enqueued tiles wait in one of eight
+``max_wait`` goes ahead of them) and only while the admitted, unfinished
+work stays within the horizon, so the short requests run first instead of
+every request sharing the GPU and few finishing.  With ``classes=True`` re-enqueued tiles wait in one of eight
 device queues by the decade of their remaining time instead of one (measured
 slower on the bench traces, kept as an option).  ``RoundServer`` is the earlier form: one
 ``atb_track_batch`` launch per round over every active request, new arrivals
@@ -258,13 +259,20 @@ class TrackingServer:
     def _work(self, req) -> float:
         return req.n * req.nturns * self.fpt[req.lattice]
 
+    def _overloaded(self) -> bool:
+        """The admitted, unfinished work plus the waiting work would take the
+        GPU longer than the horizon."""
+        total = self.live_work + sum(self._work(r) for r in self.waiting)
+        return total > self.horizon_s * self.gpu_flops
+
     def _order(self, now: float) -> list:
-        """Admission order.  "fifo": arrival order.  "sjf": requests that have
+        """Admission order.  "fifo", and "sjf" while the GPU is not
+        overloaded: arrival order.  "sjf" under overload: requests that have
         waited longer than ``max_wait`` first (in arrival order), then the
         others by increasing work (N x T x flops per particle-turn), which
         keeps short requests from queueing behind long ones when the offered
         load exceeds the GPU."""
-        if self.policy == "fifo":
+        if self.policy == "fifo" or not self._overloaded():
             return list(self.waiting)
         old = [r for r in self.waiting if now - r.arrival > self.max_wait]
         new = sorted((r for r in self.waiting if now - r.arrival <= self.max_wait),

@@ -36,12 +36,15 @@ def test_admission_order_shortest_work_first_with_aging():
     srv = serving.TrackingServer.__new__(serving.TrackingServer)
     srv.fpt = {"a": 1.0, "b": 10.0}
     srv.policy, srv.max_wait = "sjf", 5.0
+    srv.live_work, srv.horizon_s, srv.gpu_flops = 0.0, 1.0, 1.0    # overloaded
     mk = lambda k, lat, n, t, arr: serving.Request(k, lat, np.zeros((6, n)), t, arr)
     srv.waiting = [mk(0, "a", 100, 100, 0.0), mk(1, "b", 10, 10, 1.0), mk(2, "a", 5, 5, 2.0),
                    mk(3, "b", 1000, 1000, 9.0), mk(4, "a", 1, 1, 9.5)]
     assert [r.rid for r in srv._order(now=10.0)] == [0, 1, 2, 4, 3]
     assert [r.rid for r in srv._order(now=6.5)] == [0, 1, 4, 2, 3]
     srv.policy = "fifo"
+    assert [r.rid for r in srv._order(now=10.0)] == [0, 1, 2, 3, 4]
+    srv.policy, srv.horizon_s = "sjf", 1e8                         # within the horizon
     assert [r.rid for r in srv._order(now=10.0)] == [0, 1, 2, 3, 4]
 
 
