@@ -19,9 +19,9 @@ arrival order while the admitted and waiting work would take the GPU at
 most ``horizon_s`` seconds, so a burst the GPU can absorb is admitted whole
 and shared tile by tile; beyond that (overload) admission takes the waiting
 requests with the least work first (any request that has waited longer than
-``max_wait`` goes ahead of them) and only while the admitted, unfinished
-work stays within the horizon, so the short requests run first instead of
-every request sharing the GPU and few finishing.  With ``classes=True`` re-enqueued tiles wait in one of eight
+``max_wait`` goes ahead of them) and only while fewer than ``waves`` waves of
+the persistent grid's tiles are in flight, so the short requests run first
+and finish instead of every request sharing the GPU and few finishing.  With ``classes=True`` re-enqueued tiles wait in one of eight
 device queues by the decade of their remaining time instead of one (measured
 slower on the bench traces, kept as an option).  ``RoundServer`` is the earlier form: one
 ``atb_track_batch`` launch per round over every active request, new arrivals
@@ -200,7 +200,7 @@ class TrackingServer:
                  mode="exact", chunk_flops: float = 1e9, max_chunk: int = 512,
                  max_jobs: int = 1 << 16, max_tiles: int = 1 << 22, policy: str = "sjf",
                  horizon_s: float = 30.0, max_wait: float = 30.0, pack: bool = True,
-                 classes: bool = False):
+                 classes: bool = False, waves: float = 4.0):
         import ctypes as C
 
         import torch
@@ -249,6 +249,12 @@ class TrackingServer:
         self.gpu_flops = 1.0e13 if mode_code(mode) == mode_code("exact") else 2.4e13
         self.horizon_s = float(horizon_s)
         self.live_work = 0.0
+        sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
+        #: under overload, tiles in flight (admitted, not finished) above which
+        #: nothing more is admitted: a few waves of the persistent grid (two
+        #: blocks per SM)
+        self.max_live_tiles = int(waves * 2 * sms)
+        self.live_tiles = 0
         self.classes = bool(classes)
         #: re-enqueued tiles keep only their live particles (a per-request
         #: particle index, filled from a pinned 0..n-1 on the copy stream)
@@ -299,17 +305,16 @@ class TrackingServer:
 
     def _admit(self, now: float):
         """Admit waiting requests (particles copied to HBM on the side stream)
-        while the HBM budget holds and, under "sjf", while the admitted and
-        unfinished work stays within the horizon (one request is always
-        admitted into an idle server)."""
+        while the HBM budget holds and, under "sjf" when overloaded, while
+        fewer than ``max_live_tiles`` tiles are in flight (one request is
+        always admitted into an idle server)."""
         torch = self.torch
         keep = []
-        limit = self.horizon_s * self.gpu_flops
+        capped = self.policy == "sjf" and self._overloaded()
         for req in self._order(now):
             need = req.n * BYTES_PER_PARTICLE
-            busy = self.live_work > 0
-            over = (self.policy == "sjf" and busy and
-                    self.live_work + self._work(req) > limit)
+            busy = self.live_tiles > 0
+            over = capped and busy and self.live_tiles + self._tiles(req) > self.max_live_tiles
             if self.used + need > self.budget or over:
                 keep.append(req)
                 continue
@@ -335,6 +340,7 @@ class TrackingServer:
             req.dev, req._host, req._event = d, host, ev
             self.used += need
             self.live_work += self._work(req)
+            self.live_tiles += self._tiles(req)
             req.admitted = now
             self.staging.append(req)
         self.waiting = sorted(keep, key=lambda r: r.arrival)
@@ -394,6 +400,7 @@ class TrackingServer:
                 req.done_turns = req.nturns
                 self.particle_turns += req.n * req.nturns
                 self.live_work -= self._work(req)
+                self.live_tiles -= self._tiles(req)
                 self.active.remove(req)
                 with torch.cuda.stream(self.copy):
                     for k in req._host:
