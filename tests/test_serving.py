@@ -181,3 +181,21 @@ def test_sharded_server_on_one_device_equals_alone():
         sh.close()
     assert len(done) == len(reqs)
     _check_alone(lats, reqs, "exact")
+
+
+@pytest.mark.gpu
+def test_device_resident_queue_classes_equal_alone():
+    """With continuations queued by remaining time (eight device rings, taken
+    lowest first) every result still equals the request tracked alone."""
+    lats, orbits = rings.serving_pool(1, 1)
+    reqs = serving.make_trace(list(lats), 8, rate_hz=400.0, seed=13, n_range=(200, 3000),
+                              t_range=(10, 120), centre_of=orbits.get)
+    srv = serving.TrackingServer(lats, chunk_flops=1e8, classes=True)
+    try:
+        srv.serve(reqs)
+        c = srv.counters()
+    finally:
+        srv.close()
+    assert len(srv.done) == len(reqs)
+    assert c["resumed"] == c["requeued"] > c["published"]
+    _check_alone(lats, reqs, "exact")
