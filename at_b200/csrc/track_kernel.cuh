@@ -697,15 +697,24 @@ __device__ __forceinline__ int seg_at(const AtbJob& J, long long q) {
  * taken once its `seq` shows it written).  Without work the block sleeps between looks;
  * it leaves when the host sets `stop`, or after ATB_SERVE_IDLE_NS with
  * nothing claimed anywhere (no tile in flight that could still re-enqueue),
- * or after a hundred times that while tiles are in flight.  Returns 1 with
+ * or after a hundred times that while tiles are in flight, and in any case
+ * after two hundred times that in one claim.  Returns 1 with
  * the tile and the turns of its job already run, or 0 to leave. */
 __device__ __forceinline__ int serve_claim(const AtbServeCtl* ctl, int* counter,
                                            const AtbTile* tiles, const AtbServeRing& ring,
                                            int* inflight, int* status, AtbTile* tile,
                                            int* turn_off) {
     uint64_t t0 = global_ns();
+    const uint64_t entry = t0;
     while (true) {
         if (ctl->stop) return 0;
+        /* a hard bound on the whole claim, whatever resets the idle clock:
+           the block leaves and the host launches the kernel again while
+           published or re-enqueued work waits */
+        if (global_ns() - entry > 200ULL * ATB_SERVE_IDLE_NS) {
+            atomicOr(status, ATB_STATUS_IDLE);
+            return 0;
+        }
         const int pub = ctl->published;
         const int c = atomicAdd(counter, 0);
         if (c < pub) {
