@@ -209,3 +209,27 @@ def test_adjoint_validates_strengths():
                                    None, ck.data_ptr(), 0)
     finally:
         at.close()
+
+
+@pytest.mark.gpu
+def test_empty_set_and_zero_turns():
+    """No particles: empty results and a zero strength gradient.  Zero turns:
+    the final coordinates are the initial ones and the backward pass is the
+    identity (dL/d r0 = g, dL/dK = 0)."""
+    ring = rings.fodo_ring()
+    params = diff.multipole_strengths(ring)
+    at = diff.AdjointTracker(ring, params)
+    try:
+        e = torch.zeros((0, 6), dtype=torch.float64, device="cuda:0")
+        r, lost, st = at.forward(e, None, 5)
+        gx, gk = at.backward(st, e)
+        assert r.shape == (0, 6) and lost.shape == (0,) and gx.shape == (0, 6)
+        assert torch.equal(gk, torch.zeros_like(gk))
+        x0 = _rows(rings.gaussian(300, [1e-4, 1e-5, 1e-4, 1e-5, 1e-4, 1e-4], seed=8))
+        g = torch.randn_like(x0)
+        r, lost, st = at.forward(x0, None, 0)
+        gx, gk = at.backward(st, g)
+        assert torch.equal(r, x0) and not lost.any()
+        assert torch.equal(gx, g) and torch.equal(gk, torch.zeros_like(gk))
+    finally:
+        at.close()
