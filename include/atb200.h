@@ -307,9 +307,9 @@ int atb_track_noalloc(int32_t device, const double* table, int64_t nwords,
  *                     finished when its count equals its particle count; its
  *                     buffers may then be read), and
  *                     whether the kernel is running.  The kernel leaves after
- *                     ATB_SERVE_IDLE (0.2 s) without new work; poll and submit
- *                     launch it again while published or re-enqueued work
- *                     waits.
+ *                     ATB_SERVE_IDLE (0.2 s) without new work (a block also
+ *                     after 40 s in one claim); poll and submit launch it
+ *                     again while published or re-enqueued work waits.
  *   atb_serve_counters  tiles published and claimed from the host queue, and
  *                     continuations written to and taken from the device
  *                     queue since the last reset (out[4]).
