@@ -235,9 +235,7 @@ class TrackingServer:
         self.done: list[Request] = []
         self.used = 0.0
         self.jobs = 0                         # queue slots used
-        self.first_live = 0                   # lowest slot still polled
         self.particle_turns = 0
-        self.launches_seen = 0
         if policy not in ("sjf", "fifo"):
             raise ValueError("policy must be 'sjf' or 'fifo'")
         self.policy = policy
