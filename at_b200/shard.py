@@ -95,6 +95,23 @@ def gather_results(r: np.ndarray, rout: np.ndarray | None = None, losses: dict |
     return full_r, full_rout, full_ld
 
 
+def reduce_stats(alive: np.ndarray, moments: np.ndarray, group=None):
+    """The per-turn statistics of a sharded call (``gpupass(stats=True)``)
+    summed over ranks in ONE all-reduce: survivor counts (T,) and the twelve
+    coordinate sums and sums of squares per turn (T, 12), from which the
+    bunch's mean and rms follow.  Counts travel as float64 (exact below
+    2**53).  Returns (alive (T,) int64, moments (T, 12) float64)."""
+    import torch
+    import torch.distributed as dist
+
+    a = np.asarray(alive, dtype=np.float64).reshape(-1)
+    m = np.asarray(moments, dtype=np.float64).reshape(a.size, 12)
+    buf = torch.from_numpy(np.concatenate([a[:, None], m], axis=1)).to(_device(group))
+    dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+    out = buf.cpu().numpy()
+    return out[:, 0].astype(np.int64), np.ascontiguousarray(out[:, 1:])
+
+
 def max_over_ranks(seconds: float, group=None) -> float:
     """Step time of a multi-GPU run: the slowest rank's."""
     import torch

@@ -51,11 +51,23 @@ def _worker(rank, world, port, results):
                                 rest_energy=ring.particle.rest_energy, losses=True, nthreads=1)
         full, full_rout, full_ld = shard.gather_results(mine, rout, ld)
         t = shard.max_over_ranks(float(rank + 1))
+        alive, moments = shard.reduce_stats(*_stats(mine, ld))
         if rank == 0:
             results.put((np.ascontiguousarray(full), np.ascontiguousarray(full_rout),
-                         {k: np.ascontiguousarray(v) for k, v in full_ld.items()}, float(t)))
+                         {k: np.ascontiguousarray(v) for k, v in full_ld.items()}, float(t),
+                         alive, moments))
     finally:
         dist.destroy_process_group()
+
+
+def _stats(r, ld):
+    """Per-turn statistics of a tracked set, as gpupass(stats=True) gives
+    them: survivors after each turn (from the loss map) and, per turn, the
+    sums and sums of squares of the survivors' final coordinates."""
+    alive = np.array([np.sum(~ld["islost"] | (ld["turn"] > t)) for t in range(NT)])
+    ok = ~ld["islost"]
+    row = np.concatenate([r[:, ok].sum(axis=1), (r[:, ok] ** 2).sum(axis=1)])
+    return alive, np.tile(row, (NT, 1))
 
 
 def _single():
@@ -83,7 +95,7 @@ def test_two_rank_gloo_shards_equal_single_process():
     procs = [ctx.Process(target=_worker, args=(r, 2, port, results)) for r in range(2)]
     for p in procs:
         p.start()
-    full, full_rout, full_ld, t = results.get(timeout=300)        # rank 0's gathered results
+    full, full_rout, full_ld, t, alive, moments = results.get(timeout=300)   # rank 0's
     for p in procs:
         p.join(timeout=300)
         assert p.exitcode == 0
@@ -96,6 +108,9 @@ def test_two_rank_gloo_shards_equal_single_process():
         np.testing.assert_array_equal(full_ld[k], ld[k], err_msg=k)
     assert t == 2.0
     assert ld["islost"].any() and not ld["islost"].all()     # lost and surviving shards
+    a1, m1 = _stats(ref, ld)                                  # statistics summed over ranks
+    np.testing.assert_array_equal(alive, a1)
+    np.testing.assert_allclose(moments, m1, rtol=1e-13, atol=0)
 
 
 class _OracleEngine:
