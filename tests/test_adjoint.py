@@ -7,9 +7,11 @@ dL/dK_q = sum_n G_q[n] . g[n].  Both are exact derivatives of the same
 arithmetic, accumulated in a different order, so they agree to rounding:
 relative 1e-10 of each array's scale on the FODO ring (hand-written element
 adjoints), on the reference's hmba lattice (quadrupole fringes: the
-dual-number element path) and on the radiating large ring.  The forward
-pass's values equal the exact tracking engine's bit for bit, and the
-gradients do not depend on the checkpoint stride.
+dual-number element path) and on the radiating large ring.  They are also
+checked directly against differences taken in binary128 (1e-7 of the sum of
+the terms' magnitudes).  The forward pass's values equal the exact tracking
+engine's bit for bit, and the gradients do not depend on the checkpoint
+stride.
 """
 import json
 import os
@@ -233,3 +235,35 @@ def test_empty_set_and_zero_turns():
         assert torch.equal(gx, g) and torch.equal(gk, torch.zeros_like(gk))
     finally:
         at.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,nturns", [("fodo1", 1), ("fodo100", 100)])
+def test_adjoint_vs_quad_differences(case, nturns):
+    """The adjoint's gradients of L = sum_n g_n . r_n(T) against the same
+    contractions of differences taken in binary128 (golden diff_fd.npz:
+    five-point, h = 1e-8 for coordinates and 1e-5 for strengths): each within
+    1e-7 of the sum of the magnitudes of its terms."""
+    fdq = dict(np.load(os.path.join(GOLDEN, "diff_fd.npz")))
+    ring = rings.fodo_ring()
+    params = diff.multipole_strengths(ring)
+    sel = fdq["fodo100_params"] if case == "fodo100" else np.arange(128)
+    x = fdq[case + "_x"]
+    n = x.shape[1]
+    g = np.random.default_rng(3).standard_normal((n, 6))
+    at = diff.AdjointTracker(ring, params)
+    try:
+        r, lost, st = at.forward(_rows(x), None, nturns)
+        assert not bool(lost.any())
+        gx, gk = at.backward(st, torch.tensor(g, device="cuda:0"))
+        gx, gk = gx.cpu().numpy(), gk.cpu().numpy()[sel]
+    finally:
+        at.close()
+    jac4 = fdq[case + "_jac4"]                               # (n, 6, 6)
+    grad4 = fdq[case + "_grad4"]                             # (P_sel, 6, n)
+    want_x = np.einsum("ni,nij->nj", g, jac4)
+    scale_x = np.einsum("ni,nij->nj", np.abs(g), np.abs(jac4))
+    assert np.all(np.abs(gx - want_x) <= 1e-7 * scale_x + 1e-300)
+    want_k = np.einsum("ni,pin->p", g, grad4)
+    scale_k = np.einsum("ni,pin->p", np.abs(g), np.abs(grad4))
+    assert np.all(np.abs(gk - want_k) <= 1e-7 * scale_k)
