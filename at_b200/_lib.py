@@ -76,9 +76,9 @@ _SIGS = {
     "atb_tangent_device": ([_vp, _i32, _vp, _i64, _i32, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _vp,
                             _vp], C.c_int),
     "atb_adjoint_forward": ([_vp, _i32, _vp, _i64, _i32, _i32, _vp, _vp, _vp, _i32, _vp, _i32,
-                             _vp, _vp], C.c_int),
-    "atb_adjoint_backward": ([_vp, _i32, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _vp, _i32, _vp,
-                              _vp, _vp], C.c_int),
+                             _vp, _vp, _vp], C.c_int),
+    "atb_adjoint_backward": ([_vp, _i32, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp,
+                              _i32, _vp, _vp, _vp], C.c_int),
     "atb_sync": ([_vp, _vp], C.c_int),
     "atb_set_rng": ([_vp, C.c_uint64], C.c_int),
     "atb_batch_prepare": ([_vp, C.POINTER(AtbJobDesc), _i32, _i32, C.POINTER(_i32)], C.c_int),

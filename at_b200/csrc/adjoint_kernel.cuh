@@ -15,7 +15,9 @@
  *
  * Backward (atb_adjoint_turn_kernel, one launch per turn, last turn first):
  * from the turn's entry state the turn is tracked again, every element's
- * entry state going to a scratch array ([element][particle][6], coalesced);
+ * entry state going to a scratch array ([element][particle][6], coalesced)
+ * -- or, when the forward pass stored every turn's element-entry states
+ * (memory permitting), those are read instead;
  * then the elements are walked backwards with lambda <- J_e^T lambda, J_e
  * the element's Jacobian at its stored entry state, and at an element that
  * carries K_q, dL/dK_q += (d r_out / d K_q) . lambda_out, summed over the
@@ -600,6 +602,8 @@ atb_adjoint_forward_kernel(const AtbAdjoint A) {
         if (lost || (A.skip_last && tt == A.nturns - 1)) continue;
         const int nturn = A.turn0 + tt;
         for (int ei = 0; ei < A.nelem; ++ei) {
+            if (A.scratch)
+                store6(A.scratch + 6 * (((long long)tt * A.nelem + ei) * A.ld + p), r);
             track_element(r, adj_rec(A, ei), nturn, adj_param(A, ei));
             if (is_bad(r)) {                  /* pyat/at.c:115-139 */
                 lost = true;
@@ -635,12 +639,18 @@ atb_adjoint_turn_kernel(const AtbAdjoint A) {
 #pragma unroll
         for (int i = 0; i < 6; ++i) live &= isfinite(lam[i]);
     }
-    /* the turn once more, every element's entry state to the scratch array */
-    for (int ei = 0; ei < A.nelem; ++ei) {
-        if (live) {
-            store6(A.scratch + 6 * ((long long)ei * np + p), s);
-            track_element(s, adj_rec(A, ei), A.turn0, adj_param(A, ei));
-            if (is_bad(s)) live = false;      /* lost in this turn */
+    if (A.next) {
+        /* the forward pass stored this turn's element-entry states; a
+           particle lost during the turn enters the next one as NaN */
+        if (live) live = !isnan(__ldg(A.next + 6 * p));
+    } else {
+        /* the turn once more, every element's entry state to the scratch */
+        for (int ei = 0; ei < A.nelem; ++ei) {
+            if (live) {
+                store6(A.scratch + 6 * ((long long)ei * np + p), s);
+                track_element(s, adj_rec(A, ei), A.turn0, adj_param(A, ei));
+                if (is_bad(s)) live = false;      /* lost in this turn */
+            }
         }
     }
     const StepStore ss{sg + A.nparam + threadIdx.x, (int)blockDim.x};

@@ -1062,7 +1062,7 @@ unsigned adjoint_blocks(int64_t n) {
 int atb_adjoint_forward(atb_handle* h, int32_t id, double* r, int64_t np, int32_t nturns,
                         int32_t turn0, const int32_t* param_elem, const int32_t* param_order,
                         const double* param_value, int32_t nparam, double* ckpt,
-                        int32_t stride, uint8_t* islost, void* stream) {
+                        int32_t stride, double* estates, uint8_t* islost, void* stream) {
     if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
     Lattice* L = get_lat(h, id);
     if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
@@ -1072,6 +1072,8 @@ int atb_adjoint_forward(atb_handle* h, int32_t id, double* r, int64_t np, int32_
     if (nparam > 0 && (!param_elem || !param_order || !param_value))
         return fail(ATB_ERR_ARG, "parameter arrays missing");
     if (np > (int64_t)ATB_ADJ_THREADS * 0x7fffffffLL) return fail(ATB_ERR_ARG, "too many particles");
+    if (estates && (stride != 1 || !ckpt))
+        return fail(ATB_ERR_ARG, "element states need a checkpoint every turn");
     const int rc = strength_map(h, L, param_elem, param_order, nparam, "adjoint");
     if (rc != ATB_OK) return rc;
     if (np == 0) return ATB_OK;
@@ -1088,16 +1090,17 @@ int atb_adjoint_forward(atb_handle* h, int32_t id, double* r, int64_t np, int32_
     A.r = r;
     A.ckpt = ckpt;
     A.lost = islost;
+    A.scratch = estates;
     atb_adjoint_forward_kernel<<<adjoint_blocks(np), ATB_ADJ_THREADS, 0, st>>>(A);
     ATB_CUDA(cudaGetLastError());
     return ATB_OK;
 }
 
 int atb_adjoint_backward(atb_handle* h, int32_t id, const double* ckpt, int64_t np,
-                         int32_t nturns, int32_t turn0, int32_t stride,
-                         const int32_t* param_elem, const int32_t* param_order,
-                         const double* param_value, int32_t nparam, double* lam,
-                         double* gparam, void* stream) {
+                         int32_t nturns, int32_t turn0, int32_t stride, const double* estates,
+                         const double* rfinal, const int32_t* param_elem,
+                         const int32_t* param_order, const double* param_value, int32_t nparam,
+                         double* lam, double* gparam, void* stream) {
     if (!h) return fail(ATB_ERR_ARG, "handle is NULL");
     Lattice* L = get_lat(h, id);
     if (!L) return fail(ATB_ERR_NOLAT, "unknown lattice id");
@@ -1106,6 +1109,9 @@ int atb_adjoint_backward(atb_handle* h, int32_t id, const double* ckpt, int64_t 
     if (np > 0 && nturns > 0 && (!ckpt || !lam)) return fail(ATB_ERR_ARG, "ckpt or lam is NULL");
     if (nparam > 0 && (!param_elem || !param_order || !param_value || !gparam))
         return fail(ATB_ERR_ARG, "parameter arrays missing");
+    if (estates && (stride != 1 || !rfinal))
+        return fail(ATB_ERR_ARG, "element states need a checkpoint every turn and the final "
+                                 "states");
     if (((size_t)nparam + (size_t)ATB_ADJ_STEPS_SMEM * 4 * ATB_ADJ_THREADS) * sizeof(double) >
         48 * 1024)
         return fail(ATB_ERR_ARG, "at most 1024 strengths");
@@ -1119,6 +1125,25 @@ int atb_adjoint_backward(atb_handle* h, int32_t id, const double* ckpt, int64_t 
     AtbAdjoint A;
     const int rs = adjoint_setup(h, L, param_order, param_value, nparam, st, A);
     if (rs != ATB_OK) return rs;
+    const size_t smem_e =
+        ((size_t)nparam + (size_t)ATB_ADJ_STEPS_SMEM * 4 * ATB_ADJ_THREADS) * sizeof(double);
+    if (estates) {
+        /* every turn's element-entry states were stored by the forward pass:
+           no tracking here, all particles in one launch per turn */
+        A.gparam = gparam;
+        for (int t = nturns - 1; t >= 0; --t) {
+            AtbAdjoint T = A;
+            T.np = np;
+            T.ckpt = const_cast<double*>(ckpt + 6 * ((int64_t)t * np));
+            T.lam = lam;
+            T.turn0 = turn0 + t;
+            T.scratch = const_cast<double*>(estates) + 6 * ((int64_t)t * L->nelem * np);
+            T.next = (t + 1 < nturns) ? ckpt + 6 * ((int64_t)(t + 1) * np) : rfinal;
+            atb_adjoint_turn_kernel<<<adjoint_blocks(np), ATB_ADJ_THREADS, smem_e, st>>>(T);
+        }
+        ATB_CUDA(cudaGetLastError());
+        return ATB_OK;
+    }
     /* particles in chunks whose element-entry scratch fits 8 GiB */
     const int64_t per = (int64_t)std::max(L->nelem, 1) * 6 * sizeof(double);
     const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(np, (8LL << 30) / per));
@@ -1163,6 +1188,7 @@ int atb_adjoint_backward(atb_handle* h, int32_t id, const double* ckpt, int64_t 
             F.turn0 = turn0 + t0;
             F.stride = 1;
             F.skip_last = 1;
+            F.scratch = nullptr;       /* no element states from this re-tracking */
             atb_adjoint_forward_kernel<<<adjoint_blocks(n), ATB_ADJ_THREADS, 0, st>>>(F);
             for (int t = nt - 1; t >= 0; --t) {
                 AtbAdjoint T = A;

@@ -194,8 +194,15 @@ typedef struct AtbAdjoint {
     double* ckpt;               /* forward: out; turn kernel: entry states  */
     uint8_t* lost;              /* forward: optional loss flags (np)        */
     double* lam;                /* turn kernel: (np, 6) cotangent           */
-    double* scratch;            /* turn kernel: (nelem, np, 6)              */
+    double* scratch;            /* turn kernel: (nelem, np, 6) element-entry
+                                   states; forward, optional: every turn's
+                                   ((nturns, nelem, ld, 6)), stored as the
+                                   particles pass                          */
     double* gparam;             /* turn kernel: (nparam), added to          */
+    const double* next;         /* turn kernel, states stored by the forward
+                                   pass: the (np, 6) states entering the next
+                                   turn (NaN: lost in this one); NULL: the
+                                   kernel tracks the turn again itself      */
 } AtbAdjoint;
 
 /* Per-element transfer and diffusion matrices for a particle entering each

@@ -175,11 +175,14 @@ class AdjointTracker(TangentTracker):
             s *= 2
         return s
 
-    def forward(self, r0, strengths=None, nturns: int = 1, turn0: int = 0, stride=None):
+    def forward(self, r0, strengths=None, nturns: int = 1, turn0: int = 0, stride=None,
+                store_elements: bool = False):
         """Track ``r0`` ((N, 6) float64 tensor on this device, not modified)
         with ``strengths`` ((P,) tensor, default: the lattice's own).
         Returns ``(r, lost, state)``: final coordinates (N, 6), loss flags
-        (N,) and what :meth:`backward` needs."""
+        (N,) and what :meth:`backward` needs.  ``store_elements`` keeps every
+        element's entry state of every turn (N x elements x turns x 48 bytes)
+        so that the backward sweep need not track the turns again."""
         torch = self.torch
         if r0.dtype != torch.float64 or r0.dim() != 2 or r0.shape[1] != 6:
             raise ValueError("r0 must be an (N, 6) float64 tensor")
@@ -191,20 +194,29 @@ class AdjointTracker(TangentTracker):
                              (self.nparam, self.dev))
         k = k.detach().contiguous().clone()
         n, nturns = int(r0.shape[0]), int(nturns)
+        if store_elements:
+            stride = 1
         stride = self._stride(n, nturns) if stride is None else int(stride)
         nck = max(1, (nturns + stride - 1) // stride)
         r = r0.detach().contiguous().clone()
         ckpt = torch.empty((nck, n, 6), dtype=torch.float64, device=self.dev)
         lost = torch.empty((n,), dtype=torch.uint8, device=self.dev)
+        estates = None
+        if store_elements and n and nturns:
+            estates = torch.empty((nturns, self.cl.nelem, n, 6), dtype=torch.float64,
+                                  device=self.dev)
         cur = torch.cuda.current_stream(self.dev)
         self.stream.wait_stream(cur)
         self.eng.adjoint_forward(self.lid, r.data_ptr(), n, nturns, int(turn0), self.pelem,
                                  self.porder, k.data_ptr() if self.nparam else None,
                                  ckpt.data_ptr(), stride, lost.data_ptr(),
-                                 self.stream.cuda_stream)
+                                 self.stream.cuda_stream,
+                                 estates.data_ptr() if estates is not None else None)
         cur.wait_stream(self.stream)
+        # the final states, kept apart from the r handed back to the caller
+        rfinal = r.clone() if estates is not None else None
         state = {"ckpt": ckpt, "k": k, "n": n, "nturns": nturns, "turn0": int(turn0),
-                 "stride": stride}
+                 "stride": stride, "estates": estates, "rfinal": rfinal}
         return r, lost.bool(), state
 
     def backward(self, state, g):
@@ -224,7 +236,11 @@ class AdjointTracker(TangentTracker):
                                   state["turn0"], state["stride"], self.pelem, self.porder,
                                   k.data_ptr() if self.nparam else None, lam.data_ptr(),
                                   gk.data_ptr() if self.nparam else None,
-                                  self.stream.cuda_stream)
+                                  self.stream.cuda_stream,
+                                  state["estates"].data_ptr() if state["estates"] is not None
+                                  else None,
+                                  state["rfinal"].data_ptr() if state["rfinal"] is not None
+                                  else None)
         cur.wait_stream(self.stream)
         return lam, gk
 

@@ -169,27 +169,32 @@ class Engine:
     def adjoint_forward(self, lid: int, r_ptr: int, npart: int, nturns: int, turn0: int,
                         param_elem: np.ndarray, param_order: np.ndarray, value_ptr: int | None,
                         ckpt_ptr: int | None, stride: int, lost_ptr: int | None = None,
-                        stream: int | None = None):
+                        stream: int | None = None, estates_ptr: int | None = None):
         """Enqueue the adjoint's forward pass: track the device (6, N) array in
         place with the strengths at ``value_ptr`` substituted, storing the
-        state entering every ``stride``-th turn at ``ckpt_ptr``."""
+        state entering every ``stride``-th turn at ``ckpt_ptr`` (and, with
+        ``estates_ptr``, every element's entry state of every turn)."""
         pe = np.ascontiguousarray(param_elem, dtype=np.int32)
         po = np.ascontiguousarray(param_order, dtype=np.int32)
         check(lib().atb_adjoint_forward(self.h, int(lid), r_ptr, int(npart), int(nturns),
                                         int(turn0), ptr(pe) if pe.size else None,
                                         ptr(po) if po.size else None, value_ptr, int(pe.size),
-                                        ckpt_ptr, int(stride), lost_ptr, stream))
+                                        ckpt_ptr, int(stride), estates_ptr, lost_ptr, stream))
 
     def adjoint_backward(self, lid: int, ckpt_ptr: int, npart: int, nturns: int, turn0: int,
                          stride: int, param_elem: np.ndarray, param_order: np.ndarray,
                          value_ptr: int | None, lam_ptr: int, gparam_ptr: int | None,
-                         stream: int | None = None):
+                         stream: int | None = None, estates_ptr: int | None = None,
+                         rfinal_ptr: int | None = None):
         """Enqueue the backward sweep: ``lam_ptr`` ((6, N) device) goes from
-        dL/d r_final to dL/d r_initial, ``gparam_ptr`` receives dL/dK."""
+        dL/d r_final to dL/d r_initial, ``gparam_ptr`` receives dL/dK (with
+        the forward pass's element states and final states, nothing is
+        tracked again)."""
         pe = np.ascontiguousarray(param_elem, dtype=np.int32)
         po = np.ascontiguousarray(param_order, dtype=np.int32)
         check(lib().atb_adjoint_backward(self.h, int(lid), ckpt_ptr, int(npart), int(nturns),
-                                         int(turn0), int(stride), ptr(pe) if pe.size else None,
+                                         int(turn0), int(stride), estates_ptr, rfinal_ptr,
+                                         ptr(pe) if pe.size else None,
                                          ptr(po) if po.size else None, value_ptr, int(pe.size),
                                          lam_ptr, gparam_ptr, stream))
 

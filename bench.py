@@ -828,6 +828,31 @@ def run_diff(device, n=65536):
                             "speedup_vs_tangent_vjp": (t_tan + t_bwd) / (t_afwd + t_abwd),
                             "rel_diff_vs_tangent": {"d_r0": rel(ax, vjp_x),
                                                     "d_strengths": rel(ak, vjp_k)}}}
+        # the adjoint with every element's entry state stored by the forward
+        # pass (N x 385 elements x turns x 48 B: 12 GB for 10 turns), so the
+        # backward sweep tracks nothing again
+        nt = 10
+        g = torch.randn((n, 6), dtype=torch.float64, device=dev)
+        ts = {}
+        for store in (False, True):
+            _, _, st = adj.forward(x, None, nt, store_elements=store)      # warm-up
+            adj.backward(st, g)
+            del st
+            e0.record()
+            _, _, st = adj.forward(x, None, nt, store_elements=store)
+            e1.record()
+            e1.synchronize()
+            tf = e0.elapsed_time(e1) * 1e-3
+            e0.record()
+            adj.backward(st, g)
+            e1.record()
+            e1.synchronize()
+            ts[store] = (tf, e0.elapsed_time(e1) * 1e-3)
+            del st
+        out["adjoint_10_turns"] = {
+            mode: {"forward_ms": 1e3 * ts[s][0], "backward_ms": 1e3 * ts[s][1],
+                   "particle_turns_per_s": n * nt / sum(ts[s])}
+            for mode, s in (("tracked_again", False), ("element_states_stored", True))}
     finally:
         eng.free(lid)
         tr.close()

@@ -169,14 +169,19 @@ int atb_tangent_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np,
  *       `nturns` whole turns (exact arithmetic, the strengths param_value
  *       substituted) and, when ckpt is not NULL, stores the state entering
  *       turns 0, stride, 2 stride, ... in ckpt ((ceil(nturns / stride), np, 6)).
- *       Lost particles come back NaN (islost, optional, marks them).
+ *       Lost particles come back NaN (islost, optional, marks them).  With
+ *       estates (device, nturns x nelem x np x 6 doubles; stride must be 1)
+ *       it also stores every element's entry state of every turn, which
+ *       spares the backward sweep its re-tracking.
  *   atb_adjoint_backward  from those checkpoints (same np, nturns, turn0,
  *       stride and strengths) and the cotangent lam = dL/d r_final
  *       ((6, np), in place), writes lam = dL/d r_initial and
  *       gparam (nparam) = dL/dK_q = sum over particles, for any scalar L of
  *       the final coordinates: one backward sweep, one launch per turn, whose
  *       cost does not grow with the number of strengths.  With stride > 1
- *       each block of turns is tracked again from its checkpoint.  Lost
+ *       each block of turns is tracked again from its checkpoint.  With the
+ *       forward pass's estates (and rfinal, its final states) nothing is
+ *       tracked again; NULL: each turn is tracked again from its checkpoint.  Lost
  *       particles get NaN in lam and add nothing to gparam.
  * Work buffers live on the handle: calls on one handle from different
  * streams must be ordered by the caller.  Replaces, for a scalar objective,
@@ -186,12 +191,13 @@ int atb_tangent_device(atb_handle* h, int32_t lattice_id, double* r, int64_t np,
 int atb_adjoint_forward(atb_handle* h, int32_t lattice_id, double* r, int64_t np,
                         int32_t nturns, int32_t turn0, const int32_t* param_elem,
                         const int32_t* param_order, const double* param_value, int32_t nparam,
-                        double* ckpt, int32_t stride, uint8_t* islost, void* stream);
+                        double* ckpt, int32_t stride, double* estates, uint8_t* islost,
+                        void* stream);
 int atb_adjoint_backward(atb_handle* h, int32_t lattice_id, const double* ckpt, int64_t np,
-                         int32_t nturns, int32_t turn0, int32_t stride,
-                         const int32_t* param_elem, const int32_t* param_order,
-                         const double* param_value, int32_t nparam, double* lam,
-                         double* gparam, void* stream);
+                         int32_t nturns, int32_t turn0, int32_t stride, const double* estates,
+                         const double* rfinal, const int32_t* param_elem,
+                         const int32_t* param_order, const double* param_value, int32_t nparam,
+                         double* lam, double* gparam, void* stream);
 
 /* Element maps for Ohmi's envelope (device pointers, enqueued on `stream`):
  * for a particle entering element i at orbits[6 i .. 6 i + 5], its transfer
