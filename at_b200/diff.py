@@ -16,7 +16,9 @@ The adjoint kernels (``atb_adjoint_forward`` / ``atb_adjoint_backward``) give
 the reverse mode: a forward pass that stores the state entering every
 ``stride``-th turn, and one backward sweep that maps dL/d r_final to
 dL/d r_initial and dL/dK for any scalar L, at a cost that does not grow with
-the number of strengths (:class:`AdjointTracker`).
+the number of strengths (:class:`AdjointTracker`; with ``store_elements`` the
+forward pass also keeps every element's entry state, so the backward sweep
+does not track the turns again, at N x elements x turns x 48 bytes).
 
 ``track`` wraps one call as a ``torch.autograd.Function``: the forward pass
 returns the final coordinates; the backward pass is either the contraction of

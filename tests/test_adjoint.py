@@ -283,12 +283,13 @@ def test_stored_element_states_give_the_same_gradients():
     for store in (False, True):
         at = diff.AdjointTracker(ring, params)
         try:
-            r, lost, st = at.forward(x0, None, 12, store_elements=store)
+            r, lost, st = at.forward(x0, None, 30, store_elements=store)
             gx, gk = at.backward(st, g)
             out.append((r, lost, gx, gk))
         finally:
             at.close()
     (r1, l1, gx1, gk1), (r2, l2, gx2, gk2) = out
-    assert l1.any() and torch.equal(l1, l2) and torch.equal(r1, r2)
+    assert l1.any() and torch.equal(l1, l2)
+    assert torch.equal(torch.nan_to_num(r1, nan=7.0), torch.nan_to_num(r2, nan=7.0))
     assert torch.equal(torch.nan_to_num(gx1, nan=7.0), torch.nan_to_num(gx2, nan=7.0))
     assert _scale_rel(gk2.cpu(), gk1.cpu()) <= 1e-13
