@@ -324,12 +324,21 @@ __device__ __forceinline__ void bndthinkick(P6T<T>& r, const PL& pl, double L, d
 /* Radiating kicks and drifts in the reference's expression order
  * (exact and tangent kernels). */
 
+/* The reference evaluates 1/(1+delta) at the start of every radiating drift
+ * and kick and again after each kick's energy loss.  delta changes only in
+ * that energy loss, so between two kicks every evaluation repeats the last one
+ * on the same operand and gives the same IEEE result.  The _pn forms take it
+ * from the caller (pn == 1.0 / (1.0 + r.dp) as last evaluated; a kick hands
+ * back the value after its loss), so a magnet's slice loop divides once per
+ * kick for it instead of once per drift and twice per kick. */
+
 /* diff_str_kick.c:19-83 with B2perp of diff_str_kick.c:1-17 (bdiff == NULL) */
 template <class PL, class T>
-__device__ __forceinline__ void str_kick_rad(P6T<T>& r, const PL& pl, double L, double radc) {
+__device__ __forceinline__ void str_kick_rad_pn(P6T<T>& r, const PL& pl, double L, double radc,
+                                                T& pn) {
     T re, im;
     pl.field(r.x, r.y, re, im);
-    T p_norm = 1.0 / (1.0 + r.dp);
+    T p_norm = pn;
     T xpr = r.px * p_norm;
     T ypr = r.py * p_norm;
     T v_norm2 = 1.0 / (1.0 + xpr * xpr + ypr * ypr);
@@ -338,6 +347,7 @@ __device__ __forceinline__ void str_kick_rad(P6T<T>& r, const PL& pl, double L, 
     T factor = (1.0 + (xpr * xpr + ypr * ypr) / 2.0) / (p_norm * p_norm) * L;
     r.dp -= radc * b2p * factor;
     p_norm = 1.0 / (1.0 + r.dp);
+    pn = p_norm;
     r.px = xpr / p_norm;
     r.py = ypr / p_norm;
     r.px = msub(r.px, L, re);
@@ -346,11 +356,11 @@ __device__ __forceinline__ void str_kick_rad(P6T<T>& r, const PL& pl, double L, 
 
 /* diff_bnd_kick.c:101-174 with its B2perp (:85-99), bdiff == NULL */
 template <class PL, class T>
-__device__ __forceinline__ void bnd_kick_rad(P6T<T>& r, const PL& pl, double L, double irho,
-                                             double lirho, double radc) {
+__device__ __forceinline__ void bnd_kick_rad_pn(P6T<T>& r, const PL& pl, double L, double irho,
+                                                double lirho, double radc, T& pn) {
     T re, im;
     pl.field(r.x, r.y, re, im);
-    T p_norm = 1.0 / (1.0 + r.dp);
+    T p_norm = pn;
     T x = r.x;
     T xpr = r.px * p_norm;
     T ypr = r.py * p_norm;
@@ -363,6 +373,7 @@ __device__ __forceinline__ void bnd_kick_rad(P6T<T>& r, const PL& pl, double L, 
     T dp_0 = r.dp;
     r.dp -= radc * b2p * factor;
     p_norm = 1.0 / (1.0 + r.dp);
+    pn = p_norm;
     r.px = xpr / p_norm;
     r.py = ypr / p_norm;
     r.px -= L * (re - (dp_0 - r.x * irho) * irho);
@@ -372,8 +383,8 @@ __device__ __forceinline__ void bnd_kick_rad(P6T<T>& r, const PL& pl, double L, 
 
 /* diff_drift.c:30-43 (bdiff == NULL) */
 template <class T>
-__device__ __forceinline__ void diff_drift(P6T<T>& r, double L) {
-    T p_norm = 1.0 / (1.0 + r.dp);
+__device__ __forceinline__ void diff_drift_pn(P6T<T>& r, double L, const T& pn) {
+    T p_norm = pn;
     T NormL = L * p_norm;
     r.x = madd(r.x, NormL, r.px);
     r.y = madd(r.y, NormL, r.py);

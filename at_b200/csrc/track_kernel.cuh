@@ -213,19 +213,22 @@ __device__ __forceinline__ void multipole_steps_generic(P6T<T>* r, const Rec& e,
                 r[k].py = a[k].yp * a[k].opd;
             }
         } else {
+            T pn[NP];   /* 1/(1+delta) as last evaluated, as in the steps below */
+#pragma unroll
+            for (int k = 0; k < NP; ++k) pn[k] = 1.0 / (1.0 + r[k].dp);
             for (int m = 0; m < ns; ++m) {
                 for (int i = 0; i < ig.n; ++i) {
                     if (ig.c[i] != 0.0) {
                         const double ld = SL * ig.c[i];
 #pragma unroll
-                        for (int k = 0; k < NP; ++k) diff_drift(r[k], ld);
+                        for (int k = 0; k < NP; ++k) diff_drift_pn(r[k], ld, pn[k]);
                     }
                     if (ig.d[i] != 0.0) {
                         const double lk = SL * ig.d[i];
 #pragma unroll
                         for (int k = 0; k < NP; ++k) {
-                            if (BEND) bnd_kick_rad(r[k], pl, lk, irho, lk * irho, radc);
-                            else str_kick_rad(r[k], pl, lk, radc);
+                            if (BEND) bnd_kick_rad_pn(r[k], pl, lk, irho, lk * irho, radc, pn[k]);
+                            else str_kick_rad_pn(r[k], pl, lk, radc, pn[k]);
                         }
                     }
                 }
@@ -372,19 +375,24 @@ __device__ __forceinline__ void pass_multipole_n(P6T<T>* r, const Rec& e, const 
                 }
             }
         } else {
+            /* pn: 1/(1+delta) as the reference last evaluated it (it changes
+               only in a kick's energy loss, and the kick hands it on) */
+            T pn[NP];
+#pragma unroll
+            for (int k = 0; k < NP; ++k) pn[k] = 1.0 / (1.0 + r[k].dp);
             for (int m = 0; m < ns; ++m) {
 #pragma unroll
                 for (int k = 0; k < NP; ++k) {
-                    diff_drift(r[k], L1);
-                    if (BEND) bnd_kick_rad(r[k], pl, K1, irho, k1i, radc);
-                    else str_kick_rad(r[k], pl, K1, radc);
-                    diff_drift(r[k], L2);
-                    if (BEND) bnd_kick_rad(r[k], pl, K2, irho, k2i, radc);
-                    else str_kick_rad(r[k], pl, K2, radc);
-                    diff_drift(r[k], L2);
-                    if (BEND) bnd_kick_rad(r[k], pl, K1, irho, k1i, radc);
-                    else str_kick_rad(r[k], pl, K1, radc);
-                    diff_drift(r[k], L1);
+                    diff_drift_pn(r[k], L1, pn[k]);
+                    if (BEND) bnd_kick_rad_pn(r[k], pl, K1, irho, k1i, radc, pn[k]);
+                    else str_kick_rad_pn(r[k], pl, K1, radc, pn[k]);
+                    diff_drift_pn(r[k], L2, pn[k]);
+                    if (BEND) bnd_kick_rad_pn(r[k], pl, K2, irho, k2i, radc, pn[k]);
+                    else str_kick_rad_pn(r[k], pl, K2, radc, pn[k]);
+                    diff_drift_pn(r[k], L2, pn[k]);
+                    if (BEND) bnd_kick_rad_pn(r[k], pl, K1, irho, k1i, radc, pn[k]);
+                    else str_kick_rad_pn(r[k], pl, K1, radc, pn[k]);
+                    diff_drift_pn(r[k], L1, pn[k]);
                 }
             }
         }
