@@ -763,17 +763,24 @@ int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns
         ATB_CUDA(cudaMemcpyAsync(h->refpts.p, refpts, (size_t)nref * 4, cudaMemcpyHostToDevice, st));
     }
 
-    /* turn chunks bounded by the snapshot budget */
+    /* Snapshots bounded by the device budget: turns in chunks, and when one
+       turn of snapshots of all particles does not fit, particles in groups
+       whose snapshots go to their columns of every slot of rout (the
+       particles are independent, so a group sees exactly what it would in one
+       launch; per-turn statistics add up over the groups). */
     const int64_t rec_first = nref ? count_records(refpts, nref, start_elem, end_elem, nelem) : 0;
     const int64_t rec_turn = nref ? count_records(refpts, nref, 0, end_elem, nelem) : 0;
-    const int64_t slot_bytes = (int64_t)np * 48;
-    int64_t turns_per_chunk = nturns;
-    if (nref > 0 && rec_turn > 0) {
-        int64_t per_turn = rec_turn * slot_bytes;
-        turns_per_chunk = std::max<int64_t>(1, h->rout_budget / std::max<int64_t>(per_turn, 1));
-        if (std::max(rec_first, rec_turn) * slot_bytes > h->rout_budget)
-            return fail(ATB_ERR_NOMEM, "one turn of refpts snapshots exceeds the device budget");
+    const int64_t rec_max = std::max(rec_first, rec_turn);
+    int64_t group = np;
+    if (nref > 0 && rec_max > 0) {
+        group = std::min<int64_t>(np, h->rout_budget / (rec_max * 48));
+        if (group < 1)
+            return fail(ATB_ERR_NOMEM, "one turn of refpts snapshots of one particle exceeds the device budget");
     }
+    const int64_t slot_bytes = group * 48;
+    int64_t turns_per_chunk = nturns;
+    if (nref > 0 && rec_turn > 0)
+        turns_per_chunk = std::max<int64_t>(1, h->rout_budget / (rec_turn * slot_bytes));
     const int64_t max_slots = nref ? std::max<int64_t>(rec_first, 0) +
                                          (turns_per_chunk - 1) * rec_turn + rec_turn
                                    : 0;
@@ -788,46 +795,54 @@ int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns
     int rc = kernel_config(h, lats, mode, &smem, &grid_max, &gen);
     if (rc) return rc;
 
-    int64_t slot_done = 0;
-    for (int64_t t0 = 0; t0 < nturns; t0 += turns_per_chunk) {
-        const int nt = (int)std::min<int64_t>(turns_per_chunk, nturns - t0);
-        AtbJob J;
-        std::memset(&J, 0, sizeof(J));
-        fill_job_lattice(J, *L, t0 == 0 ? start_elem : 0, end_elem);
-        J.rng_key = job_key(h, 0);
-        J.check_loss = (flags & ATB_FLAG_ELEMENT) ? 0 : 1;
-        J.r = h->r.as<double>();
-        J.np = np;
-        J.turn0 = turn0 + (int32_t)t0;
-        J.nturns = nt;
-        J.refpts = h->refpts.as<uint32_t>();
-        J.nref = nref;
-        J.losses = losses ? 1 : 0;
-        J.rout = nref ? h->rout.as<double>() : nullptr;
-        J.rout_slot0 = 0;
-        J.lost = h->lost.as<uint8_t>();
-        J.lturn = h->lturn.as<uint32_t>();
-        J.lelem = h->lelem.as<uint32_t>();
-        J.lcoord = h->lcoord.as<double>();
-        J.alive = (alive || moments) ? h->alive.as<uint32_t>() + t0 : nullptr;
-        J.moments = (alive || moments) ? h->moments.as<double>() + 12 * t0 : nullptr;
-        std::vector<AtbJob> jobs{J};
-        h->h_tiles.clear();
-        const int pp = gen ? 1 : ppt_for(h, np);
-        const int thr = pp > 1 ? h->threads : threads_for(h, np);
-        make_tiles(h->h_tiles, 0, np, thr * pp);
-        rc = launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr, pp, gen);
-        if (rc) return rc;
-        if (nref) {
-            int64_t slots = (t0 == 0 ? rec_first : rec_turn) + (int64_t)(nt - 1) * rec_turn;
-            if (slots > 0)
-                ATB_CUDA(cudaMemcpyAsync(rout + slot_done * (slot_bytes / 8), h->rout.p,
-                                         (size_t)(slots * slot_bytes), cudaMemcpyDeviceToHost, st));
-            slot_done += slots;
+    for (int64_t a = 0; a < np; a += group) {
+        const int64_t gn = std::min<int64_t>(group, np - a);
+        int64_t slot_done = 0;
+        for (int64_t t0 = 0; t0 < nturns; t0 += turns_per_chunk) {
+            const int nt = (int)std::min<int64_t>(turns_per_chunk, nturns - t0);
+            AtbJob J;
+            std::memset(&J, 0, sizeof(J));
+            fill_job_lattice(J, *L, t0 == 0 ? start_elem : 0, end_elem);
+            J.rng.key = job_key(h, 0);
+            J.check_loss = (flags & ATB_FLAG_ELEMENT) ? 0 : 1;
+            J.rng.pbase = a;
+            J.r = h->r.as<double>() + 6 * a;
+            J.np = gn;
+            J.turn0 = turn0 + (int32_t)t0;
+            J.nturns = nt;
+            J.refpts = h->refpts.as<uint32_t>();
+            J.nref = nref;
+            J.losses = losses ? 1 : 0;
+            J.rout = nref ? h->rout.as<double>() : nullptr;
+            J.rout_slot0 = 0;
+            J.lost = losses ? h->lost.as<uint8_t>() + a : nullptr;
+            J.lturn = losses ? h->lturn.as<uint32_t>() + a : nullptr;
+            J.lelem = losses ? h->lelem.as<uint32_t>() + a : nullptr;
+            J.lcoord = losses ? h->lcoord.as<double>() + 6 * a : nullptr;
+            J.alive = (alive || moments) ? h->alive.as<uint32_t>() + t0 : nullptr;
+            J.moments = (alive || moments) ? h->moments.as<double>() + 12 * t0 : nullptr;
+            std::vector<AtbJob> jobs{J};
+            h->h_tiles.clear();
+            const int pp = gen ? 1 : ppt_for(h, gn);
+            const int thr = pp > 1 ? h->threads : threads_for(h, gn);
+            make_tiles(h->h_tiles, 0, gn, thr * pp);
+            rc = launch(h, jobs, h->h_tiles, smem, grid_max, mode, st, thr, pp, gen);
+            if (rc) return rc;
+            if (nref) {
+                int64_t slots = (t0 == 0 ? rec_first : rec_turn) + (int64_t)(nt - 1) * rec_turn;
+                if (slots > 0 && gn == np)
+                    ATB_CUDA(cudaMemcpyAsync(rout + slot_done * np * 6, h->rout.p,
+                                             (size_t)(slots * gn * 48), cudaMemcpyDeviceToHost, st));
+                else if (slots > 0)
+                    ATB_CUDA(cudaMemcpy2DAsync(rout + (slot_done * np + a) * 6, (size_t)np * 48,
+                                               h->rout.p, (size_t)gn * 48, (size_t)gn * 48,
+                                               (size_t)slots, cudaMemcpyDeviceToHost, st));
+                slot_done += slots;
+            }
+            /* the job/tile lists are host vectors reused next chunk: make sure
+               the copies above have consumed them */
+            ATB_CUDA(cudaStreamSynchronize(st));
         }
-        /* the job/tile lists are host vectors reused next chunk: make sure
-           the copies above have consumed them */
-        ATB_CUDA(cudaStreamSynchronize(st));
     }
     ATB_CUDA(cudaMemcpyAsync(rin, h->r.p, rbytes, cudaMemcpyDeviceToHost, st));
     if (losses) {
@@ -865,7 +880,7 @@ int atb_track_device(atb_handle* h, int32_t id, double* r, int64_t np, int32_t n
     AtbJob J;
     std::memset(&J, 0, sizeof(J));
     fill_job_lattice(J, *L, 0, L->nelem);
-    J.rng_key = job_key(h, 0);
+    J.rng.key = job_key(h, 0);
     J.check_loss = 1;
     J.r = r;
     J.np = np;
@@ -1224,7 +1239,7 @@ int atb_track_batch(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, int3
         lats.push_back(L);
         std::memset(&J[j], 0, sizeof(AtbJob));
         fill_job_lattice(J[j], *L, 0, L->nelem);
-        J[j].rng_key = job_key(h, j);
+        J[j].rng.key = job_key(h, j);
         J[j].check_loss = 1;
         J[j].r = d.r;
         J[j].np = d.np;
@@ -1271,7 +1286,7 @@ int atb_batch_prepare(atb_handle* h, const atb_job_desc* jobs, int32_t njobs, in
         lats.push_back(L);
         std::memset(&J[j], 0, sizeof(AtbJob));
         fill_job_lattice(J[j], *L, 0, L->nelem);
-        J[j].rng_key = job_key(h, j);
+        J[j].rng.key = job_key(h, j);
         J[j].check_loss = 1;
         J[j].r = d.r;
         J[j].np = d.np;
@@ -1652,7 +1667,7 @@ int atb_serve_submit(atb_server* s, const atb_job_desc* d, int32_t chunk_turns,
     AtbJob& J = *s->h_job;
     std::memset(&J, 0, sizeof(AtbJob));
     fill_job_lattice(J, *L, 0, L->nelem);
-    J.rng_key = job_key(h, s->njobs);
+    J.rng.key = job_key(h, s->njobs);
     J.check_loss = 1;
     J.r = d->r;
     J.np = d->np;

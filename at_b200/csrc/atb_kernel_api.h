@@ -87,6 +87,14 @@ typedef struct AtbSeg {
     int32_t pad;
 } AtbSeg;
 
+/* The quantum-diffusion kicks of a job: the normals of its particle p are
+ * a function of (key, pbase + p, turn, element), pbase placing the job's
+ * particles in a larger set that the host tracks in parts. */
+typedef struct AtbRng {
+    uint64_t key;
+    int64_t pbase;
+} AtbRng;
+
 typedef struct AtbJob {
     const double* table;        /* element table words                      */
     const AtbSeg* segs;         /* segment list                             */
@@ -114,7 +122,7 @@ typedef struct AtbJob {
     double* lcoord;
     uint32_t* alive;            /* optional: survivors after each turn     */
     double* moments;            /* optional: 12 sums per turn              */
-    uint64_t rng_key;           /* key of the quantum-diffusion kicks      */
+    AtbRng rng;                 /* quantum-diffusion kicks                  */
     int32_t chunk;              /* serving: turns per claim, 0 all (a tile
                                    re-enqueues itself for the rest)         */
     int32_t pad_serve;

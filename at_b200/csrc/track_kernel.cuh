@@ -599,16 +599,16 @@ __device__ __forceinline__ void pass_corrector(P6T<T>& r, const Rec& e) {
 
 /* One element on one particle; lost particles (x is NaN) are skipped as every
  * reference pass method does (e.g. StrMPoleSymplectic4Pass.c:59). */
-/* QuantDiffPass.c: random kicks keyed by (key, p, nturn, ei); without a
- * key (the derivative kernels) the element is the identity, as the
+/* QuantDiffPass.c: random kicks keyed by (key, pbase + p, nturn, ei);
+ * without a key (the derivative kernels) the element is the identity, as the
  * reference's envelope code disables it */
 template <class T>
-__device__ __forceinline__ void pass_quantdiff(P6T<T>& r, const Rec& e, const uint64_t* rng_key,
+__device__ __forceinline__ void pass_quantdiff(P6T<T>& r, const Rec& e, const AtbRng* rng,
                                                long long p, int nturn, int ei) {
     if constexpr (!is_dual<T>::value) {
-        if (rng_key) {
+        if (rng) {
             double z[6];
-            quantdiff_normals(*rng_key, p, nturn, ei, z);
+            quantdiff_normals(rng->key, rng->pbase + p, nturn, ei, z);
             quantdiff_kick(r, e.p + ATB_QD_L, z);
         }
     }
@@ -617,7 +617,7 @@ __device__ __forceinline__ void pass_quantdiff(P6T<T>& r, const Rec& e, const ui
 template <bool GEN = false, class T>
 __device__ __forceinline__ void track_element(P6T<T>& r, const Rec& e, int nturn,
                                               const Param& pm = Param{-1, 0.0},
-                                              const uint64_t* rng_key = nullptr, long long p = 0,
+                                              const AtbRng* rng = nullptr, long long p = 0,
                                               int ei = 0) {
     if (isnan(val(r.x))) return;
     switch (e.op()) {
@@ -631,7 +631,7 @@ __device__ __forceinline__ void track_element(P6T<T>& r, const Rec& e, int nturn
         case ATB_OP_RFCAVITY: pass_rfcavity(r, e, nturn); break;
         case ATB_OP_CORRECTOR: pass_corrector(r, e); break;
         case ATB_OP_APERTURE: check_rect(r, e.p + ATB_AP_LIM); break;
-        case ATB_OP_QUANTDIFF: pass_quantdiff(r, e, rng_key, p, nturn, ei); break;
+        case ATB_OP_QUANTDIFF: pass_quantdiff(r, e, rng, p, nturn, ei); break;
         default: break;
     }
 }
@@ -1035,7 +1035,7 @@ __device__ __forceinline__ void track_tiles(const AtbJob* __restrict__ jobs,
                     } else {
 #pragma unroll
                         for (int k = 0; k < NP; ++k)
-                            track_element<GEN>(r[k], e, nturn[k], Param{-1, 0.0}, &J.rng_key,
+                            track_element<GEN>(r[k], e, nturn[k], Param{-1, 0.0}, &J.rng,
                                                p[k], ei);
                     }
 #pragma unroll

@@ -58,6 +58,7 @@ class Engine:
         self.h = h
         self.device = int(device)
         self.lock = threading.Lock()
+        self.nelem = {}            # lattice id -> number of elements
 
     @classmethod
     def get(cls, device: int = 0) -> "Engine":
@@ -96,6 +97,7 @@ class Engine:
         off = np.ascontiguousarray(cl.offsets, dtype=np.uint32)
         check(lib().atb_lattice_upload(self.h, ptr(words) if words.size else None,
                                        int(words.size), ptr(off), int(cl.nelem), C.byref(lid)))
+        self.nelem[lid.value] = int(cl.nelem)
         return lid.value
 
     def update(self, lid: int, cl: CompiledLattice):
@@ -105,14 +107,20 @@ class Engine:
 
     def free(self, lid: int):
         check(lib().atb_lattice_free(self.h, int(lid)))
+        self.nelem.pop(int(lid), None)
 
     # -- tracking -----------------------------------------------------------
     def track(self, lid: int, r: np.ndarray, nturns: int, turn0: int = 0, start_elem: int = 0,
-              end_elem: int = 0, refpts: np.ndarray | None = None, losses: bool = False,
+              end_elem: int | None = None, refpts: np.ndarray | None = None, losses: bool = False,
               stats: bool = False, mode=None, element: bool = False):
-        """Track the (6, N) Fortran-ordered array ``r`` in place.
+        """Track the (6, N) Fortran-ordered array ``r`` in place through
+        elements [start_elem, end_elem) of the first turn and [0, end_elem) of
+        the others (``end_elem`` None: every element of the lattice; 0 stops
+        before the first element, as in the C interface).
 
         Returns ``(rout, loss_dict or None, (alive, moments) or None)``."""
+        if end_elem is None:
+            end_elem = self.nelem[int(lid)]
         npart = r.size // 6
         nref = 0 if refpts is None else int(refpts.size)
         rout = np.empty((6, npart, nref, nturns), dtype=np.float64, order="F")

@@ -128,7 +128,12 @@ int atb_lattice_free(atb_handle* h, int32_t lattice_id);
  *           squares over survivors after each turn, or NULL
  * turn0 is the reference's param.nturn at the first turn (the `turn` or kept
  * counter, pyat/at.c:428-431); start_elem/end_elem as pyat/at.c:514-536.
- * Blocks until the results are back in host memory. */
+ * The snapshots pass through a device buffer of at most the handle's
+ * snapshot budget (atb_set_launch, 4 GB by default): the turns are tracked
+ * in chunks whose snapshots fit it, and when one turn of all particles' does
+ * not, the particles in groups (same results; ATB_ERR_NOMEM only if one
+ * particle's turn exceeds the budget).  Blocks until the results are back in
+ * host memory. */
 int atb_track(atb_handle* h, int32_t lattice_id, double* rin, int64_t np, int32_t nturns,
               int32_t turn0, int32_t start_elem, int32_t end_elem, const uint32_t* refpts,
               int32_t nref, double* rout, int32_t losses, uint8_t* islost, uint32_t* lturn,

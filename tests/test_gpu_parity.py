@@ -316,8 +316,45 @@ def test_pipelined_segments_match_resident(mode):
     finally:
         eng.set_launch(seg_cap_words=6144, resident_max_words=14336)
         eng.free(lid)
+    assert not np.array_equal(ra, r0, equal_nan=True)             # tracked
     np.testing.assert_array_equal(ra, rb)
 
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_snapshots_beyond_the_budget_track_in_particle_groups(mode):
+    """When one turn of refpts snapshots of all particles exceeds the device
+    budget, the runtime tracks the particles in groups and copies each
+    group's snapshots into its columns of rout: the snapshots, final
+    coordinates, loss map (quantum-diffusion kicks included, keyed by the
+    particle's index in the whole set) and survivors per turn equal one
+    launch's; the per-turn moments are float sums in another order."""
+    qd = E.QuantumDiffusion("QD", np.diag([2e-5, 2e-6, 2e-5, 2e-6, 1e-4, 1e-5]))
+    fodo = rings.radiating(rings.fodo_ring())
+    ring = E.Lattice(list(fodo) + [qd], energy=fodo.energy, particle=fodo.particle)
+    eng = Engine.get(0)
+    cl = compile_lattice(ring, ring.energy, ELECTRON_REST)
+    lid = eng.upload(cl)
+    n, nt = 1000, 3
+    refs = np.arange(cl.nelem + 1, dtype=np.uint32)      # every element and the turn's end
+    r0 = rings.gaussian(n, seed=4) * 40.0                # about a quarter lost in 3 turns
+    try:
+        ra = r0.copy(order="F")
+        oa = eng.track(lid, ra, nt, refpts=refs, losses=True, stats=True, mode=mode)
+        eng.set_launch(rout_budget_bytes=refs.size * 48 * 150)     # 150 particles a group
+        rb = r0.copy(order="F")
+        ob = eng.track(lid, rb, nt, refpts=refs, losses=True, stats=True, mode=mode)
+    finally:
+        eng.set_launch(rout_budget_bytes=4 << 30)
+        eng.free(lid)
+    assert oa[1]["islost"].any() and not oa[1]["islost"].all()
+    np.testing.assert_array_equal(rb, ra)
+    np.testing.assert_array_equal(ob[0], oa[0])
+    for k in oa[1]:
+        np.testing.assert_array_equal(ob[1][k], oa[1][k], err_msg=k)
+    np.testing.assert_array_equal(ob[2][0], oa[2][0])
+    scale = np.abs(oa[2][1]).max(axis=0)                 # per moment, over the turns
+    assert (np.abs(ob[2][1] - oa[2][1]) <= 1e-12 * scale).all()
 
 def test_large_ring_one_turn():
     """The radiating large ring (misaligned, 1954 elements) against the oracle.

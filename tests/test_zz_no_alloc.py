@@ -154,4 +154,5 @@ def test_handle_path_after_noalloc_keeps_its_shared_memory_limit():
     finally:
         eng.set_launch(resident_max_words=14336)
         eng.free(lid)
+    assert not np.array_equal(ra, r0, equal_nan=True)         # tracked
     np.testing.assert_array_equal(rb, ra)
