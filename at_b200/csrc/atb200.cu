@@ -781,9 +781,13 @@ int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns
     int64_t turns_per_chunk = nturns;
     if (nref > 0 && rec_turn > 0)
         turns_per_chunk = std::max<int64_t>(1, h->rout_budget / (rec_turn * slot_bytes));
-    const int64_t max_slots = nref ? std::max<int64_t>(rec_first, 0) +
-                                         (turns_per_chunk - 1) * rec_turn + rec_turn
-                                   : 0;
+    /* the first chunk holds rec_first + (nt - 1) rec_turn slots, the others
+       nt rec_turn, nt <= turns_per_chunk: within the budget */
+    const int64_t max_slots =
+        nref ? std::max<int64_t>(
+                   rec_first + (std::min<int64_t>(turns_per_chunk, nturns) - 1) * rec_turn,
+                   turns_per_chunk * rec_turn)
+             : 0;
     if (nref > 0 && max_slots > 0) {
         if (h->rout.ensure((size_t)(max_slots * slot_bytes)) != cudaSuccess)
             return fail(ATB_ERR_NOMEM, "cudaMalloc(refpts snapshots) failed");

@@ -338,23 +338,30 @@ def test_snapshots_beyond_the_budget_track_in_particle_groups(mode):
     n, nt = 1000, 3
     refs = np.arange(cl.nelem + 1, dtype=np.uint32)      # every element and the turn's end
     r0 = rings.gaussian(n, seed=4) * 40.0                # about a quarter lost in 3 turns
+    # budgets in particle-turns of snapshots: groups of 150 one turn at a time;
+    # all particles one turn at a time (turn chunks only); groups of 800 (and
+    # the remaining 200) two turns at a time
+    runs = []
     try:
         ra = r0.copy(order="F")
         oa = eng.track(lid, ra, nt, refpts=refs, losses=True, stats=True, mode=mode)
-        eng.set_launch(rout_budget_bytes=refs.size * 48 * 150)     # 150 particles a group
-        rb = r0.copy(order="F")
-        ob = eng.track(lid, rb, nt, refpts=refs, losses=True, stats=True, mode=mode)
+        for pt in (150, 1000, 1600):
+            eng.set_launch(rout_budget_bytes=refs.size * 48 * pt)
+            rb = r0.copy(order="F")
+            runs.append((rb, eng.track(lid, rb, nt, refpts=refs, losses=True, stats=True,
+                                       mode=mode)))
     finally:
         eng.set_launch(rout_budget_bytes=4 << 30)
         eng.free(lid)
     assert oa[1]["islost"].any() and not oa[1]["islost"].all()
-    np.testing.assert_array_equal(rb, ra)
-    np.testing.assert_array_equal(ob[0], oa[0])
-    for k in oa[1]:
-        np.testing.assert_array_equal(ob[1][k], oa[1][k], err_msg=k)
-    np.testing.assert_array_equal(ob[2][0], oa[2][0])
     scale = np.abs(oa[2][1]).max(axis=0)                 # per moment, over the turns
-    assert (np.abs(ob[2][1] - oa[2][1]) <= 1e-12 * scale).all()
+    for rb, ob in runs:
+        np.testing.assert_array_equal(rb, ra)
+        np.testing.assert_array_equal(ob[0], oa[0])
+        for k in oa[1]:
+            np.testing.assert_array_equal(ob[1][k], oa[1][k], err_msg=k)
+        np.testing.assert_array_equal(ob[2][0], oa[2][0])
+        assert (np.abs(ob[2][1] - oa[2][1]) <= 1e-12 * scale).all()
 
 def test_large_ring_one_turn():
     """The radiating large ring (misaligned, 1954 elements) against the oracle.
