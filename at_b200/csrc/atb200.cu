@@ -13,6 +13,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/atb200.h"
@@ -159,6 +160,8 @@ struct atb_handle {
     std::vector<int32_t> h_pelem;
     std::vector<AtbTile> h_tiles;
     std::vector<struct Batch> batches;
+    char* stage[2] = {nullptr, nullptr};            /* pinned snapshot staging */
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
 };
 
 /* The serving loop: a persistent kernel that claims tiles from a queue the
@@ -570,6 +573,10 @@ int atb_destroy(atb_handle* h) {
                           &h->adj_state,
                           &h->jobnext})
             b->release();
+        for (int i = 0; i < 2; ++i) {
+            if (h->stage[i]) cudaFreeHost(h->stage[i]);
+            if (h->stage_ev[i]) cudaEventDestroy(h->stage_ev[i]);
+        }
         if (h->stream) cudaStreamDestroy(h->stream);
     }
     delete h;
@@ -712,6 +719,79 @@ int atb_lattice_free(atb_handle* h, int32_t id) {
     return ATB_OK;
 }
 
+namespace {
+
+constexpr int64_t kStageBytes = 64LL << 20;   /* each of the two staging buffers */
+constexpr int64_t kStageDirect = 8LL << 20;   /* smaller copies go directly      */
+
+/* The snapshots of one chunk -- `slots` slots of gn particles, gn * 48 bytes
+   each, contiguous on the device -- to slots [slot0, slot0 + slots) of the
+   caller's rout (np particles a slot), columns [a, a + gn).  Small copies go
+   directly; large ones through two pinned staging buffers: the GPU fills one
+   while host threads place the other, so the copy is not held to one
+   thread's pace through the caller's fresh (not yet touched) pages. */
+int copy_snapshots(atb_handle* h, cudaStream_t st, const double* dev, int64_t slots, int64_t gn,
+                   double* rout, int64_t np, int64_t a, int64_t slot0) {
+    const int64_t row = gn * 48, pitch = np * 48, total = slots * row;
+    char* dst = reinterpret_cast<char*>(rout + (slot0 * np + a) * 6);
+    if (total <= kStageDirect) {
+        if (gn == np)
+            ATB_CUDA(cudaMemcpyAsync(dst, dev, (size_t)total, cudaMemcpyDeviceToHost, st));
+        else
+            ATB_CUDA(cudaMemcpy2DAsync(dst, (size_t)pitch, dev, (size_t)row, (size_t)row,
+                                       (size_t)slots, cudaMemcpyDeviceToHost, st));
+        return ATB_OK;
+    }
+    for (int i = 0; i < 2; ++i) {
+        if (!h->stage[i])
+            ATB_CUDA(cudaHostAlloc((void**)&h->stage[i], (size_t)kStageBytes, cudaHostAllocDefault));
+        if (!h->stage_ev[i])
+            ATB_CUDA(cudaEventCreateWithFlags(&h->stage_ev[i], cudaEventDisableTiming));
+    }
+    const char* src = reinterpret_cast<const char*>(dev);
+    const int64_t npieces = (total + kStageBytes - 1) / kStageBytes;
+    auto issue = [&](int64_t p) {
+        const int64_t off = p * kStageBytes, len = std::min(kStageBytes, total - off);
+        cudaError_t e = cudaMemcpyAsync(h->stage[p & 1], src + off, (size_t)len,
+                                        cudaMemcpyDeviceToHost, st);
+        return e == cudaSuccess ? cudaEventRecord(h->stage_ev[p & 1], st) : e;
+    };
+    const int nthr = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    for (int64_t p = 0; p < std::min<int64_t>(2, npieces); ++p) ATB_CUDA(issue(p));
+    for (int64_t p = 0; p < npieces; ++p) {
+        ATB_CUDA(cudaEventSynchronize(h->stage_ev[p & 1]));
+        const int64_t off = p * kStageBytes, len = std::min(kStageBytes, total - off);
+        const char* stage = h->stage[p & 1];
+        /* device bytes [b0, b1) of this piece to their rows of rout */
+        auto place = [=](int64_t b0, int64_t b1) {
+            while (b0 < b1) {
+                const int64_t slot = b0 / row, within = b0 - slot * row;
+                const int64_t n = std::min(b1 - b0, row - within);
+                std::memcpy(dst + slot * pitch + within, stage + (b0 - off), (size_t)n);
+                b0 += n;
+            }
+        };
+        const int64_t part = (len + nthr - 1) / nthr;
+        std::vector<std::thread> th;
+        for (int t = 1; t < nthr; ++t) {
+            const int64_t b0 = off + std::min<int64_t>(len, t * part);
+            const int64_t b1 = off + std::min<int64_t>(len, (t + 1) * part);
+            if (b0 >= b1) continue;
+            try {
+                th.emplace_back(place, b0, b1);
+            } catch (...) {
+                place(b0, b1);     /* no thread to be had: this one does it */
+            }
+        }
+        place(off, off + std::min<int64_t>(len, part));
+        for (std::thread& x : th) x.join();
+        if (p + 2 < npieces) ATB_CUDA(issue(p + 2));   /* into the buffer just placed */
+    }
+    return ATB_OK;
+}
+
+}  // namespace
+
 int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns, int32_t turn0,
               int32_t start_elem, int32_t end_elem, const uint32_t* refpts, int32_t nref,
               double* rout, int32_t losses, uint8_t* islost, uint32_t* lturn, uint32_t* lelem,
@@ -834,13 +914,11 @@ int atb_track(atb_handle* h, int32_t id, double* rin, int64_t np, int32_t nturns
             if (rc) return rc;
             if (nref) {
                 int64_t slots = (t0 == 0 ? rec_first : rec_turn) + (int64_t)(nt - 1) * rec_turn;
-                if (slots > 0 && gn == np)
-                    ATB_CUDA(cudaMemcpyAsync(rout + slot_done * np * 6, h->rout.p,
-                                             (size_t)(slots * gn * 48), cudaMemcpyDeviceToHost, st));
-                else if (slots > 0)
-                    ATB_CUDA(cudaMemcpy2DAsync(rout + (slot_done * np + a) * 6, (size_t)np * 48,
-                                               h->rout.p, (size_t)gn * 48, (size_t)gn * 48,
-                                               (size_t)slots, cudaMemcpyDeviceToHost, st));
+                if (slots > 0) {
+                    rc = copy_snapshots(h, st, h->rout.as<double>(), slots, gn, rout, np, a,
+                                        slot_done);
+                    if (rc) return rc;
+                }
                 slot_done += slots;
             }
             /* the job/tile lists are host vectors reused next chunk: make sure

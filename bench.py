@@ -87,6 +87,8 @@ def _args():
                     help="skip the FODO (10,000 particles x 1000 turns) line")
     ap.add_argument("--no-alt-line", action="store_true",
                     help="skip timing the other arithmetic mode beside the headline's")
+    ap.add_argument("--refpts-line", action="store_true",
+                    help="also time snapshots at every element (FODO, 10,000 particles)")
     return ap.parse_args()
 
 
@@ -483,6 +485,9 @@ def run_b200(a):
     acc = None
     if world == 1 and not a.no_acceptance:
         acc = run_acceptance(mode, cpu)
+    refl = None
+    if world == 1 and a.refpts_line:
+        refl = run_refpts_line(local, mode)
 
     traffic = None
     prof = os.path.join(REPO, "profiles", "traffic_%s.json" % a.workload)
@@ -512,6 +517,8 @@ def run_b200(a):
             "serving": serve, "differentiation": dif, "batching": bat, "acceptance": acc,
             "%s_arithmetic" % alt: alt_line,
         }
+        if refl is not None:
+            line["refpts_every_element"] = refl
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -590,6 +597,37 @@ def run_fodo_line(device, with_cpu):
         c = cpu_rate("fodo")
         out["cpu_baseline"] = {"value": c["rate"], "unit": UNIT, "cores": c["threads"],
                                "kind": c["kind"], "sample": c["sample"]}
+    return out
+
+
+def run_refpts_line(device, mode, n=10_000, nt=20, reps=3):
+    """Snapshots at every element: the FODO ring, ``n`` particles (Gaussian,
+    seed 0), ``nt`` turns, refpts at each of the 385 elements and at the
+    turn's end, end to end through ``gpupass`` on host arrays (the result
+    array allocated by the call, as the reference's is), beside the same call
+    without refpts.  The difference is the cost of writing the snapshots and
+    returning them to the host, reported against the snapshot bytes."""
+    from at_b200 import rings, tracking
+
+    ring = rings.fodo_ring()
+    refs = np.arange(len(ring) + 1, dtype=np.uint32)
+    r0 = rings.gaussian(n, seed=0)
+    out = {"workload": "FODO ring (385 elements), %d particles, %d turns, refpts at all %d "
+                       "points, losses on" % (n, nt, refs.size),
+           "arithmetic": mode, "rout_bytes": 48 * n * refs.size * nt}
+    for name, rp in (("without_refpts", None), ("with_refpts", refs)):
+        r = r0.copy(order="F")
+        tracking.gpupass(ring, r, 1, rp, losses=True, mode=mode, gpu_pool=[device])
+        times = []
+        for _ in range(reps):
+            r = r0.copy(order="F")
+            t0 = time.perf_counter()
+            res = tracking.gpupass(ring, r, nt, rp, losses=True, mode=mode, gpu_pool=[device])
+            times.append(time.perf_counter() - t0)
+            del res
+        out[name] = {"wall_s": min(times), "particle_turns_per_s": n * nt / min(times)}
+    extra = out["with_refpts"]["wall_s"] - out["without_refpts"]["wall_s"]
+    out["snapshot_gb_per_s"] = out["rout_bytes"] / max(extra, 1e-9) / 1e9
     return out
 
 

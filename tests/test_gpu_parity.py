@@ -363,6 +363,34 @@ def test_snapshots_beyond_the_budget_track_in_particle_groups(mode):
         np.testing.assert_array_equal(ob[2][0], oa[2][0])
         assert (np.abs(ob[2][1] - oa[2][1]) <= 1e-12 * scale).all()
 
+
+def test_large_snapshot_copies_through_staging_match_direct():
+    """Snapshots above 8 MB a chunk come back through two pinned staging
+    buffers of 64 MB placed by host threads (pieces that end inside a slot's
+    row); below it, by direct copies.  593 MB of snapshots in nine pieces must
+    equal the same run returned in direct copies of 150-particle groups."""
+    ring = rings.fodo_ring()
+    eng = Engine.get(0)
+    cl = compile_lattice(ring, ring.energy, ELECTRON_REST)
+    lid = eng.upload(cl)
+    n, nt = 4000, 8
+    refs = np.arange(cl.nelem + 1, dtype=np.uint32)
+    r0 = rings.gaussian(n, seed=3) * 20.0
+    try:
+        ra = r0.copy(order="F")
+        oa, la, _ = eng.track(lid, ra, nt, refpts=refs, losses=True)
+        eng.set_launch(rout_budget_bytes=refs.size * 48 * 150)
+        rb = r0.copy(order="F")
+        ob, lb, _ = eng.track(lid, rb, nt, refpts=refs, losses=True)
+    finally:
+        eng.set_launch(rout_budget_bytes=4 << 30)
+        eng.free(lid)
+    assert oa.nbytes > 8 * (64 << 20) and la["islost"].any()
+    np.testing.assert_array_equal(rb, ra)
+    np.testing.assert_array_equal(ob, oa)
+    for k in la:
+        np.testing.assert_array_equal(lb[k], la[k], err_msg=k)
+
 def test_large_ring_one_turn():
     """The radiating large ring (misaligned, 1954 elements) against the oracle.
 
