@@ -49,6 +49,10 @@ def _args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--ref-step-seconds", type=float, default=10.0,
+                    help="reference arm: CPU seconds of tracking per step")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own GPU backend")
     ap.add_argument("--workload", default="large", choices=["large", "fodo"])
     ap.add_argument("--particles", type=int, default=None)
     ap.add_argument("--turns-per-step", type=int, default=None)
@@ -201,8 +205,8 @@ def run_reference(a):
     if not ref_runner.available():
         kind, fn = "port", _port_sample
     probe = fn(a.workload, max(64, 8 * threads), 1, threads)
-    # each step: about 10 s of CPU work, so K+W steps stay within minutes
-    n = int(max(64, min(200_000, probe["rate"] * 10.0)))
+    # each step: about 10 s of CPU work by default, so K+W steps stay within minutes
+    n = int(max(64, min(200_000, probe["rate"] * a.ref_step_seconds)))
     for _ in range(a.warmup):
         fn(a.workload, max(64, n // 10), 1, threads)
     rates, secs = [], []
@@ -225,10 +229,10 @@ def run_reference(a):
     # stock path, and with R1/R2 in the one-dimensional form it reads)
     gpu_ref = {}
     for tag, flat in (("stock", False), ("r1_r2_as_1d", True)):
-        if flat and a.workload != "large":
+        if a.no_reference_gpu or (flat and a.workload != "large"):
             continue
         gpu_ref[tag] = _atgpu_sample(a.workload, a.particles, a.turns_per_step, flat)
-    line["reference_gpu_backend"] = gpu_ref
+    line["reference_gpu_backend"] = gpu_ref or None
     print(json.dumps(line), flush=True)
     return 0
 
