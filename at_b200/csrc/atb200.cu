@@ -764,6 +764,10 @@ int copy_snapshots(atb_handle* h, cudaStream_t st, const double* dev, int64_t sl
         const char* stage = h->stage[p & 1];
         /* device bytes [b0, b1) of this piece to their rows of rout */
         auto place = [=](int64_t b0, int64_t b1) {
+            if (pitch == row) {              /* all particles: one block */
+                std::memcpy(dst + b0, stage + (b0 - off), (size_t)(b1 - b0));
+                return;
+            }
             while (b0 < b1) {
                 const int64_t slot = b0 / row, within = b0 - slot * row;
                 const int64_t n = std::min(b1 - b0, row - within);
